@@ -140,6 +140,8 @@ class Oracle:
     def msac(self, xn, X, P, sq_thr):
         s = C.c_double()
         c = C.c_int64()
+        xn = np.ascontiguousarray(xn, np.float64)
+        X = np.ascontiguousarray(X, np.float64)
         self.lib.orc_msac(xn, X, xn.shape[0], np.ascontiguousarray(P, np.float64).reshape(12), sq_thr,
                           C.byref(s), C.byref(c))
         return s.value, c.value
@@ -156,7 +158,8 @@ class Oracle:
 
     def get_inliers(self, q, t, xn, X, sq_thr):
         m = np.zeros(xn.shape[0], np.uint8)
-        self.lib.orc_get_inliers(np.asarray(q, np.float64), np.asarray(t, np.float64), xn, X,
+        self.lib.orc_get_inliers(np.ascontiguousarray(q, np.float64), np.ascontiguousarray(t, np.float64),
+                                 np.ascontiguousarray(xn, np.float64), np.ascontiguousarray(X, np.float64),
                                  xn.shape[0], sq_thr, m.ctypes.data)
         return m
 
@@ -169,6 +172,8 @@ class Oracle:
             hc = np.zeros(dump, np.int64)
             hi = np.zeros(dump, np.int64)
             hp = np.zeros((dump, 12))
+        xn = np.ascontiguousarray(xn, np.float64)
+        X = np.ascontiguousarray(X, np.float64)
         rc = self.lib.orc_ransac(xn, X, xn.shape[0], sq_thr, C.byref(cfg), C.byref(out),
                                  hs.ctypes.data if dump else None, hc.ctypes.data if dump else None,
                                  hi.ctypes.data if dump else None, hp.ctypes.data if dump else None, dump)

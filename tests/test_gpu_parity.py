@@ -1,0 +1,155 @@
+"""CUDA path (through the C ABI) against the FP64 oracle on identical samples.
+
+Tolerances (the parity bar):
+  * P3P hypotheses: same solution count per sample, poses within 1e-9
+  * FP32 MSAC scores: within 1e-5 relative of the FP64 scores
+  * inlier counts: exact except for points within 1e-4 px of the threshold
+  * selected best hypothesis: same sample and solution, FP64 score within 1e-12 relative
+  * final pose: within 1e-6 rad and 1e-6 m of the FP64 pipeline
+"""
+import numpy as np
+import pytest
+
+from helpers import near_threshold, normalized, quat_angle, sq_thr
+from turboransac_b200 import (BundleOptions_cuda, Camera_cuda, CameraPose_cuda, RansacOptions_cuda, TbrError,
+                              scenes)
+
+pytestmark = pytest.mark.gpu
+
+
+def cam_of(f):
+    return Camera_cuda(1, 640, 480, list(f.K))
+
+
+def test_debug_scores_counts_vs_oracle(ctx, oracle):
+    f = scenes.plain_frame(1)
+    S = 512
+    tr = oracle.sample_triples(f.seed, 0, S, f.n)
+    ids, poses, s32, cnt = ctx.debug_score_samples(f.uv, f.xyz, f.K, 4.0, tr, counts=True)
+    xn = normalized(f)
+    sq = sq_thr(f)
+    o = oracle.ransac(xn, f.xyz, sq, dump=4 * S, replay=tr, force_samples=S, samples_per_round=S)
+    np.testing.assert_array_equal(ids, o["hyp_ids"])
+    np.testing.assert_allclose(poses.reshape(-1, 12), o["hyp_poses"], rtol=1e-9, atol=1e-9)
+    s64 = o["hyp_scores"] / sq
+    rel = np.abs(s32.astype(np.float64) - s64) / s64
+    assert rel.max() < 1e-5, rel.max()
+    focal = 0.5 * (f.K[0] + f.K[1])
+    for k in range(ids.size):
+        d = abs(int(cnt[k]) - int(o["hyp_counts"][k]))
+        if d:
+            allowed = near_threshold(o["hyp_poses"][k].reshape(3, 4), xn, f.xyz, focal).sum()
+            assert d <= allowed, (k, d, allowed)
+
+
+@pytest.mark.parametrize("frame_id", [0, 3])
+def test_plain_call_matches_oracle(ctx, oracle, frame_id):
+    f = scenes.plain_frame(frame_id)
+    ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000)
+    d = st.details
+    info = o["info"]
+    assert d["samples"] == info.ransac.samples
+    assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+    assert d["ransac_inliers"] == info.ransac.count
+    assert abs(d["model_score"] - info.ransac.score) <= 1e-12 * info.ransac.score
+    assert d["num_inliers"] == info.num_inliers
+    np.testing.assert_array_equal(inl, o["inliers"])
+    assert quat_angle(pose.q, o["q"]) < 1e-6
+    assert np.abs(pose.t - o["t"]).max() < 1e-6
+    ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
+    assert ae < 5 and te < 5
+
+
+def test_scoring_bound_config_matches_oracle(ctx, oracle):
+    """N=20000, 15 % inliers, exactly 4096 samples (no early stop)."""
+    f = scenes.scoring_frame(0)
+    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                               force_samples=4096)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=4096, force_samples=4096, threads=8)
+    info = o["info"]
+    d = st.details
+    assert d["samples"] == 4096 == info.ransac.samples
+    assert d["hypotheses"] == info.ransac.hypotheses
+    assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+    assert d["ransac_inliers"] == info.ransac.count
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+    np.testing.assert_array_equal(inl, o["inliers"])
+
+
+def test_multi_round_termination_matches_oracle(ctx, oracle):
+    """10 % inliers: ~28 rounds of 1000 under the reference's stop rule, run by the
+    engine in a couple of speculative steps; samples, selection and pose must be
+    those of the sequential round loop."""
+    f = scenes.make_frame(3000, 0.10, 1.0, 4242)
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
+    info = o["info"]
+    d = st.details
+    assert info.ransac.rounds > 5
+    assert d["samples"] == info.ransac.samples and d["rounds"] == info.ransac.rounds
+    assert d["hypotheses"] == info.ransac.hypotheses
+    assert d["best_sample"] == info.ransac.best_sample
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_replayed_samples(ctx, oracle):
+    f = scenes.plain_frame(5)
+    rng = np.random.default_rng(1)
+    tr = np.stack([rng.choice(f.n, 3, replace=False) for _ in range(3000)]).astype(np.int32)
+    ro = RansacOptions_cuda(max_iterations=300, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), replay=tr)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, replay=tr, samples_per_round=300)
+    assert st.details["samples"] == o["info"].ransac.samples
+    assert st.details["best_sample"] == o["info"].ransac.best_sample
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_edge_cases(ctx, oracle):
+    ro = RansacOptions_cuda(max_iterations=64, max_reproj_error=4.0)
+    cam = Camera_cuda(1, 640, 480, [525.0, 525.0, 319.5, 239.5])
+    with pytest.raises(TbrError):
+        ctx.estimate_absolute_pose(np.zeros((2, 2)), np.zeros((2, 3)), cam, ro)
+    with pytest.raises(ValueError):
+        ctx.estimate_absolute_pose(np.zeros((5, 2)), np.zeros((4, 3)), cam, ro)
+    # exactly three points: every sample is a permutation of the one triple
+    f = scenes.make_frame(3, 1.0, 0.0, 77)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, seed=3)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=3, samples_per_round=64)
+    assert st.details["best_sample"] == o["info"].ransac.best_sample
+    np.testing.assert_array_equal(inl, o["inliers"])
+    # all points identical: P3P degenerates, no hypothesis is valid or all are NaN-poses
+    uv = np.tile([[300.0, 200.0]], (10, 1))
+    X = np.tile([[0.1, 0.2, 2.0]], (10, 1))
+    st, pose, inl = ctx.estimate_absolute_pose(uv, X, cam, ro, seed=1)
+    o = oracle.estimate(uv, X, np.array(cam.params), 4.0, seed=1, samples_per_round=64)
+    assert st.details["samples"] == o["info"].ransac.samples
+    # ragged small n
+    for n in (4, 5, 7, 65, 129):
+        f = scenes.make_frame(n, 0.8, 0.5, 100 + n)
+        st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, seed=f.seed)
+        o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=64)
+        assert st.details["best_sample"] == o["info"].ransac.best_sample
+        assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_get_inliers_matches_oracle(ctx, oracle):
+    f = scenes.plain_frame(2)
+    xn = normalized(f)
+    q = oracle.rotmat_to_quat(f.R_gt)
+    m = ctx.get_inliers(CameraPose_cuda(q, f.t_gt), xn, f.xyz, sq_thr(f))
+    np.testing.assert_array_equal(m, oracle.get_inliers(q, f.t_gt, xn, f.xyz, sq_thr(f)))
+
+
+def test_bundle_adjust_matches_reference_fixture(ctx):
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "lm.npz"))
+    for k in range(3):
+        cam = Camera_cuda(1, 640, 480, list(d[f"cam{k}"]))
+        pose, st = ctx.bundle_adjust(d[f"x{k}"], d[f"X{k}"], cam, CameraPose_cuda(d[f"q0_{k}"], d[f"t0_{k}"]),
+                                     BundleOptions_cuda(loss_scale=float(d[f"scale{k}"])))
+        assert quat_angle(pose.q, d[f"q1_{k}"]) < 1e-6
+        assert np.abs(pose.t - d[f"t1_{k}"]).max() < 1e-6

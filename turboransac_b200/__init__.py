@@ -1,0 +1,14 @@
+"""B200-native absolute-pose RANSAC (P3P + truncated MSAC + LM) behind the
+TurboRANSAC ``estimate_absolute_pose_cuda`` interface.
+
+The compute path is libtbr.so (hand-written sm_100a kernels behind the C ABI in
+include/tbr.h); this package is its Python host mirror.
+"""
+from . import build, scenes
+from .api import (BundleOptions_cuda, Camera_cuda, CameraPose_cuda, Context, RansacOptions_cuda,
+                  RansacStats_cuda, TbrError, bundle_adjust_cuda, default_context,
+                  estimate_absolute_pose_cuda, get_inliers_mx)
+
+__all__ = ["BundleOptions_cuda", "Camera_cuda", "CameraPose_cuda", "Context", "RansacOptions_cuda",
+           "RansacStats_cuda", "TbrError", "bundle_adjust_cuda", "default_context",
+           "estimate_absolute_pose_cuda", "get_inliers_mx"]

@@ -1,0 +1,290 @@
+"""Python mirror of the reference's absolute-pose interface, over libtbr.so.
+
+Names, argument meaning and defaults follow the reference's C++ API
+(Module/TbrCudaPnP/include/TbrCudaPnP/): ``RansacOptions_cuda``,
+``BundleOptions_cuda``, ``RansacStats_cuda`` (utils.h:14-72), ``Camera_cuda``
+(camera.cuh:10-85), ``CameraPose_cuda`` (pose.cuh:12-80),
+``estimate_absolute_pose_cuda`` / ``get_inliers_mx`` (entry.h:13-25) and
+``bundle_adjust_cuda`` (ba.cuh:17-24). Instead of exiting the process on a CUDA
+error (cudaCheck.h:4-14) every call raises ``TbrError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import TbrError, check
+
+__all__ = ["RansacOptions_cuda", "BundleOptions_cuda", "RansacStats_cuda", "Camera_cuda",
+           "CameraPose_cuda", "Context", "estimate_absolute_pose_cuda", "get_inliers_mx",
+           "bundle_adjust_cuda", "TbrError"]
+
+
+@dataclasses.dataclass
+class RansacOptions_cuda:
+    max_iterations: int = 100000      # reference meaning: samples per round (grid size)
+    min_iterations: int = 1000
+    dyn_num_trials_mult: float = 3.0
+    success_prob: float = 0.9999
+    max_reproj_error: float = 12.0
+    max_epipolar_error: float = 1.0
+    seed: int = 0
+    progressive_sampling: bool = False
+    max_prosac_iterations: int = 100000
+    real_focal_check: bool = False
+    score_initial_model: bool = False
+
+    def to_c(self) -> _lib.RansacOptionsC:
+        return _lib.RansacOptionsC(self.max_iterations, self.min_iterations, self.dyn_num_trials_mult,
+                                   self.success_prob, self.max_reproj_error, self.max_epipolar_error,
+                                   self.seed & 0xFFFFFFFFFFFFFFFF, int(self.progressive_sampling),
+                                   self.max_prosac_iterations, int(self.real_focal_check),
+                                   int(self.score_initial_model))
+
+
+@dataclasses.dataclass
+class BundleOptions_cuda:
+    TRIVIAL, TRUNCATED, HUBER, CAUCHY, TRUNCATED_LE_ZACH = range(5)
+    max_iterations: int = 100
+    loss_type: int = 3
+    loss_scale: float = 1.0
+    gradient_tol: float = 1e-10
+    step_tol: float = 1e-8
+    initial_lambda: float = 1e-3
+    min_lambda: float = 1e-10
+    max_lambda: float = 1e10
+    verbose: bool = False
+
+    def to_c(self) -> _lib.BundleOptionsC:
+        return _lib.BundleOptionsC(self.max_iterations, self.loss_type, self.loss_scale, self.gradient_tol,
+                                   self.step_tol, self.initial_lambda, self.min_lambda, self.max_lambda,
+                                   int(self.verbose))
+
+
+@dataclasses.dataclass
+class RansacStats_cuda:
+    refinements: int = 0
+    iterations: int = 0
+    num_inliers: int = 0
+    inlier_ratio: float = 0.0
+    model_score: float = float("inf")
+    # Beyond the reference (which returns these unfilled): engine details.
+    details: dict = dataclasses.field(default_factory=dict)
+
+
+@dataclasses.dataclass
+class Camera_cuda:
+    model_id: int = 1  # PINHOLE
+    width: int = -1
+    height: int = -1
+    params: list = dataclasses.field(default_factory=lambda: [0.0, 0.0, 0.0, 0.0])  # fx, fy, cx, cy
+
+    def focal(self) -> float:
+        return 0.5 * (self.params[0] + self.params[1])
+
+    def unproject(self, xp):
+        fx, fy, cx, cy = self.params
+        xp = np.asarray(xp, np.float64)
+        return np.stack([(xp[..., 0] - cx) / fx, (xp[..., 1] - cy) / fy], axis=-1)
+
+    def project(self, x):
+        fx, fy, cx, cy = self.params
+        x = np.asarray(x, np.float64)
+        return np.stack([fx * x[..., 0] + cx, fy * x[..., 1] + cy], axis=-1)
+
+    def rescale(self, scale: float) -> None:
+        self.params = [p * scale for p in self.params]
+
+
+def _quat_to_rotmat(q):
+    w, x, y, z = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+@dataclasses.dataclass
+class CameraPose_cuda:
+    """Unit quaternion q = (w, x, y, z) and t, with X_cam = R X + t."""
+
+    q: np.ndarray = dataclasses.field(default_factory=lambda: np.array([1.0, 0.0, 0.0, 0.0]))
+    t: np.ndarray = dataclasses.field(default_factory=lambda: np.zeros(3))
+
+    def R(self) -> np.ndarray:
+        return _quat_to_rotmat(self.q)
+
+    def Rt(self) -> np.ndarray:
+        return np.hstack([self.R(), np.asarray(self.t).reshape(3, 1)])
+
+    def Rt_homo(self) -> np.ndarray:
+        m = np.eye(4)
+        m[:3, :4] = self.Rt()
+        return m
+
+    def apply(self, X):
+        return np.asarray(X) @ self.R().T + self.t
+
+    def center(self) -> np.ndarray:
+        return -self.R().T @ self.t
+
+
+def _f64(a, cols):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if a.ndim != 2 or a.shape[1] != cols:
+        raise ValueError(f"expected an (N, {cols}) array, got {a.shape}")
+    return a
+
+
+class Context:
+    """One device context: a CUDA stream plus a reusable device workspace."""
+
+    def __init__(self, device: int = 0, workspace_bytes: int = 0):
+        L = _lib.lib()
+        h = C.c_void_p()
+        check(L.tbr_context_create(device, workspace_bytes, C.byref(h)))
+        self._h = h
+        self._lock = threading.Lock()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            _lib.lib().tbr_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- the reference's calls -------------------------------------------------
+    def estimate_absolute_pose(self, points2D, points3D, camera: Camera_cuda,
+                               ransac_opt: RansacOptions_cuda | None = None,
+                               bundle_opt: BundleOptions_cuda | None = None, *, seed: int | None = None,
+                               replay=None, force_samples: int = 0, skip_refine: bool = False,
+                               honor_options: bool = False, hyp_per_thread: int = 0,
+                               chunk_points: int = 0, max_total_samples: int = 0):
+        """Returns (RansacStats_cuda, CameraPose_cuda, inliers uint8[N])."""
+        x = _f64(points2D, 2)
+        X = _f64(points3D, 3)
+        if x.shape[0] != X.shape[0]:
+            raise ValueError("2D and 3D point counts must match")
+        ro = (ransac_opt or RansacOptions_cuda()).to_c()
+        bo = (bundle_opt or BundleOptions_cuda()).to_c()
+        ext = _lib.ExtOptionsC()
+        ext.honor_options = int(honor_options)
+        ext.skip_refine = int(skip_refine)
+        ext.force_samples = force_samples
+        ext.max_total_samples = max_total_samples
+        ext.seed = (seed or 0) & 0xFFFFFFFFFFFFFFFF
+        ext.hyp_per_thread = hyp_per_thread
+        ext.chunk_points = chunk_points
+        rep = None
+        if replay is not None:
+            rep = np.ascontiguousarray(np.asarray(replay, np.int32).reshape(-1, 3))
+            ext.replay_idx = rep.ctypes.data
+            ext.replay_count = rep.shape[0]
+        K = np.asarray(camera.params, np.float64)
+        q = np.zeros(4)
+        t = np.zeros(3)
+        inl = np.zeros(x.shape[0], np.uint8)
+        st = _lib.StatsC()
+        with self._lock:
+            check(_lib.lib().tbr_estimate_absolute_pose(
+                self._h, x.ctypes.data, X.ctypes.data, x.shape[0], K.ctypes.data, camera.width,
+                camera.height, C.byref(ro), C.byref(bo), C.byref(ext), q.ctypes.data, t.ctypes.data,
+                inl.ctypes.data, C.byref(st)))
+        stats = RansacStats_cuda(refinements=1 if not skip_refine else 0, iterations=st.samples,
+                                 num_inliers=st.num_inliers, inlier_ratio=st.inlier_ratio,
+                                 model_score=st.model_score, details=st.as_dict())
+        return stats, CameraPose_cuda(q, t), inl
+
+    def get_inliers(self, pose: CameraPose_cuda, x, X, sq_threshold: float):
+        x = _f64(x, 2)
+        X = _f64(X, 3)
+        q = np.ascontiguousarray(pose.q, np.float64)
+        t = np.ascontiguousarray(pose.t, np.float64)
+        out = np.zeros(x.shape[0], np.uint8)
+        cnt = C.c_int64()
+        with self._lock:
+            check(_lib.lib().tbr_get_inliers(self._h, q.ctypes.data, t.ctypes.data, x.ctypes.data,
+                                             X.ctypes.data, x.shape[0], sq_threshold, out.ctypes.data,
+                                             C.byref(cnt)))
+        return out
+
+    def bundle_adjust(self, x, X, camera: Camera_cuda, pose: CameraPose_cuda,
+                      opt: BundleOptions_cuda | None = None, weights=None, honor_options=False):
+        x = _f64(x, 2)
+        X = _f64(X, 3)
+        K = np.asarray(camera.params, np.float64)
+        q = np.array(pose.q, np.float64)
+        t = np.array(pose.t, np.float64)
+        bo = (opt or BundleOptions_cuda()).to_c()
+        ext = _lib.ExtOptionsC()
+        ext.honor_options = int(honor_options)
+        w = None
+        if weights is not None:
+            w = np.ascontiguousarray(weights, np.float64)
+        st = _lib.StatsC()
+        with self._lock:
+            check(_lib.lib().tbr_bundle_adjust(self._h, x.ctypes.data, X.ctypes.data, x.shape[0], K.ctypes.data,
+                                               q.ctypes.data, t.ctypes.data, C.byref(bo),
+                                               w.ctypes.data if w is not None else None, C.byref(ext),
+                                               C.byref(st)))
+        return CameraPose_cuda(q, t), st.as_dict()
+
+    def debug_score_samples(self, points2D, points3D, K, max_reproj_error, triples, counts=False):
+        """Per-hypothesis (ids, FP64 poses (H,3,4), FP32 scores in tau^2 units, counts or None)."""
+        x = _f64(points2D, 2)
+        X = _f64(points3D, 3)
+        tr = np.ascontiguousarray(np.asarray(triples, np.int32).reshape(-1, 3))
+        cap = 4 * tr.shape[0]
+        ids = np.zeros(cap, np.int64)
+        poses = np.zeros((cap, 12))
+        s32 = np.zeros(cap, np.float32)
+        cnt = np.zeros(cap, np.int64) if counts else None
+        nh = C.c_int64()
+        Kc = np.asarray(K, np.float64)
+        with self._lock:
+            check(_lib.lib().tbr_debug_score_samples(
+                self._h, x.ctypes.data, X.ctypes.data, x.shape[0], Kc.ctypes.data, max_reproj_error,
+                tr.ctypes.data, tr.shape[0], ids.ctypes.data, poses.ctypes.data, s32.ctypes.data,
+                cnt.ctypes.data if counts else None, cap, C.byref(nh)))
+        m = nh.value
+        return ids[:m], poses[:m].reshape(m, 3, 4), s32[:m], (cnt[:m] if counts else None)
+
+
+_default_ctx = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default_ctx
+    with _default_lock:
+        if _default_ctx is None:
+            _default_ctx = Context()
+        return _default_ctx
+
+
+def estimate_absolute_pose_cuda(points2D, points3D, camera: Camera_cuda, ransac_opt: RansacOptions_cuda,
+                                bundle_opt: BundleOptions_cuda, **kw):
+    """entry.h:13-19: returns (RansacStats_cuda, CameraPose_cuda, inliers)."""
+    return default_context().estimate_absolute_pose(points2D, points3D, camera, ransac_opt, bundle_opt, **kw)
+
+
+def get_inliers_mx(pose: CameraPose_cuda, x, X, sq_threshold: float):
+    """entry.h:22-25: inlier mask (uint8) with the reprojection and cheirality test."""
+    return default_context().get_inliers(pose, x, X, sq_threshold)
+
+
+def bundle_adjust_cuda(x, X, camera: Camera_cuda, pose: CameraPose_cuda, opt: BundleOptions_cuda,
+                       weights=None):
+    """ba.cuh:17-24: LM refinement; returns the refined CameraPose_cuda."""
+    return default_context().bundle_adjust(x, X, camera, pose, opt, weights)[0]

@@ -1,0 +1,849 @@
+// Host engine and C ABI of libtbr.so (see include/tbr.h).
+//
+// One Engine per tbr_context: a CUDA stream, a device workspace carved once
+// from one allocation (points, staging blocks, hypotheses, candidates, LM
+// arrays), pinned host staging, and the step launcher. The reference allocates
+// and frees every buffer per call (turbo_ransac.cu:36-112, 272-286; ba.cu:41-62)
+// and synchronises the whole device 4 times per round; here nothing is
+// allocated per call and a round needs no host round-trip.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/tbr.h"
+#include "tbr_kernels.cuh"
+
+namespace tbr {
+
+thread_local std::string g_last_error;
+
+static tbr_status fail(tbr_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+#define TBR_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(TBR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));         \
+    } while (0)
+
+// First-fit allocator over staging blocks, with coalescing on free.
+class BlockAllocator {
+   public:
+    void reset(int64_t cap) {
+        free_.clear();
+        if (cap > 0) free_[0] = cap;
+        cap_ = cap;
+        used_ = 0;
+    }
+    int64_t alloc(int64_t n) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                const int64_t off = it->first, sz = it->second;
+                free_.erase(it);
+                if (sz > n) free_[off + n] = sz - n;
+                used_ += n;
+                return off;
+            }
+        }
+        return -1;
+    }
+    void release(int64_t off, int64_t n) {
+        used_ -= n;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    int64_t used() const { return used_; }
+    int64_t capacity() const { return cap_; }
+
+   private:
+    std::map<int64_t, int64_t> free_;
+    int64_t cap_ = 0, used_ = 0;
+};
+
+struct FrameHost {
+    const double *uv;
+    const double *xyz;
+    int64_t n;
+    double K[4];
+    uint64_t seed;
+    double max_reproj_error;
+    const int32_t *replay;  // host
+    int64_t replay_count;
+};
+
+struct RunOptions {
+    int64_t B = 1000;
+    int64_t max_total = 100000;
+    int64_t force_samples = 0;
+    double success_prob = 0.9999;
+    double trials_mult = 3.0;
+    int skip_refine = 0;
+    int hr = 8;
+    int chunk_points = 0;
+    // LM (compat: default BundleOptions_cuda with loss_scale = 1/f)
+    int64_t lm_max_iter = 100;
+    double lm_loss_scale_px = 1.0;  // loss scale in pixels (multiplied by 1/f)
+    double lm_grad_tol = 1e-10, lm_step_tol = 1e-8, lm_lambda0 = 1e-3, lm_min_lambda = 1e-10,
+           lm_max_lambda = 1e10;
+};
+
+static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundle_options *bo,
+                                   const tbr_ext_options *ext) {
+    RunOptions o;
+    if (ro) o.B = (int64_t)ro->max_iterations;
+    const bool honor = ext && ext->honor_options;
+    if (ext) {
+        o.skip_refine = ext->skip_refine;
+        o.force_samples = ext->force_samples;
+        if (ext->max_total_samples > 0) o.max_total = ext->max_total_samples;
+        if (ext->hyp_per_thread == 4 || ext->hyp_per_thread == 8) o.hr = ext->hyp_per_thread;
+        o.chunk_points = ext->chunk_points;
+    }
+    if (honor && ro) {
+        o.success_prob = ro->success_prob;
+        o.trials_mult = ro->dyn_num_trials_mult;
+    }
+    if (honor && bo) {
+        o.lm_max_iter = (int64_t)bo->max_iterations;
+        o.lm_loss_scale_px = bo->loss_scale;
+        o.lm_grad_tol = bo->gradient_tol;
+        o.lm_step_tol = bo->step_tol;
+        o.lm_lambda0 = bo->initial_lambda;
+        o.lm_min_lambda = bo->min_lambda;
+        o.lm_max_lambda = bo->max_lambda;
+    }
+    return o;
+}
+
+class Engine {
+   public:
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    Pools P{};            // device pointers (host copy)
+    int max_frames = 0;
+    int64_t max_blocks = 0;
+    void *d_base = nullptr;
+    size_t d_bytes = 0;
+    BlockAllocator blocks;
+    std::vector<int> free_slots;
+    // pinned host staging
+    void *h_stage = nullptr;
+    size_t h_stage_bytes = 0;
+    unsigned long long *h_counters = nullptr;
+    int32_t *d_active = nullptr;
+    int32_t *d_replay = nullptr;
+    int64_t d_replay_cap = 0;
+    int score_grid[2] = {0, 0};
+    int rescore_grid = 0, p3p_grid = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::mutex mu;  // one call at a time per context
+
+    ~Engine() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (d_base) cudaFree(d_base);
+        if (h_stage) cudaFreeHost(h_stage);
+        if (h_counters) cudaFreeHost(h_counters);
+        if (d_replay) cudaFree(d_replay);
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    tbr_status init(int dev, uint64_t budget, int frames_cap = 256) {
+        device = dev;
+        TBR_CUDA(cudaSetDevice(dev));
+        TBR_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        TBR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        TBR_CUDA(cudaEventCreate(&ev0));
+        TBR_CUDA(cudaEventCreate(&ev1));
+        if (budget == 0) budget = 1ull << 30;
+        max_frames = std::min(frames_cap, kMaxActive);
+        // Split: 30 % hypotheses, the rest points, after the per-frame state.
+        const size_t per_frame = sizeof(FrameDev) + sizeof(FrameResult) + sizeof(int32_t) +
+                                 (size_t)kMaxCand * (4 + 8 + 8 + 4) +
+                                 (size_t)kMaxCand * kMaxRChunks * 12 + 64;
+        const size_t fixed = (size_t)max_frames * per_frame + 3 * (kMaxActive + 1) * 8 + 4096 * 8;
+        if (budget < fixed + (64ull << 20)) return fail(TBR_ERR_INVALID_ARG, "workspace too small");
+        const size_t rest = budget - fixed;
+        const size_t per_hyp = 96 + 48 + 8 + 4 + 4 * 32 + 4;
+        P.max_hyps = (int64_t)(rest * 0.3 / per_hyp);
+        P.max_hyps = std::max<int64_t>(P.max_hyps, 4096);
+        P.max_parts = P.max_hyps * 32;
+        P.max_hb = P.max_hyps / 32 + kMaxActive;
+        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 16 + 16) + kBlockBytes;
+        max_blocks = (int64_t)((rest - (size_t)(P.max_hyps * per_hyp) - P.max_hb * 4) / per_block) - 1;
+        if (max_blocks < 64) return fail(TBR_ERR_INVALID_ARG, "workspace too small for points");
+        // One allocation, carved with 256-byte alignment.
+        std::vector<std::pair<void **, size_t>> parts;
+        const int64_t np = max_blocks * kSub;
+        auto add = [&](void **p, size_t bytes) { parts.push_back({p, bytes}); };
+        add((void **)&P.frames, sizeof(FrameDev) * max_frames);
+        add((void **)&P.results, sizeof(FrameResult) * max_frames);
+        add((void **)&d_active, sizeof(int32_t) * kMaxActive);
+        add((void **)&P.uv64, 16 * np);
+        add((void **)&P.X64, 24 * np);
+        add((void **)&P.xn64, 16 * np);
+        add((void **)&P.mask, np);
+        add((void **)&P.lx64, 16 * np);
+        add((void **)&P.lX64, 24 * np);
+        add((void **)&P.lA32, 16 * np);
+        add((void **)&P.lB32, 16 * np);
+        add((void **)&P.pts32, (size_t)kBlockBytes * max_blocks);
+        add((void **)&P.sample_prefix, 8 * (kMaxActive + 1));
+        add((void **)&P.item_prefix, 8 * (kMaxActive + 1));
+        add((void **)&P.ritem_prefix, 8 * (kMaxActive + 1));
+        add((void **)&P.hP64, 96 * P.max_hyps);
+        add((void **)&P.hP32, 48 * P.max_hyps);
+        add((void **)&P.hId, 8 * P.max_hyps);
+        add((void **)&P.hS32, 4 * P.max_hyps);
+        add((void **)&P.part, 4 * P.max_parts);
+        add((void **)&P.hb_arrive, 4 * P.max_hb);
+        add((void **)&P.cHyp, 4 * (size_t)max_frames * kMaxCand);
+        add((void **)&P.cS64, 8 * (size_t)max_frames * kMaxCand);
+        add((void **)&P.cCnt, 8 * (size_t)max_frames * kMaxCand);
+        add((void **)&P.cpS, 8 * (size_t)max_frames * kMaxCand * kMaxRChunks);
+        add((void **)&P.cpC, 4 * (size_t)max_frames * kMaxCand * kMaxRChunks);
+        add((void **)&P.c_arrive, 4 * (size_t)max_frames * kMaxCand);
+        add((void **)&P.counters, 8 * kCNum);
+        add((void **)&P.dbg_counts, 8 * P.max_hyps);
+        size_t total = 0;
+        for (auto &p : parts) total += (p.second + 255) & ~size_t(255);
+        TBR_CUDA(cudaMalloc(&d_base, total));
+        d_bytes = total;
+        char *cur = (char *)d_base;
+        for (auto &p : parts) {
+            *p.first = cur;
+            cur += (p.second + 255) & ~size_t(255);
+        }
+        P.active = d_active;
+        P.num_sms = num_sms;
+        TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
+        TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
+        blocks.reset(max_blocks);
+        for (int i = max_frames - 1; i >= 0; --i) free_slots.push_back(i);
+        int occ = 0;
+        TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_score<2>, kScoreWarps * 32, 0));
+        score_grid[0] = num_sms * std::max(occ, 1);
+        TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_score<4>, kScoreWarps * 32, 0));
+        score_grid[1] = num_sms * std::max(occ, 1);
+        TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rescore, 256, 0));
+        rescore_grid = num_sms * std::max(occ, 1);
+        p3p_grid = num_sms * 8;
+        TBR_CUDA(cudaStreamSynchronize(stream));
+        return TBR_OK;
+    }
+
+    tbr_status ensure_stage(size_t bytes) {
+        if (bytes <= h_stage_bytes) return TBR_OK;
+        if (h_stage) {
+            TBR_CUDA(cudaStreamSynchronize(stream));
+            cudaFreeHost(h_stage);
+            h_stage = nullptr;
+        }
+        size_t nb = std::max(bytes, h_stage_bytes * 2);
+        TBR_CUDA(cudaMallocHost(&h_stage, nb));
+        h_stage_bytes = nb;
+        return TBR_OK;
+    }
+
+    tbr_status ensure_replay(int64_t count) {
+        if (count <= d_replay_cap) return TBR_OK;
+        if (d_replay) {
+            TBR_CUDA(cudaStreamSynchronize(stream));
+            cudaFree(d_replay);
+            d_replay = nullptr;
+        }
+        TBR_CUDA(cudaMalloc(&d_replay, sizeof(int32_t) * 3 * count));
+        d_replay_cap = count;
+        return TBR_OK;
+    }
+
+    // Builds the device state of one frame (no device traffic).
+    FrameDev make_frame(const FrameHost &fh, int64_t blk_off, const RunOptions &o,
+                        const int32_t *d_rep) const {
+        FrameDev f;
+        std::memset(&f, 0, sizeof(f));
+        f.n = fh.n;
+        f.blk_off = blk_off;
+        f.n_blocks = (int32_t)((fh.n + kSub - 1) / kSub);
+        f.status = kRansac;
+        f.seed = fh.seed;
+        f.replay = d_rep;
+        f.replay_count = fh.replay_count;
+        for (int k = 0; k < 4; ++k) f.K[k] = fh.K[k];
+        f.focal = 0.5 * (fh.K[0] + fh.K[1]);          // Camera_cuda::focal, camera.cuh:64-67
+        f.tau = fh.max_reproj_error / f.focal;        // entry.cu:48-49
+        f.sq_thr = f.tau * f.tau;                     // turbo_ransac.cu:34
+        for (int k = 0; k < 3; ++k) {
+            f.bmin[k] = ~0ull;
+            f.bmax[k] = 0ull;
+        }
+        f.B = o.B;
+        f.max_total = o.max_total;
+        f.force_samples = o.force_samples;
+        f.log_missing = std::log(1.0 - o.success_prob);
+        f.trials_mult = o.trials_mult;
+        f.skip_refine = o.skip_refine;
+        f.hr = o.hr;
+        f.chunk_points = o.chunk_points;
+        f.lm_max_iter = o.lm_max_iter;
+        const double sc = 1.0 / f.focal;  // entry.cu:87,107-114: LM in pixel/f units
+        for (int k = 0; k < 4; ++k) f.lm_cam[k] = fh.K[k] * sc;
+        const double ls = o.lm_loss_scale_px / f.focal;  // entry.cu:122-123
+        f.lm_inv_sq_thr = 1.0 / (ls * ls);
+        f.lm_grad_tol = o.lm_grad_tol;
+        f.lm_step_tol = o.lm_step_tol;
+        f.lm_lambda0 = o.lm_lambda0;
+        f.lm_min_lambda = o.lm_min_lambda;
+        f.lm_max_lambda = o.lm_max_lambda;
+        f.best_score = DBL_MAX;
+        f.best_sample = -1;
+        f.best_sol = -1;
+        return f;
+    }
+
+    // Enqueue the step kernels for the current active list.
+    void launch_step(int n_active, int hr) {
+        k_plan<<<1, kMaxActive, 0, stream>>>(P);
+        k_sample_p3p<<<p3p_grid, 128, 0, stream>>>(P);
+        k_score_plan<<<1, kMaxActive, 0, stream>>>(P);
+        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, stream>>>(P);
+        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, stream>>>(P);
+        k_select<<<n_active, 256, 0, stream>>>(P);
+        k_rescore_plan<<<1, kMaxActive, 0, stream>>>(P);
+        k_rescore<<<rescore_grid, 256, 0, stream>>>(P);
+        k_finalize<<<(n_active + 127) / 128, 128, 0, stream>>>(P);
+        k_inliers<<<n_active, 1024, 0, stream>>>(P);
+        k_lm<<<n_active, kLMThreads, 0, stream>>>(P);
+    }
+
+    void launch_prep(int n_active, int64_t max_n) {
+        const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024));
+        k_prep_bounds<<<dim3(bx, n_active), 256, 0, stream>>>(P);
+        k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(P);
+    }
+
+    // Runs admitted frames (slots) to completion with one host check per step.
+    tbr_status run(const std::vector<int> &slots, int hr, int max_steps, int *steps_out) {
+        const int na = (int)slots.size();
+        int steps = 0;
+        for (;;) {
+            TBR_CUDA(cudaMemsetAsync(P.counters + kCStillRansac, 0, 16, stream));
+            launch_step(na, hr);
+            TBR_CUDA(cudaGetLastError());
+            TBR_CUDA(cudaMemcpyAsync(h_counters, P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, stream));
+            TBR_CUDA(cudaStreamSynchronize(stream));
+            ++steps;
+            if (h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+            if (h_counters[kCStillRansac] == 0) break;
+            if (steps >= max_steps) return fail(TBR_ERR_INTERNAL, "step limit reached");
+        }
+        if (steps_out) *steps_out = steps;
+        return TBR_OK;
+    }
+};
+
+// Uploads frames into slots (host -> device through pinned staging).
+static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
+                               std::vector<int> &slots, int64_t &max_n) {
+    if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
+    size_t stage = 0;
+    int64_t replay_total = 0;
+    for (auto &f : fr) {
+        stage += (size_t)f.n * 40;
+        replay_total += f.replay ? f.replay_count : 0;
+    }
+    stage += sizeof(FrameDev) * fr.size() + 4 * fr.size() + 256;
+    tbr_status st = E.ensure_stage(stage);
+    if (st) return st;
+    if (replay_total) {
+        st = E.ensure_replay(replay_total);
+        if (st) return st;
+    }
+    char *h = (char *)E.h_stage;
+    std::vector<FrameDev> devs;
+    int64_t rep_off = 0;
+    max_n = 0;
+    for (auto &f : fr) {
+        const int64_t nb = (f.n + kSub - 1) / kSub;
+        const int64_t off = E.blocks.alloc(nb);
+        if (off < 0) {
+            for (size_t i = 0; i < slots.size(); ++i) E.blocks.release(devs[i].blk_off, devs[i].n_blocks);
+            for (int s : slots) E.free_slots.push_back(s);
+            slots.clear();
+            return fail(TBR_ERR_OOM, "point workspace exhausted");
+        }
+        const int slot = E.free_slots.back();
+        E.free_slots.pop_back();
+        slots.push_back(slot);
+        const int32_t *d_rep = nullptr;
+        if (f.replay) {
+            d_rep = E.d_replay + 3 * rep_off;
+            TBR_CUDA(cudaMemcpyAsync((void *)d_rep, f.replay, 12 * f.replay_count, cudaMemcpyHostToDevice, E.stream));
+            rep_off += f.replay_count;
+        }
+        devs.push_back(E.make_frame(f, off, o, d_rep));
+        const int64_t p0 = off * kSub;
+        std::memcpy(h, f.uv, 16 * f.n);
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), h, 16 * f.n, cudaMemcpyHostToDevice, E.stream));
+        h += (16 * f.n + 255) & ~int64_t(255);
+        std::memcpy(h, f.xyz, 24 * f.n);
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), h, 24 * f.n, cudaMemcpyHostToDevice, E.stream));
+        h += (24 * f.n + 255) & ~int64_t(255);
+        max_n = std::max(max_n, f.n);
+    }
+    for (size_t i = 0; i < slots.size(); ++i) {
+        FrameDev *hd = (FrameDev *)h;
+        *hd = devs[i];
+        TBR_CUDA(cudaMemcpyAsync(E.P.frames + slots[i], hd, sizeof(FrameDev), cudaMemcpyHostToDevice, E.stream));
+        h += (sizeof(FrameDev) + 255) & ~size_t(255);
+    }
+    int32_t *ha = (int32_t *)h;
+    for (size_t i = 0; i < slots.size(); ++i) ha[i] = slots[i];
+    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * slots.size(), cudaMemcpyHostToDevice, E.stream));
+    E.P.n_active = (int32_t)slots.size();
+    return TBR_OK;
+}
+
+static void fill_stats(const FrameResult &r, int64_t n, tbr_stats *st, float ms) {
+    if (!st) return;
+    st->samples = r.samples;
+    st->rounds = r.rounds;
+    st->hypotheses = r.hypotheses;
+    st->ransac_inliers = r.ransac_inliers;
+    st->num_inliers = r.num_inliers;
+    st->inlier_ratio = n > 0 ? (double)r.num_inliers / (double)n : 0.0;
+    st->model_score = r.model_score;
+    st->best_sample = r.best_sample;
+    st->best_solution = r.best_sol;
+    st->steps = r.steps;
+    st->candidates_rescored = r.rescored;
+    st->candidate_overflow = r.overflow;
+    st->lm_iterations = r.lm_iters;
+    st->lm_invalid_steps = r.lm_invalid;
+    st->lm_initial_cost = r.lm_cost0;
+    st->lm_cost = r.lm_cost;
+    st->gpu_ms = ms;
+}
+
+}  // namespace tbr
+
+using namespace tbr;
+
+struct tbr_context {
+    Engine E;
+};
+
+// =================================================================== C ABI ==
+extern "C" {
+
+int tbr_abi_version(void) { return TBR_ABI_VERSION; }
+const char *tbr_last_error(void) { return g_last_error.c_str(); }
+
+void tbr_default_ransac_options(tbr_ransac_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_iterations = 100000;
+    o->min_iterations = 1000;
+    o->dyn_num_trials_mult = 3.0;
+    o->success_prob = 0.9999;
+    o->max_reproj_error = 12.0;
+    o->max_epipolar_error = 1.0;
+    o->seed = 0;
+    o->max_prosac_iterations = 100000;
+}
+
+void tbr_default_bundle_options(tbr_bundle_options *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->max_iterations = 100;
+    o->loss_type = 3;
+    o->loss_scale = 1.0;
+    o->gradient_tol = 1e-10;
+    o->step_tol = 1e-8;
+    o->initial_lambda = 1e-3;
+    o->min_lambda = 1e-10;
+    o->max_lambda = 1e10;
+}
+
+tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context **out) {
+    if (!out) return fail(TBR_ERR_INVALID_ARG, "out is NULL");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(TBR_ERR_CUDA, "no CUDA device available");
+    if (device < 0 || device >= ndev) return fail(TBR_ERR_INVALID_ARG, "bad device ordinal");
+    auto *c = new tbr_context();
+    tbr_status s = c->E.init(device, workspace_bytes);
+    if (s != TBR_OK) {
+        delete c;
+        return s;
+    }
+    *out = c;
+    return TBR_OK;
+}
+
+void tbr_context_destroy(tbr_context *ctx) { delete ctx; }
+
+static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                  std::vector<FrameResult> &res, std::vector<uint8_t *> masks,
+                                  float *ms_out, int *steps_out) {
+    Engine &E = ctx->E;
+    std::vector<int> slots;
+    int64_t max_n = 0;
+    TBR_CUDA(cudaSetDevice(E.device));
+    TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
+    tbr_status st = admit_frames(E, fr, o, slots, max_n);
+    if (st) return st;
+    std::vector<int64_t> offs;
+    TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
+    E.launch_prep((int)slots.size(), max_n);
+    st = E.run(slots, o.hr, 100000, steps_out);
+    TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    if (st == TBR_OK) {
+        res.resize(fr.size());
+        FrameResult *hres = (FrameResult *)E.h_stage;
+        for (size_t i = 0; i < slots.size(); ++i)
+            TBR_CUDA(cudaMemcpyAsync(hres + i, E.P.results + slots[i], sizeof(FrameResult),
+                                     cudaMemcpyDeviceToHost, E.stream));
+        // inlier masks go straight into the caller's buffers (pageable: copied synchronously
+        // with respect to the stream by the driver)
+        FrameDev fd;
+        for (size_t i = 0; i < slots.size(); ++i) {
+            if (i < masks.size() && masks[i]) {
+                TBR_CUDA(cudaMemcpyAsync(&fd, E.P.frames + slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream));
+                TBR_CUDA(cudaStreamSynchronize(E.stream));
+                TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + fd.blk_off * kSub, fr[i].n, cudaMemcpyDeviceToHost, E.stream));
+            }
+        }
+        TBR_CUDA(cudaStreamSynchronize(E.stream));
+        for (size_t i = 0; i < slots.size(); ++i) res[i] = hres[i];
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, E.ev0, E.ev1);
+        if (ms_out) *ms_out = ms;
+    }
+    // release
+    cudaStreamSynchronize(E.stream);
+    std::vector<FrameDev> hd(slots.size());
+    for (size_t i = 0; i < slots.size(); ++i)
+        cudaMemcpy(&hd[i], E.P.frames + slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost);
+    for (size_t i = 0; i < slots.size(); ++i) {
+        E.blocks.release(hd[i].blk_off, hd[i].n_blocks);
+        E.free_slots.push_back(slots[i]);
+    }
+    return st;
+}
+
+tbr_status tbr_estimate_absolute_pose(tbr_context *ctx, const double *points2D, const double *points3D,
+                                      int64_t n, const double K[4], int32_t width, int32_t height,
+                                      const tbr_ransac_options *ransac_opt,
+                                      const tbr_bundle_options *bundle_opt, const tbr_ext_options *ext,
+                                      double q[4], double t[3], uint8_t *inliers, tbr_stats *stats) {
+    (void)width;
+    (void)height;
+    if (!ctx || !points2D || !points3D || !K || !q || !t) return fail(TBR_ERR_INVALID_ARG, "NULL argument");
+    if (n < 3) return fail(TBR_ERR_INVALID_ARG, "need at least 3 correspondences");
+    if (!(K[0] > 0) || !(K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "focal lengths must be positive");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations (samples per round) must be >= 1");
+    if (!(ro.max_reproj_error > 0)) return fail(TBR_ERR_INVALID_ARG, "max_reproj_error must be > 0");
+    RunOptions o = make_run_options(&ro, bundle_opt, ext);
+    FrameHost fh{points2D, points3D, n, {K[0], K[1], K[2], K[3]}, ro.seed, ro.max_reproj_error, nullptr, 0};
+    if (ext && ext->seed) fh.seed = ext->seed;
+    if (ext && ext->replay_idx) {
+        if (ext->replay_count < 1) return fail(TBR_ERR_INVALID_ARG, "empty replay buffer");
+        for (int64_t i = 0; i < 3 * ext->replay_count; ++i)
+            if (ext->replay_idx[i] < 0 || ext->replay_idx[i] >= n)
+                return fail(TBR_ERR_INVALID_ARG, "replayed index out of range");
+        if (o.force_samples > 0) {
+            if (o.force_samples > ext->replay_count)
+                return fail(TBR_ERR_INVALID_ARG, "replay buffer shorter than force_samples");
+        } else {
+            // Rounds always draw B samples; a replayed run stops at the last full round.
+            if (ext->replay_count < o.B) return fail(TBR_ERR_INVALID_ARG, "replay buffer shorter than one round");
+            o.max_total = std::min<int64_t>(o.max_total, (ext->replay_count / o.B) * o.B);
+        }
+        fh.replay = ext->replay_idx;
+        fh.replay_count = ext->replay_count;
+    }
+    std::lock_guard<std::mutex> lk(ctx->E.mu);
+    std::vector<FrameResult> res;
+    float ms = 0.f;
+    int steps = 0;
+    tbr_status st = estimate_frames(ctx, {fh}, o, res, {inliers}, &ms, &steps);
+    if (st) return st;
+    for (int k = 0; k < 4; ++k) q[k] = res[0].q[k];
+    for (int k = 0; k < 3; ++k) t[k] = res[0].t[k];
+    fill_stats(res[0], n, stats, ms);
+    return TBR_OK;
+}
+
+tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                              const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                              tbr_frame_result *results, uint8_t *const *inliers) {
+    if (!ctx || !frames || n_frames < 1 || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    RunOptions o = make_run_options(&ro, nullptr, ext);
+    std::vector<FrameHost> fr;
+    for (int i = 0; i < n_frames; ++i) {
+        const tbr_frame_desc &d = frames[i];
+        if (d.n < 3 || !d.points2D || !d.points3D) return fail(TBR_ERR_INVALID_ARG, "bad frame");
+        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
+                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+    }
+    std::lock_guard<std::mutex> lk(ctx->E.mu);
+    std::vector<FrameResult> res;
+    std::vector<uint8_t *> masks(n_frames, nullptr);
+    if (inliers)
+        for (int i = 0; i < n_frames; ++i) masks[i] = inliers[i];
+    float ms = 0.f;
+    int steps = 0;
+    tbr_status st = estimate_frames(ctx, fr, o, res, masks, &ms, &steps);
+    if (st) return st;
+    for (int i = 0; i < n_frames; ++i) {
+        for (int k = 0; k < 4; ++k) results[i].q[k] = res[i].q[k];
+        for (int k = 0; k < 3; ++k) results[i].t[k] = res[i].t[k];
+        results[i].status = TBR_OK;
+        fill_stats(res[i], fr[i].n, &results[i].stats, ms);
+    }
+    return TBR_OK;
+}
+
+tbr_status tbr_get_inliers(tbr_context *ctx, const double q[4], const double t[3], const double *x,
+                           const double *X, int64_t n, double sq_threshold, uint8_t *inliers,
+                           int64_t *count) {
+    if (!ctx || !q || !t || !x || !X || n < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    if (n == 0) {
+        if (count) *count = 0;
+        return TBR_OK;
+    }
+    const int64_t nb = (n + kSub - 1) / kSub;
+    const int64_t off = E.blocks.alloc(nb);
+    if (off < 0) return fail(TBR_ERR_OOM, "point workspace exhausted");
+    const int64_t p0 = off * kSub;
+    tbr_status st = E.ensure_stage(40 * n + 1024 + n);
+    if (st) { E.blocks.release(off, nb); return st; }
+    char *h = (char *)E.h_stage;
+    std::memcpy(h, x, 16 * n);
+    std::memcpy(h + 16 * n, X, 24 * n);
+    double *hq = (double *)(h + 40 * n);
+    for (int k = 0; k < 4; ++k) hq[k] = q[k];
+    for (int k = 0; k < 3; ++k) hq[4 + k] = t[k];
+    // x goes to the normalized-coordinate pool, X to the world-point pool; the
+    // pose rides in the first hypothesis slot.
+    TBR_CUDA(cudaMemcpyAsync(E.P.xn64 + 2 * p0, h, 16 * n, cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), h + 16 * n, 24 * n, cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.P.hP64, hq, 7 * 8, cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemsetAsync(E.P.counters + kCWorkPairs, 0, 8, E.stream));
+    const int grid = (int)std::min<int64_t>(E.num_sms * 4, (n + 255) / 256);
+    k_pose_mask<<<grid, 256, 0, E.stream>>>(E.P.xn64 + 2 * p0, E.P.X64 + 3 * p0, n, E.P.hP64, sq_threshold,
+                                            E.P.mask + p0, E.P.counters + kCWorkPairs);
+    st = TBR_OK;
+    if (cudaGetLastError() != cudaSuccess) st = fail(TBR_ERR_CUDA, "k_pose_mask launch failed");
+    uint8_t *hm = (uint8_t *)(h + 40 * n + 64);
+    if (!st) {
+        cudaMemcpyAsync(hm, E.P.mask + p0, n, cudaMemcpyDeviceToHost, E.stream);
+        cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream);
+    }
+    if (cudaStreamSynchronize(E.stream) != cudaSuccess && !st) st = fail(TBR_ERR_CUDA, "get_inliers failed");
+    E.blocks.release(off, nb);
+    if (st) return st;
+    if (inliers) std::memcpy(inliers, hm, n);
+    if (count) *count = (int64_t)E.h_counters[kCWorkPairs];
+    return TBR_OK;
+}
+
+tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X, int64_t n, const double K[4],
+                             double q[4], double t[3], const tbr_bundle_options *opt, const double *weights,
+                             const tbr_ext_options *ext, tbr_stats *stats) {
+    (void)weights;  // ignored, as in the reference (jaco.cuh:36,123 use a uniform weight)
+    (void)ext;
+    if (!ctx || !x || !X || !K || !q || !t || n < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    tbr_bundle_options bo;
+    tbr_default_bundle_options(&bo);
+    if (opt) bo = *opt;
+    if (!(bo.loss_scale > 0)) return fail(TBR_ERR_INVALID_ARG, "loss_scale must be > 0");
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    RunOptions o;
+    FrameHost fh{x, X, std::max<int64_t>(n, 1), {K[0], K[1], K[2], K[3]}, 0, 1.0, nullptr, 0};
+    if (n == 0) {
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return TBR_OK;
+    }
+    std::vector<int> slots;
+    int64_t max_n = 0;
+    TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
+    tbr_status st = admit_frames(E, {fh}, o, slots, max_n);
+    if (st) return st;
+    FrameDev fd;
+    TBR_CUDA(cudaMemcpyAsync(&fd, E.P.frames + slots[0], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    fd.status = kLMPending;
+    fd.focal = 1.0;
+    for (int k = 0; k < 4; ++k) fd.lm_cam[k] = K[k];
+    fd.lm_inv_sq_thr = 1.0 / (bo.loss_scale * bo.loss_scale);  // CauchyLoss_cuda(loss_scale)
+    fd.lm_max_iter = (int64_t)bo.max_iterations;
+    fd.lm_grad_tol = bo.gradient_tol;
+    fd.lm_step_tol = bo.step_tol;
+    fd.lm_lambda0 = bo.initial_lambda;
+    fd.lm_min_lambda = bo.min_lambda;
+    fd.lm_max_lambda = bo.max_lambda;
+    fd.skip_refine = 0;
+    FrameResult r0;
+    std::memset(&r0, 0, sizeof(r0));
+    for (int k = 0; k < 4; ++k) r0.q[k] = q[k];
+    for (int k = 0; k < 3; ++k) r0.t[k] = t[k];
+    TBR_CUDA(cudaMemcpyAsync(E.P.frames + slots[0], &fd, sizeof(FrameDev), cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.P.results + slots[0], &r0, sizeof(FrameResult), cudaMemcpyHostToDevice, E.stream));
+    const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (n + 1023) / 1024));
+    k_prep_bounds<<<dim3(bx, 1), 256, 0, E.stream>>>(E.P);
+    k_lm_pack<<<bx, 256, 0, E.stream>>>(E.P);
+    k_lm<<<1, kLMThreads, 0, E.stream>>>(E.P);
+    st = TBR_OK;
+    if (cudaGetLastError() != cudaSuccess) st = fail(TBR_ERR_CUDA, "bundle_adjust launch failed");
+    FrameResult res;
+    if (!st) cudaMemcpyAsync(&res, E.P.results + slots[0], sizeof(FrameResult), cudaMemcpyDeviceToHost, E.stream);
+    if (cudaStreamSynchronize(E.stream) != cudaSuccess && !st) st = fail(TBR_ERR_CUDA, "bundle_adjust failed");
+    E.blocks.release(fd.blk_off, fd.n_blocks);
+    E.free_slots.push_back(slots[0]);
+    if (st) return st;
+    for (int k = 0; k < 4; ++k) q[k] = res.q[k];
+    for (int k = 0; k < 3; ++k) t[k] = res.t[k];
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->lm_iterations = res.lm_iters;
+        stats->lm_invalid_steps = res.lm_invalid;
+        stats->lm_initial_cost = res.lm_cost0;
+        stats->lm_cost = res.lm_cost;
+    }
+    return TBR_OK;
+}
+
+// Placeholders until the graph-captured batch handle and the serving loop land.
+tbr_status tbr_batch_create(tbr_context *, const tbr_frame_desc *, int32_t, const tbr_ransac_options *,
+                            const tbr_ext_options *, tbr_batch **) {
+    return fail(TBR_ERR_INTERNAL, "tbr_batch_create: not available in this build");
+}
+tbr_status tbr_batch_run(tbr_batch *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
+tbr_status tbr_batch_sync(tbr_batch *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
+tbr_status tbr_batch_results(tbr_batch *, tbr_frame_result *) {
+    return fail(TBR_ERR_INTERNAL, "not available in this build");
+}
+void tbr_batch_destroy(tbr_batch *) {}
+tbr_status tbr_server_create(tbr_context *, const tbr_server_config *, tbr_server **) {
+    return fail(TBR_ERR_INTERNAL, "tbr_server_create: not available in this build");
+}
+tbr_status tbr_server_submit(tbr_server *, const tbr_frame_desc *, uint64_t *) {
+    return fail(TBR_ERR_INTERNAL, "not available in this build");
+}
+tbr_status tbr_server_poll(tbr_server *, tbr_server_result *, int32_t, int32_t *) {
+    return fail(TBR_ERR_INTERNAL, "not available in this build");
+}
+tbr_status tbr_server_cancel(tbr_server *, uint64_t) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
+tbr_status tbr_server_drain(tbr_server *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
+void tbr_server_destroy(tbr_server *) {}
+
+tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, const double *points3D,
+                                   int64_t n, const double K[4], double max_reproj_error,
+                                   const int32_t *triples, int64_t n_samples, int64_t *ids, double *poses,
+                                   float *scores32, int64_t *counts, int64_t cap, int64_t *n_hyp) {
+    if (!ctx || !points2D || !points3D || !K || !triples || n < 3 || n_samples < 1)
+        return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    RunOptions o;
+    o.B = n_samples;
+    o.force_samples = n_samples;
+    o.skip_refine = 1;
+    FrameHost fh{points2D, points3D, n, {K[0], K[1], K[2], K[3]}, 0, max_reproj_error, triples, n_samples};
+    if (4 * n_samples > E.P.max_hyps) return fail(TBR_ERR_OOM, "too many samples for the hypothesis pool");
+    std::vector<int> slots;
+    int64_t max_n = 0;
+    TBR_CUDA(cudaSetDevice(E.device));
+    TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
+    tbr_status st = admit_frames(E, {fh}, o, slots, max_n);
+    if (st) return st;
+    E.launch_prep(1, max_n);
+    TBR_CUDA(cudaMemsetAsync(E.P.counters + kCStillRansac, 0, 16, E.stream));
+    k_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
+    k_sample_p3p<<<E.p3p_grid, 128, 0, E.stream>>>(E.P);
+    k_score_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
+    if (o.hr == 4) k_score<2><<<E.score_grid[0], kScoreWarps * 32, 0, E.stream>>>(E.P);
+    else k_score<4><<<E.score_grid[1], kScoreWarps * 32, 0, E.stream>>>(E.P);
+    if (counts) k_debug_counts<<<E.num_sms * 4, 256, 0, E.stream>>>(E.P);
+    TBR_CUDA(cudaGetLastError());
+    FrameDev fd;
+    TBR_CUDA(cudaMemcpyAsync(&fd, E.P.frames + slots[0], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    if (E.h_counters[kCError]) {
+        E.blocks.release(fd.blk_off, fd.n_blocks);
+        E.free_slots.push_back(slots[0]);
+        return fail(TBR_ERR_TIMEOUT, "device error flag set");
+    }
+    const int64_t nh = fd.hyp_count;
+    std::vector<int64_t> hid(nh);
+    std::vector<double> hp(12 * nh);
+    std::vector<float> hs(nh);
+    std::vector<int64_t> hc(nh);
+    TBR_CUDA(cudaMemcpy(hid.data(), E.P.hId + fd.hyp_base, 8 * nh, cudaMemcpyDeviceToHost));
+    TBR_CUDA(cudaMemcpy(hp.data(), E.P.hP64 + 12 * fd.hyp_base, 96 * nh, cudaMemcpyDeviceToHost));
+    TBR_CUDA(cudaMemcpy(hs.data(), E.P.hS32 + fd.hyp_base, 4 * nh, cudaMemcpyDeviceToHost));
+    if (counts) TBR_CUDA(cudaMemcpy(hc.data(), E.P.dbg_counts, 8 * nh, cudaMemcpyDeviceToHost));
+    E.blocks.release(fd.blk_off, fd.n_blocks);
+    E.free_slots.push_back(slots[0]);
+    // Sort by id (sample order, solution order).
+    std::vector<int64_t> order(nh);
+    for (int64_t i = 0; i < nh; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return hid[a] < hid[b]; });
+    const int64_t m = std::min(nh, cap);
+    for (int64_t k = 0; k < m; ++k) {
+        const int64_t i = order[k];
+        if (ids) ids[k] = hid[i];
+        if (poses) std::memcpy(poses + 12 * k, &hp[12 * i], 96);
+        if (scores32) scores32[k] = hs[i];
+        if (counts) counts[k] = hc[i];
+    }
+    if (n_hyp) *n_hyp = m;
+    return TBR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1364 @@
+// Kernels of one engine step (sm_100a). Host orchestration lives in tbr_engine.cu.
+//
+// A step advances every resident frame in the RANSAC state by a planned number
+// of rounds:
+//   k_plan          rounds to run this step per frame (adaptive-termination aware)
+//   k_sample_p3p    one thread per minimal sample: Philox triple (or replay), FP64 P3P
+//   k_score_plan    work items (frame, 32*HR hypotheses, point chunk)
+//   k_score         FP32 truncated-MSAC filter pass (the hot kernel)
+//   k_select        candidates within a safe band of each round's running minimum
+//   k_rescore_plan / k_rescore   exact FP64 MSAC of the candidates (reference formula)
+//   k_finalize      the reference's selection and stop rule, round by round
+// then, for frames whose RANSAC ended:
+//   k_inliers       get_inliers_mx semantics + ordered compaction of the inliers
+//   k_lm            Levenberg-Marquardt, FP32 compensated J^T J / J^T r, FP64 solve
+#pragma once
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+
+#include "tbr_device.cuh"
+
+namespace tbr {
+
+constexpr int kSub = 64;                          // points per FP32 staging block
+constexpr int kBlockFloat2 = kSub * 5;            // float2 entries per block
+constexpr uint32_t kBlockBytes = kBlockFloat2 * 8;  // 2560 B per block
+constexpr int kMaxRoundsPerStep = 128;
+constexpr int kMaxCand = 64;                      // FP64 re-rank candidates per frame and step
+constexpr int kMaxRChunks = 64;                   // FP64 rescoring point chunks per frame
+constexpr int kMaxScoreChunks = 32;               // FP32 scoring point chunks per frame
+constexpr int kMaxActive = 1024;                  // frames advanced by one step
+constexpr uint32_t kMaxPolls = 1u << 26;          // bounded mbarrier waits (~seconds)
+constexpr int kScoreWarps = 4;                    // warps per scoring CTA
+constexpr int kLMThreads = 256;
+
+enum FrameStatus : int32_t { kFree = 0, kRansac = 1, kLMPending = 2, kDone = 3, kFailed = 4 };
+
+enum Counter : int {
+    kCScoreNext = 0,
+    kCScoreTotal,
+    kCRescoreNext,
+    kCRescoreTotal,
+    kCSamplesTotal,
+    kCError,
+    kCStillRansac,
+    kCLMPending,
+    kCWorkPairs,
+    kCNum
+};
+
+enum ErrorBits : unsigned long long { kErrTimeout = 1ull, kErrOverflow = 2ull };
+
+struct FrameResult {
+    double q[4];
+    double t[3];
+    int64_t samples, rounds, hypotheses, ransac_inliers, num_inliers;
+    double model_score;
+    int64_t best_sample;
+    int32_t best_sol, steps;
+    int64_t rescored;
+    int32_t overflow, lm_iters, lm_invalid, status;
+    double lm_cost0, lm_cost;
+};
+
+struct FrameDev {
+    // ---- inputs, fixed at admission ----
+    int64_t n;
+    int64_t blk_off;  // first staging block; the frame's points start at blk_off * kSub
+    int32_t n_blocks;
+    int32_t status;
+    uint64_t seed;
+    const int32_t *replay;  // device triples or nullptr
+    int64_t replay_count;
+    double K[4];
+    double focal, tau, sq_thr;
+    double centre[3];
+    unsigned long long bmin[3], bmax[3];
+    int64_t B;
+    int64_t max_total;
+    int64_t force_samples;
+    double log_missing, trials_mult;
+    int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass
+    int64_t lm_max_iter;
+    double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
+    double lm_inv_sq_thr, lm_grad_tol, lm_step_tol, lm_lambda0, lm_min_lambda, lm_max_lambda;
+    int32_t chunk_points, pad0;
+    // ---- RANSAC progress ----
+    int64_t samples_done, rounds_done, hyps_done;
+    int32_t steps, found;
+    double best_score;
+    int64_t best_count, best_sample;
+    int32_t best_sol, overflow;
+    double best_P[12];
+    int64_t rescored;
+    // ---- current step ----
+    int64_t step_first, step_samples, step_rounds, step_div;
+    int64_t hyp_base;
+    int32_t hyp_count, n_hblocks;
+    int32_t n_chunks, chunk_blocks;
+    int64_t part_base, hb_base;
+    int32_t cand_count, n_rchunks;
+    int64_t rchunk;
+    unsigned long long round_min[kMaxRoundsPerStep];
+    int32_t round_hyps[kMaxRoundsPerStep];
+    // ---- LM ----
+    int64_t num_inliers;
+};
+
+struct Pools {
+    FrameDev *frames;
+    FrameResult *results;
+    const int32_t *active;  // slots advanced by this launch
+    int32_t n_active;
+    int32_t num_sms;
+    // per point (blocks * kSub entries)
+    const double *uv64;  // raw pixels (2/pt)
+    const double *X64;   // world points (3/pt)
+    double *xn64;        // normalized image points (2/pt)
+    uint8_t *mask;       // final inlier mask (1/pt)
+    double *lx64;        // LM: pixels / f (2/pt)
+    double *lX64;        // LM: world points (3/pt)
+    float4 *lA32;        // LM: (Xc, Yc, Zc, u/f) centred, FP32
+    float4 *lB32;        // LM: (X, Y, Z, v/f) world, FP32
+    float2 *pts32;       // staging blocks: [X|Y|Z|-x/tau|-y/tau] x kSub, each value duplicated
+    // step prefixes (n_active + 1)
+    int64_t *sample_prefix;
+    int64_t *item_prefix;
+    int64_t *ritem_prefix;
+    // hypotheses
+    double *hP64;
+    float *hP32;
+    int64_t *hId;
+    float *hS32;
+    float *part;
+    unsigned *hb_arrive;
+    int64_t max_hyps, max_parts, max_hb;
+    // candidates (frame slot * kMaxCand)
+    int32_t *cHyp;
+    double *cS64;
+    int64_t *cCnt;
+    double *cpS;  // (slot * kMaxCand + c) * kMaxRChunks + chunk
+    int32_t *cpC;
+    unsigned *c_arrive;
+    unsigned long long *counters;
+    // debug: per-hypothesis counts (tbr_debug_score_samples)
+    int64_t *dbg_counts;
+};
+
+// ------------------------------------------------------------- helpers -----
+__device__ __forceinline__ int64_t needed_samples(int64_t inliers, int64_t n, double log_missing,
+                                                  double mult) {
+    // turbo_ransac.cu:223-231; the int conversion behaves like x86 cvttsd2si:
+    // NaN and out-of-range values give INT_MIN, which ends the round loop.
+    const double w = (double)inliers / (double)n;
+    const double prob_outlier = 1.0 - pow(w, 3.0);
+    const double v = ceil(log_missing / log(prob_outlier) * mult);
+    if (!(v >= -2147483648.0 && v < 2147483648.0)) return (int64_t)INT_MIN;
+    return (int64_t)(int)v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide exclusive scan over blockDim.x <= 1024 values; returns the
+// exclusive prefix, writes the total. Uses 33 int64 of shared scratch.
+__device__ __forceinline__ int64_t block_exclusive_scan(int64_t v, int64_t *sh, int64_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    int64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) sh[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int64_t w = lane < nw ? sh[lane] : 0;
+        int64_t wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
+        }
+        if (lane < nw) sh[lane] = wi - w;
+        if (lane == nw - 1) sh[32] = wi;
+    }
+    __syncthreads();
+    const int64_t r = sh[warp] + incl - v;
+    total = sh[32];
+    __syncthreads();
+    return r;
+}
+
+__device__ __forceinline__ int find_segment(const int64_t *prefix, int n, int64_t g) {
+    int lo = 0, hi = n - 1;  // largest i with prefix[i] <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void flag_error(const Pools &P, unsigned long long bits) {
+    atomicOr(&P.counters[kCError], bits);
+}
+
+// ----------------------------------------------------------- admission -----
+// AABB of the frame's world points (ordered-integer atomics: order independent).
+__global__ void k_prep_bounds(Pools P) {
+    const int a = blockIdx.y;
+    if (a >= P.n_active) return;
+    FrameDev &f = P.frames[P.active[a]];
+    const int64_t base = f.blk_off * kSub;
+    double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < f.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double v = P.X64[3 * (base + i) + k];
+            lo[k] = fmin(lo[k], v);
+            hi[k] = fmax(hi[k], v);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fmin(lo[k], __shfl_down_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmax(hi[k], __shfl_down_sync(0xffffffffu, hi[k], o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&f.bmin[k], dbl_to_ordered(lo[k]));
+            atomicMax(&f.bmax[k], dbl_to_ordered(hi[k]));
+        }
+    }
+}
+
+// Normalized coordinates (Camera_cuda::unproject, camera.cuh:51-62) and the FP32
+// staging blocks: centred world points and -x/tau, -y/tau, each duplicated so
+// that one 64-bit lane pair feeds both halves of a packed FP32x2 instruction.
+__global__ void k_prep_pack(Pools P) {
+    const int a = blockIdx.y;
+    if (a >= P.n_active) return;
+    FrameDev &f = P.frames[P.active[a]];
+    const int64_t base = f.blk_off * kSub;
+    const double c0 = 0.5 * (ordered_to_dbl(f.bmin[0]) + ordered_to_dbl(f.bmax[0]));
+    const double c1 = 0.5 * (ordered_to_dbl(f.bmin[1]) + ordered_to_dbl(f.bmax[1]));
+    const double c2 = 0.5 * (ordered_to_dbl(f.bmin[2]) + ordered_to_dbl(f.bmax[2]));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        f.centre[0] = c0;
+        f.centre[1] = c1;
+        f.centre[2] = c2;
+    }
+    const double fx = f.K[0], fy = f.K[1], cx = f.K[2], cy = f.K[3];
+    const double itau = 1.0 / f.tau;
+    const int64_t npad = (int64_t)f.n_blocks * kSub;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npad;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        float v[5];
+        if (i < f.n) {
+            const double u = P.uv64[2 * (base + i)], w = P.uv64[2 * (base + i) + 1];
+            const double xn = (u - cx) / fx, yn = (w - cy) / fy;
+            P.xn64[2 * (base + i)] = xn;
+            P.xn64[2 * (base + i) + 1] = yn;
+            v[0] = (float)(P.X64[3 * (base + i)] - c0);
+            v[1] = (float)(P.X64[3 * (base + i) + 1] - c1);
+            v[2] = (float)(P.X64[3 * (base + i) + 2] - c2);
+            v[3] = (float)(-xn * itau);
+            v[4] = (float)(-yn * itau);
+        } else {
+            v[0] = v[1] = v[2] = v[3] = v[4] = 0.0f;
+        }
+        float2 *blk = P.pts32 + (f.blk_off + i / kSub) * kBlockFloat2;
+        const int j = (int)(i % kSub);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) blk[k * kSub + j] = make_float2(v[k], v[k]);
+    }
+}
+
+// ---------------------------------------------------------------- plan -----
+// Rounds per frame for this step. The first step runs one round; later steps
+// run exactly the rounds the current best's inlier ratio still requires under
+// the reference's stop rule (turbo_ransac.cu:223-257), so a frame normally
+// finishes in one or two steps while its samples, selection and stop point are
+// those of the sequential round loop. Hypothesis-pool capacity is shared in
+// frame order; a frame that does not fit waits for the next step.
+__global__ void k_plan(Pools P) {
+    __shared__ int64_t sh[33];
+    const int a = threadIdx.x;
+    int64_t samples = 0, rounds = 0, div = 0;
+    FrameDev *f = nullptr;
+    if (a < P.n_active) {
+        f = &P.frames[P.active[a]];
+        f->step_samples = 0;
+        f->step_rounds = 0;
+        f->hyp_count = 0;
+        f->cand_count = 0;
+        if (f->status == kRansac) {
+            if (f->force_samples > 0) {
+                samples = f->force_samples - f->samples_done;
+                rounds = 1;
+                div = f->force_samples;
+            } else {
+                const int64_t max_rounds = (f->max_total + f->B - 1) / f->B;
+                int64_t r = 1;
+                if (f->rounds_done > 0) {
+                    const int64_t need = needed_samples(f->found ? f->best_count : 0, f->n,
+                                                        f->log_missing, f->trials_mult);
+                    r = need / f->B + 1 - f->rounds_done;
+                    if (need < 0 || r < 1) r = 1;
+                }
+                r = min(r, max_rounds - f->rounds_done);
+                r = min(r, (int64_t)kMaxRoundsPerStep);
+                if (r < 1) r = 1;
+                rounds = r;
+                samples = r * f->B;
+                div = f->B;
+            }
+        }
+    }
+    // Capacity: 4 hypotheses per sample at most.
+    int64_t total;
+    int64_t excl = block_exclusive_scan(4 * samples, sh, total);
+    if (f && samples > 0 && excl + 4 * samples > P.max_hyps) {
+        const int64_t room = P.max_hyps - excl;
+        if (room <= 0) {
+            samples = rounds = 0;
+        } else if (f->force_samples > 0) {
+            samples = room / 4;
+        } else {
+            rounds = room / (4 * f->B);
+            samples = rounds * f->B;
+        }
+    }
+    const int64_t hyp_excl = block_exclusive_scan(4 * samples, sh, total);
+    const int64_t s_excl = block_exclusive_scan(samples, sh, total);
+    if (f) {
+        f->step_first = f->samples_done;
+        f->step_samples = samples;
+        f->step_rounds = samples > 0 ? rounds : 0;
+        f->step_div = div;
+        f->hyp_base = hyp_excl;
+        P.sample_prefix[a] = s_excl;
+    }
+    if (a == 0) {
+        P.sample_prefix[P.n_active] = total;
+        P.counters[kCSamplesTotal] = (unsigned long long)total;
+        P.counters[kCScoreNext] = 0;
+        P.counters[kCRescoreNext] = 0;
+    }
+}
+
+// -------------------------------------------------------- sample + P3P -----
+// One thread per minimal sample (replaces thread 0 of a 384-thread block in
+// ransac.cuh:176-217). Solutions are appended to the frame's hypothesis region
+// with one atomic per frame per warp; each carries id = sample*4 + solution,
+// so ordering never depends on scheduling.
+__global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
+    const int64_t total = (int64_t)P.counters[kCSamplesTotal];
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < total; g0 += stride) {
+        const int64_t g = g0 + threadIdx.x;
+        const bool valid = g < total;
+        int a = -1;
+        int nsol = 0;
+        double sols[48];
+        if (valid) {
+            a = find_segment(P.sample_prefix, P.n_active, g);
+            const FrameDev &f = P.frames[P.active[a]];
+            const int64_t s = f.step_first + (g - P.sample_prefix[a]);
+            int32_t idx[3];
+            if (f.replay) {
+                idx[0] = f.replay[3 * s];
+                idx[1] = f.replay[3 * s + 1];
+                idx[2] = f.replay[3 * s + 2];
+            } else {
+                draw_triple(f.seed, (uint64_t)s, (uint32_t)f.n, idx);
+            }
+            const int64_t base = f.blk_off * kSub;
+            d3 xb[3], Xs[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int64_t p = base + idx[k];
+                xb[k] = bearing(P.xn64[2 * p], P.xn64[2 * p + 1]);
+                Xs[k] = {P.X64[3 * p], P.X64[3 * p + 1], P.X64[3 * p + 2]};
+            }
+            nsol = p3p_solve(xb, Xs, sols);
+        }
+        // Warp-aggregated reservation; a warp's samples are contiguous in g, so
+        // lanes of one frame form one contiguous run.
+        const unsigned act = __activemask();
+        const unsigned grp = __match_any_sync(act, a);
+        int incl = nsol;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(act, incl, o);
+            if (lane >= o) incl += u;
+        }
+        const int first = __ffs(grp) - 1, last = 31 - __clz(grp);
+        const int before = __shfl_sync(act, incl - nsol, first);
+        const int grp_total = __shfl_sync(act, incl, last) - before;
+        int slot0 = 0;
+        if (lane == first && a >= 0 && grp_total > 0)
+            slot0 = atomicAdd(&P.frames[P.active[a]].hyp_count, grp_total);
+        slot0 = __shfl_sync(act, slot0, first);
+        if (valid && nsol > 0) {
+            const FrameDev &f = P.frames[P.active[a]];
+            const int64_t s = f.step_first + (g - P.sample_prefix[a]);
+            const int64_t h0 = f.hyp_base + slot0 + (incl - nsol - before);
+            const double itau = 1.0 / f.tau;
+            for (int k = 0; k < nsol; ++k) {
+                const double *S = sols + 12 * k;
+                const int64_t h = h0 + k;
+#pragma unroll
+                for (int e = 0; e < 12; ++e) P.hP64[12 * h + e] = S[e];
+                P.hId[h] = s * 4 + k;
+                // Scoring form: rows 0, 1 scaled by 1/tau, translation moved to the
+                // centred frame (t + R c), all in FP64 before the FP32 rounding.
+                float *Q = P.hP32 + 12 * h;
+#pragma unroll
+                for (int r = 0; r < 3; ++r) {
+                    const double tc = S[4 * r + 3] + S[4 * r] * f.centre[0] + S[4 * r + 1] * f.centre[1] +
+                                      S[4 * r + 2] * f.centre[2];
+                    const double sc = r < 2 ? itau : 1.0;
+                    Q[4 * r] = (float)(S[4 * r] * sc);
+                    Q[4 * r + 1] = (float)(S[4 * r + 1] * sc);
+                    Q[4 * r + 2] = (float)(S[4 * r + 2] * sc);
+                    Q[4 * r + 3] = (float)(tc * sc);
+                }
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------ scoring -----
+// Work items: (frame, block of 32*HR hypotheses, point chunk). Chunks are sized
+// so that the step has enough items to keep every SM busy.
+__global__ void k_score_plan(Pools P) {
+    __shared__ int64_t sh[33];
+    __shared__ unsigned long long pairs_total;
+    const int a = threadIdx.x;
+    FrameDev *f = a < P.n_active ? &P.frames[P.active[a]] : nullptr;
+    const bool act = f && f->step_samples > 0;
+    if (a == 0) pairs_total = 0;
+    __syncthreads();
+    if (act) atomicAdd(&pairs_total, (unsigned long long)f->hyp_count * (unsigned long long)f->n);
+    __syncthreads();
+    int64_t items = 0, parts = 0, hbs = 0;
+    if (act) {
+        const int HB = 32 * f->hr;
+        const int nhb = (f->hyp_count + HB - 1) / HB;
+        // Target about 8 items per warp slot of the GPU, at least 4 blocks per item.
+        const double target_items = 8.0 * P.num_sms * 16;
+        const double pairs_per_item = fmax((double)pairs_total / target_items, 4.0 * kSub * HB);
+        int cb = (int)ceil(pairs_per_item / ((double)HB * kSub));
+        if (f->chunk_points > 0) cb = max(1, f->chunk_points / kSub);
+        cb = max(cb, (f->n_blocks + kMaxScoreChunks - 1) / kMaxScoreChunks);
+        cb = max(1, min(cb, f->n_blocks));
+        const int nch = (f->n_blocks + cb - 1) / cb;
+        f->n_hblocks = nhb;
+        f->chunk_blocks = cb;
+        f->n_chunks = nch;
+        items = (int64_t)nhb * nch;
+        parts = (int64_t)f->hyp_count * nch;
+        hbs = nhb;
+#pragma unroll 1
+        for (int r = 0; r < kMaxRoundsPerStep; ++r) f->round_min[r] = ~0ull;
+    }
+    int64_t tot;
+    const int64_t iexcl = block_exclusive_scan(items, sh, tot);
+    if (a < P.n_active) P.item_prefix[a] = iexcl;
+    if (a == 0) {
+        P.item_prefix[P.n_active] = tot;
+        P.counters[kCScoreTotal] = (unsigned long long)tot;
+        P.counters[kCWorkPairs] = pairs_total;
+    }
+    const int64_t pexcl = block_exclusive_scan(parts, sh, tot);
+    if (act) f->part_base = pexcl;
+    if (a == 0 && tot > P.max_parts) flag_error(P, kErrOverflow);
+    const int64_t hexcl = block_exclusive_scan(hbs, sh, tot);
+    if (act) {
+        f->hb_base = hexcl;
+        for (int i = 0; i < hbs; ++i) P.hb_arrive[hexcl + i] = 0;
+    }
+    if (a == 0 && tot > P.max_hb) flag_error(P, kErrOverflow);
+}
+
+// One (hypothesis pair, point) update: returns nothing, accumulates
+// min(r^2 / tau^2, 1) into both halves of acc, counting a point with
+// non-positive depth as an outlier (msac.cuh:46 semantics). Division-free
+// sign test: the reciprocal of the depth carries its sign into the squared
+// residual's sign bit, and an unsigned min against 1.0f clamps NaN, +inf,
+// and any negative-signed value to 1.
+__device__ __forceinline__ void msac_pair(const uint64_t (&p)[12], uint64_t X, uint64_t Y, uint64_t Z,
+                                          uint64_t NX, uint64_t NY, uint64_t &acc) {
+    const uint64_t z0 = f2fma(p[0], X, f2fma(p[1], Y, f2fma(p[2], Z, p[3])));
+    const uint64_t z1 = f2fma(p[4], X, f2fma(p[5], Y, f2fma(p[6], Z, p[7])));
+    const uint64_t z2 = f2fma(p[8], X, f2fma(p[9], Y, f2fma(p[10], Z, p[11])));
+    float za, zb;
+    f2unpack(z2, za, zb);
+    const float ia = rcp_approx(za), ib = rcp_approx(zb);
+    const uint64_t inv = f2pack(ia, ib);
+    const uint64_t r0 = f2fma(z0, inv, NX);
+    const uint64_t r1 = f2fma(z1, inv, NY);
+    const uint64_t q = f2fma(r0, r0, f2mul(r1, r1));
+    float qa, qb;
+    f2unpack(q, qa, qb);
+    const uint32_t ca = min(__float_as_uint(qa) | (__float_as_uint(ia) & 0x80000000u), 0x3f800000u);
+    const uint32_t cb = min(__float_as_uint(qb) | (__float_as_uint(ib) & 0x80000000u), 0x3f800000u);
+    acc = f2add(acc, f2pack(__uint_as_float(ca), __uint_as_float(cb)));
+}
+
+// One staging block (kSub points) against the lane's HP hypothesis pairs.
+template <int HP>
+__device__ __forceinline__ void score_block(const float2 *blk, int valid, const uint64_t (&c)[HP][12],
+                                            uint64_t (&acc)[HP]) {
+    const ulonglong2 *sX = reinterpret_cast<const ulonglong2 *>(blk);
+    const ulonglong2 *sY = sX + kSub / 2;
+    const ulonglong2 *sZ = sY + kSub / 2;
+    const ulonglong2 *sNX = sZ + kSub / 2;
+    const ulonglong2 *sNY = sNX + kSub / 2;
+    if (valid == kSub) {
+#pragma unroll 2
+        for (int j = 0; j < kSub / 2; ++j) {
+            const ulonglong2 X = sX[j], Y = sY[j], Z = sZ[j], NX = sNX[j], NY = sNY[j];
+#pragma unroll
+            for (int h = 0; h < HP; ++h) {
+                msac_pair(c[h], X.x, Y.x, Z.x, NX.x, NY.x, acc[h]);
+                msac_pair(c[h], X.y, Y.y, Z.y, NX.y, NY.y, acc[h]);
+            }
+        }
+    } else {
+        for (int j = 0; j < valid; ++j) {
+            const uint64_t *u = reinterpret_cast<const uint64_t *>(blk);
+            const uint64_t X = u[j], Y = u[kSub + j], Z = u[2 * kSub + j], NX = u[3 * kSub + j],
+                           NY = u[4 * kSub + j];
+#pragma unroll
+            for (int h = 0; h < HP; ++h) msac_pair(c[h], X, Y, Z, NX, NY, acc[h]);
+        }
+    }
+}
+
+// The FP32 filter pass. Persistent: each warp repeatedly takes a work item,
+// streams its point chunk through a private two-stage shared-memory pipeline
+// fed by 1-D bulk copies (TMA engine, mbarrier completion), and accumulates
+// per-hypothesis truncated-MSAC costs for 32*HR hypotheses held in registers
+// as packed FP32x2 pairs. The warp that completes the last chunk of a
+// hypothesis block sums the chunk partials in fixed order and publishes the
+// per-round minimum as a packed (score, index) key.
+template <int HP>
+__global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
+    __shared__ __align__(128) float2 stage[kScoreWarps][2][kBlockFloat2];
+    __shared__ __align__(8) uint64_t bars[kScoreWarps][2];
+    constexpr int HR = 2 * HP;
+    constexpr int HB = 32 * HR;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint64_t *bar = bars[w];
+    float2 *st0 = stage[w][0], *st1 = stage[w][1];
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+    uint32_t phase0 = 0, phase1 = 0;
+    const int64_t total = (int64_t)P.counters[kCScoreTotal];
+    for (;;) {
+        int64_t item = 0;
+        if (lane == 0) item = (int64_t)atomicAdd(&P.counters[kCScoreNext], 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= total) break;
+        const int a = find_segment(P.item_prefix, P.n_active, item);
+        FrameDev &f = P.frames[P.active[a]];
+        const int64_t local = item - P.item_prefix[a];
+        const int nch = f.n_chunks;
+        const int hb = (int)(local / nch), ch = (int)(local % nch);
+        const int nh = f.hyp_count;
+        const int64_t hbase = f.hyp_base;
+        // Hypotheses: lane owns HR consecutive ones.
+        uint64_t c[HP][12];
+        uint64_t acc[HP];
+#pragma unroll
+        for (int h = 0; h < HP; ++h) {
+            const int i0 = hb * HB + lane * HR + 2 * h, i1 = i0 + 1;
+            const float *A = P.hP32 + 12 * (hbase + i0), *Bp = P.hP32 + 12 * (hbase + i1);
+#pragma unroll
+            for (int e = 0; e < 12; ++e)
+                c[h][e] = f2pack(i0 < nh ? __ldg(A + e) : 0.0f, i1 < nh ? __ldg(Bp + e) : 0.0f);
+            acc[h] = 0ull;
+        }
+        const int b0 = ch * f.chunk_blocks;
+        const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
+        const int nb = b1 - b0;
+        const float2 *g = P.pts32 + (f.blk_off + b0) * kBlockFloat2;
+        if (lane == 0) {
+            fence_proxy_async();
+            bulk_load(st0, g, kBlockBytes, &bar[0]);
+            if (nb > 1) bulk_load(st1, g + kBlockFloat2, kBlockBytes, &bar[1]);
+        }
+        bool ok = true;
+        for (int i = 0; i < nb; ++i) {
+            const int s = i & 1;
+            const uint32_t ph = s ? phase1 : phase0;
+            if (!mbar_wait(&bar[s], ph, kMaxPolls)) {
+                ok = false;
+                break;
+            }
+            if (s) phase1 ^= 1u; else phase0 ^= 1u;
+            const int64_t pt0 = (int64_t)(b0 + i) * kSub;
+            const int valid = (int)(f.n - pt0 < kSub ? f.n - pt0 : kSub);
+            score_block<HP>(s ? st1 : st0, valid, c, acc);
+            __syncwarp();
+            if (lane == 0 && i + 2 < nb) {
+                fence_proxy_async();
+                bulk_load(s ? st1 : st0, g + (int64_t)(i + 2) * kBlockFloat2, kBlockBytes, &bar[s]);
+            }
+        }
+        if (!ok) {
+            // Give up: record it, let any copy still in flight land, and leave.
+            if (lane == 0) flag_error(P, kErrTimeout);
+            mbar_wait(&bar[0], phase0, kMaxPolls);
+            mbar_wait(&bar[1], phase1, kMaxPolls);
+            return;
+        }
+        // Chunk partials.
+        float *part = P.part + f.part_base;
+#pragma unroll
+        for (int h = 0; h < HP; ++h) {
+            float lo, hi;
+            f2unpack(acc[h], lo, hi);
+            const int i0 = hb * HB + lane * HR + 2 * h;
+            if (i0 < nh) part[(int64_t)i0 * nch + ch] = lo;
+            if (i0 + 1 < nh) part[(int64_t)(i0 + 1) * nch + ch] = hi;
+        }
+        __threadfence();
+        __syncwarp();
+        unsigned prev = 0;
+        if (lane == 0) prev = atomicAdd(&P.hb_arrive[f.hb_base + hb], 1u);
+        prev = __shfl_sync(0xffffffffu, prev, 0);
+        if (prev == (unsigned)(nch - 1)) {
+            __threadfence();
+            for (int k = 0; k < HR; ++k) {
+                const int i = hb * HB + lane * HR + k;
+                if (i >= nh) break;
+                float s = 0.0f;
+                for (int q = 0; q < nch; ++q) s += __ldcg(part + (int64_t)i * nch + q);
+                P.hS32[hbase + i] = s;
+                const int64_t sample = P.hId[hbase + i] >> 2;
+                const int64_t r = (sample - f.step_first) / f.step_div;
+                const unsigned long long key =
+                    ((unsigned long long)__float_as_uint(s) << 32) | (unsigned)i;
+                atomicMin(&f.round_min[r], key);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------- candidates -----
+// Candidates for the exact FP64 re-rank: every hypothesis whose FP32 score is
+// within a band of the running minimum (over this step's rounds so far and the
+// best of earlier steps). The band, 2^-12 of the score plus one tau^2, is
+// far wider than the FP32-vs-FP64 score difference, so the FP64 best of every
+// round that can change the running best is always among the candidates. If
+// more than kMaxCand qualify the band is halved (up to 7 times) before the
+// overflow flag is raised.
+__global__ void k_select(Pools P) {
+    __shared__ float thr[kMaxRoundsPerStep];
+    __shared__ int rh[kMaxRoundsPerStep];
+    __shared__ int cnt[8];
+    __shared__ int level;
+    const int slot = P.active[blockIdx.x];
+    FrameDev &f = P.frames[slot];
+    if (f.status != kRansac || f.step_samples == 0) return;
+    const int R = (int)f.step_rounds;
+    if (threadIdx.x == 0) {
+        float pm = f.found ? (float)(f.best_score / f.sq_thr) : __int_as_float(0x7f800000);
+        for (int r = 0; r < R; ++r) {
+            const unsigned long long k = f.round_min[r];
+            const float rm = k == ~0ull ? __int_as_float(0x7f800000) : __uint_as_float((unsigned)(k >> 32));
+            pm = fminf(pm, rm);
+            thr[r] = pm;
+        }
+    }
+    if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
+    for (int r = threadIdx.x; r < kMaxRoundsPerStep; r += blockDim.x) rh[r] = 0;
+    __syncthreads();
+    const int nh = f.hyp_count;
+    const int64_t hb = f.hyp_base;
+    int my[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) {
+        const float s = P.hS32[hb + i];
+        const int64_t r = ((P.hId[hb + i] >> 2) - f.step_first) / f.step_div;
+        const float pm = thr[r];
+        const float band = pm * (1.0f / 4096.0f) + 1.0f;
+        atomicAdd(&rh[r], 1);
+#pragma unroll
+        for (int l = 0; l < 8; ++l) my[l] += (s <= pm + band * (1.0f / (float)(1 << l))) ? 1 : 0;
+    }
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const int v = warp_sum(my[l]);
+        if ((threadIdx.x & 31) == 0) atomicAdd(&cnt[l], v);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < kMaxRoundsPerStep; r += blockDim.x) f.round_hyps[r] = rh[r];
+    if (threadIdx.x == 0) {
+        int lv = 7;
+        for (int l = 0; l < 8; ++l)
+            if (cnt[l] <= kMaxCand) { lv = l; break; }
+        level = lv;
+        f.overflow |= (cnt[7] > kMaxCand) ? 1 : 0;
+        f.cand_count = 0;
+    }
+    __syncthreads();
+    const float scale = 1.0f / (float)(1 << level);
+    for (int i = threadIdx.x; i < nh; i += blockDim.x) {
+        const float s = P.hS32[hb + i];
+        const int64_t r = ((P.hId[hb + i] >> 2) - f.step_first) / f.step_div;
+        const float pm = thr[r];
+        const float band = pm * (1.0f / 4096.0f) + 1.0f;
+        if (s <= pm + band * scale) {
+            const int c = atomicAdd(&f.cand_count, 1);
+            if (c < kMaxCand) P.cHyp[slot * kMaxCand + c] = i;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && f.cand_count > kMaxCand) f.cand_count = kMaxCand;
+}
+
+__global__ void k_rescore_plan(Pools P) {
+    __shared__ int64_t sh[33];
+    const int a = threadIdx.x;
+    int64_t items = 0;
+    if (a < P.n_active) {
+        const int slot = P.active[a];
+        FrameDev &f = P.frames[slot];
+        if (f.status == kRansac && f.step_samples > 0) {
+            const int nrc = (int)((f.n + 2047) / 2048 < kMaxRChunks ? (f.n + 2047) / 2048 : kMaxRChunks);
+            f.n_rchunks = nrc;
+            f.rchunk = (f.n + nrc - 1) / nrc;
+            items = (int64_t)f.cand_count * nrc;
+            for (int c = 0; c < f.cand_count; ++c) P.c_arrive[slot * kMaxCand + c] = 0;
+        }
+    }
+    int64_t tot;
+    const int64_t ex = block_exclusive_scan(items, sh, tot);
+    if (a < P.n_active) P.ritem_prefix[a] = ex;
+    if (a == 0) {
+        P.ritem_prefix[P.n_active] = tot;
+        P.counters[kCRescoreTotal] = (unsigned long long)tot;
+    }
+}
+
+// Exact FP64 truncated MSAC of one candidate over one point chunk, with the
+// per-point formula of msac.cuh:18-56 (reciprocal of the depth, then
+// products); the last chunk to finish sums the partials in chunk order and adds
+// (n - count) * tau^2 (ransac.cuh:322).
+__global__ void __launch_bounds__(256) k_rescore(Pools P) {
+    __shared__ double ss[8];
+    __shared__ int sc[8];
+    __shared__ int64_t s_item;
+    __shared__ unsigned s_prev;
+    const int64_t total = (int64_t)P.counters[kCRescoreTotal];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(&P.counters[kCRescoreNext], 1ull);
+        __syncthreads();
+        const int64_t item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        const int a = find_segment(P.ritem_prefix, P.n_active, item);
+        const int slot = P.active[a];
+        const FrameDev &f = P.frames[slot];
+        const int64_t local = item - P.ritem_prefix[a];
+        const int ci = (int)(local / f.n_rchunks), ch = (int)(local % f.n_rchunks);
+        const int h = P.cHyp[slot * kMaxCand + ci];
+        const double *Pp = P.hP64 + 12 * (f.hyp_base + h);
+        double M[12];
+#pragma unroll
+        for (int e = 0; e < 12; ++e) M[e] = Pp[e];
+        const int64_t base = f.blk_off * kSub;
+        const int64_t p0 = (int64_t)ch * f.rchunk, p1 = (f.n < p0 + f.rchunk ? f.n : p0 + f.rchunk);
+        double s = 0.0;
+        int cnt = 0;
+        const double sq = f.sq_thr;
+        for (int64_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+            const int64_t p = base + i;
+            const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
+            const double z0 = M[0] * X0 + M[1] * X1 + M[2] * X2 + M[3];
+            const double z1 = M[4] * X0 + M[5] * X1 + M[6] * X2 + M[7];
+            const double z2 = M[8] * X0 + M[9] * X1 + M[10] * X2 + M[11];
+            const double inv_z2 = 1.0 / z2;
+            const double r0 = z0 * inv_z2 - P.xn64[2 * p];
+            const double r1 = z1 * inv_z2 - P.xn64[2 * p + 1];
+            const double r_sq = r0 * r0 + r1 * r1;
+            if (r_sq < sq && z2 > 0.0) {
+                s += r_sq;
+                ++cnt;
+            }
+        }
+        s = warp_sum(s);
+        cnt = warp_sum(cnt);
+        if ((threadIdx.x & 31) == 0) {
+            ss[threadIdx.x >> 5] = s;
+            sc[threadIdx.x >> 5] = cnt;
+        }
+        __syncthreads();
+        const int cs = slot * kMaxCand + ci;
+        if (threadIdx.x == 0) {
+            double S = 0.0;
+            int C = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+                S += ss[k];
+                C += sc[k];
+            }
+            P.cpS[(int64_t)cs * kMaxRChunks + ch] = S;
+            P.cpC[(int64_t)cs * kMaxRChunks + ch] = C;
+            __threadfence();
+            s_prev = atomicAdd(&P.c_arrive[cs], 1u);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && s_prev == (unsigned)(f.n_rchunks - 1)) {
+            __threadfence();
+            double S = 0.0;
+            int64_t C = 0;
+            for (int q = 0; q < f.n_rchunks; ++q) {
+                S += __ldcg(P.cpS + (int64_t)cs * kMaxRChunks + q);
+                C += __ldcg(P.cpC + (int64_t)cs * kMaxRChunks + q);
+            }
+            P.cS64[cs] = S + (double)(f.n - C) * sq;
+            P.cCnt[cs] = C;
+        }
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------ finalize -----
+// The reference's per-round bookkeeping (turbo_ransac.cu:176-257 with the
+// merge/argmin kernels ransac.cuh:41-137), replayed in round order on the
+// exact FP64 scores: a round's best (lowest score, then lowest sample and
+// solution) replaces the running best only if strictly better; after each
+// round the stop rule uses the running best's inlier count.
+__global__ void k_finalize(Pools P) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= P.n_active) return;
+    const int slot = P.active[a];
+    FrameDev &f = P.frames[slot];
+    if (f.status != kRansac) return;
+    if (f.step_samples == 0) {  // waiting for hypothesis capacity
+        atomicAdd(&P.counters[kCStillRansac], 1ull);
+        return;
+    }
+    const int C = f.cand_count;
+    int order[kMaxCand];
+    for (int i = 0; i < C; ++i) order[i] = i;
+    // Insertion sort by hypothesis id = sample*4 + solution (rounds ascending).
+    for (int i = 1; i < C; ++i) {
+        const int v = order[i];
+        const int64_t key = P.hId[f.hyp_base + P.cHyp[slot * kMaxCand + v]];
+        int j = i - 1;
+        while (j >= 0 && P.hId[f.hyp_base + P.cHyp[slot * kMaxCand + order[j]]] > key) {
+            order[j + 1] = order[j];
+            --j;
+        }
+        order[j + 1] = v;
+    }
+    f.rescored += C;
+    const bool forced = f.force_samples > 0;
+    int ci = 0;
+    bool stop = false;
+    int64_t r_end = f.step_rounds;
+    for (int64_t r = 0; r < f.step_rounds; ++r) {
+        // best candidate of round r
+        int best = -1;
+        double bs = 0.0;
+        int64_t bid = 0;
+        while (ci < C) {
+            const int cs = slot * kMaxCand + order[ci];
+            const int64_t id = P.hId[f.hyp_base + P.cHyp[cs]];
+            const int64_t rr = ((id >> 2) - f.step_first) / f.step_div;
+            if (rr != r) break;
+            const double s = P.cS64[cs];
+            if (best < 0 || s < bs || (s == bs && id < bid)) {
+                best = cs;
+                bs = s;
+                bid = id;
+            }
+            ++ci;
+        }
+        if (best >= 0 && (!f.found || bs < f.best_score)) {
+            f.found = 1;
+            f.best_score = bs;
+            f.best_count = P.cCnt[best];
+            f.best_sample = bid >> 2;
+            f.best_sol = (int32_t)(bid & 3);
+            const double *Pp = P.hP64 + 12 * (f.hyp_base + P.cHyp[best]);
+            for (int e = 0; e < 12; ++e) f.best_P[e] = Pp[e];
+        }
+        if (forced) continue;
+        const int64_t after = f.step_first + (r + 1) * f.B;
+        const int64_t need = needed_samples(f.found ? f.best_count : 0, f.n, f.log_missing, f.trials_mult);
+        if (after > need || after >= f.max_total) {
+            stop = true;
+            r_end = r + 1;
+            break;
+        }
+    }
+    // Hypotheses of the rounds actually consumed.
+    int64_t hyps = 0;
+    for (int64_t r = 0; r < r_end; ++r) hyps += f.round_hyps[r];
+    f.hyps_done += hyps;
+    f.steps += 1;
+    if (forced) {
+        f.samples_done += f.step_samples;
+        f.rounds_done += 1;
+        if (f.samples_done >= f.force_samples) stop = true;
+    } else {
+        f.samples_done = f.step_first + r_end * f.B;
+        f.rounds_done += r_end;
+    }
+    if (stop) {
+        f.status = kLMPending;
+        atomicAdd(&P.counters[kCLMPending], 1ull);
+    } else {
+        atomicAdd(&P.counters[kCStillRansac], 1ull);
+    }
+}
+
+// ------------------------------------------------------------- inliers -----
+// get_inliers_mx (entry.cu:12-26) with the pose entry.cu:79-83 builds from the
+// RANSAC result (R -> quaternion -> R), then an ordered compaction of the
+// inliers into the LM arrays in pixel/f units (entry.cu:87-103).
+__global__ void __launch_bounds__(1024) k_inliers(Pools P) {
+    __shared__ int64_t sh[33];
+    __shared__ double sR[9], st[3], sq[4];
+    const int slot = P.active[blockIdx.x];
+    FrameDev &f = P.frames[slot];
+    if (f.status != kLMPending) return;
+    if (threadIdx.x == 0) {
+        double R[9];
+        for (int r = 0; r < 3; ++r) {
+            for (int c = 0; c < 3; ++c) R[3 * r + c] = f.found ? f.best_P[4 * r + c] : (r == c ? 1.0 : 0.0);
+            st[r] = f.found ? f.best_P[4 * r + 3] : 0.0;
+        }
+        double q[4];
+        rotmat_to_quat(R, q);
+        quat_to_rotmat(q, sR);
+        for (int k = 0; k < 4; ++k) sq[k] = q[k];
+    }
+    __syncthreads();
+    const int64_t base = f.blk_off * kSub;
+    const double sqthr = f.sq_thr;
+    const double scale = 1.0 / f.focal;  // entry.cu:87,98
+    int64_t written = 0;
+    for (int64_t i0 = 0; i0 < f.n; i0 += blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        int in = 0;
+        if (i < f.n) {
+            const int64_t p = base + i;
+            const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
+            const double Z0 = sR[0] * X0 + sR[1] * X1 + sR[2] * X2 + st[0];
+            const double Z1 = sR[3] * X0 + sR[4] * X1 + sR[5] * X2 + st[1];
+            const double Z2 = sR[6] * X0 + sR[7] * X1 + sR[8] * X2 + st[2];
+            const double h0 = Z0 / Z2 - P.xn64[2 * p], h1 = Z1 / Z2 - P.xn64[2 * p + 1];
+            const double r2 = h0 * h0 + h1 * h1;
+            in = (r2 < sqthr && Z2 > 0.0) ? 1 : 0;
+            P.mask[p] = (uint8_t)in;
+        }
+        int64_t tot;
+        const int64_t ex = block_exclusive_scan(in, sh, tot);
+        if (in) {
+            const int64_t p = base + i;
+            const int64_t o = base + written + ex;
+            const double u = P.uv64[2 * p] * scale, v = P.uv64[2 * p + 1] * scale;
+            const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
+            P.lx64[2 * o] = u;
+            P.lx64[2 * o + 1] = v;
+            P.lX64[3 * o] = X0;
+            P.lX64[3 * o + 1] = X1;
+            P.lX64[3 * o + 2] = X2;
+            P.lA32[o] = make_float4((float)(X0 - f.centre[0]), (float)(X1 - f.centre[1]),
+                                    (float)(X2 - f.centre[2]), (float)u);
+            P.lB32[o] = make_float4((float)X0, (float)X1, (float)X2, (float)v);
+        }
+        written += tot;
+    }
+    if (threadIdx.x == 0) {
+        f.num_inliers = written;
+        FrameResult &res = P.results[slot];
+        for (int k = 0; k < 4; ++k) res.q[k] = sq[k];
+        for (int k = 0; k < 3; ++k) res.t[k] = st[k];
+    }
+}
+
+// ------------------------------------------------------------------ LM -----
+__device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+// Block-wide FP64 sum of NV values per thread into out[] (thread 0 gets them).
+template <int NV>
+__device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch /*32*NV*/, double *out) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        v[k] = warp_sum(v[k]);
+        if (lane == 0) scratch[w * NV + k] = v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        for (int q = 0; q < nw; ++q) s += scratch[q * NV + threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    __syncthreads();
+}
+
+// FP64 Cauchy cost of (q, t) over the compacted inliers (jaco.cuh:31-104).
+__device__ double lm_cost(const Pools &P, int64_t base, int64_t n, const double *q, const double *t,
+                          const double *cam, double inv_sq_thr, double *scratch, double *red) {
+    double acc[1] = {0.0};
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const int64_t o = base + i;
+        double Z[3];
+        quat_rotate(q, P.lX64[3 * o], P.lX64[3 * o + 1], P.lX64[3 * o + 2], Z);
+        Z[0] += t[0];
+        Z[1] += t[1];
+        Z[2] += t[2];
+        const bool valid = Z[2] >= 0.0;
+        const double inv_z = valid ? 1.0 / Z[2] : 0.0;
+        double p0 = Z[0] * inv_z, p1 = Z[1] * inv_z;
+        p0 = cam[0] * p0 + cam[2];
+        p1 = cam[1] * p1 + cam[3];
+        const double r0 = p0 - P.lx64[2 * o], r1 = p1 - P.lx64[2 * o + 1];
+        const double r_squared = r0 * r0 + r1 * r1;
+        acc[0] += valid ? log1p(r_squared * inv_sq_thr) : 0.0;
+    }
+    block_sum_d<1>(acc, scratch, red);
+    return red[0];
+}
+
+// Levenberg-Marquardt with the control flow of lm.cuh:15-171 (damping, accept
+// rule, lambda schedule, the removal of damping after a rejected step, and both
+// stop tests). J^T W J (lower triangle, jaco.cuh:173-200) and J^T W r
+// (:202-209) are accumulated per thread in FP32 with Kahan compensation from
+// centred coordinates, then summed across the block in FP64; the 6x6 Cholesky
+// (lm_utils.cuh:14-100), the step and the cost used for acceptance are FP64.
+__global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
+    __shared__ double scratch[32 * 27];
+    __shared__ double red[27];
+    __shared__ double sJ[36], sg[6], q[4], t[3], qn[4], tn[3];
+    __shared__ float R32[9], tc32[3];
+    __shared__ double cost, cost_new, lambda, grad_norm, step_norm;
+    __shared__ int brk, recompute, iters, invalid;
+    const int slot = P.active[blockIdx.x];
+    FrameDev &f = P.frames[slot];
+    if (f.status != kLMPending) return;
+    FrameResult &res = P.results[slot];
+    const int64_t base = f.blk_off * kSub;
+    const int64_t n = f.num_inliers;
+    const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
+    const float camf[4] = {(float)cam[0], (float)cam[1], (float)cam[2], (float)cam[3]};
+    const double inv_sq_thr = f.lm_inv_sq_thr;
+    const float inv_sq_thr_f = (float)inv_sq_thr;
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) q[k] = res.q[k];
+        for (int k = 0; k < 3; ++k) t[k] = res.t[k];
+    }
+    __syncthreads();
+    double c0 = 0.0;
+    if (!f.skip_refine) c0 = lm_cost(P, base, n, q, t, cam, inv_sq_thr, scratch, red);
+    if (threadIdx.x == 0) {
+        cost = c0;
+        lambda = f.lm_lambda0;
+        recompute = 1;
+        iters = 0;
+        invalid = 0;
+        res.lm_cost0 = c0;
+    }
+    __syncthreads();
+    const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
+    for (int64_t it = 0; it < max_it; ++it) {
+        if (threadIdx.x == 0) brk = 0;
+        if (recompute) {
+            if (threadIdx.x == 0) {
+                double R[9];
+                quat_to_rotmat(q, R);
+                for (int k = 0; k < 9; ++k) R32[k] = (float)R[k];
+                for (int r = 0; r < 3; ++r)
+                    tc32[r] = (float)(t[r] + R[3 * r] * f.centre[0] + R[3 * r + 1] * f.centre[1] +
+                                      R[3 * r + 2] * f.centre[2]);
+            }
+            __syncthreads();
+            float S[27], Cc[27];
+#pragma unroll
+            for (int k = 0; k < 27; ++k) S[k] = Cc[k] = 0.0f;
+            const float r00 = R32[0], r01 = R32[1], r02 = R32[2], r10 = R32[3], r11 = R32[4], r12 = R32[5],
+                        r20 = R32[6], r21 = R32[7], r22 = R32[8];
+            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const float4 A = P.lA32[base + i], Bw = P.lB32[base + i];
+                const float Z0 = r00 * A.x + r01 * A.y + r02 * A.z + tc32[0];
+                const float Z1 = r10 * A.x + r11 * A.y + r12 * A.z + tc32[1];
+                const float Z2 = r20 * A.x + r21 * A.y + r22 * A.z + tc32[2];
+                const float iz = 1.0f / Z2;
+                const float z0 = Z0 * iz, z1 = Z1 * iz;
+                const float rx = (camf[0] * z0 + camf[2]) - A.w;
+                const float ry = (camf[1] * z1 + camf[3]) - Bw.w;
+                const float r2 = rx * rx + ry * ry;
+                float wgt = inv_sq_thr_f / (1.0f + r2 * inv_sq_thr_f);
+                wgt = fmaxf(wgt, FLT_MIN);
+                const float wv = (Z2 >= 0.0f) ? wgt : 0.0f;
+                // dZ = (1/Z2) [fx 0 -fx z0; 0 fy -fy z1] R
+                const float a0 = camf[0] * iz, a2 = -camf[0] * z0 * iz;
+                const float b1 = camf[1] * iz, b2 = -camf[1] * z1 * iz;
+                const float dZ00 = a0 * r00 + a2 * r20, dZ01 = a0 * r01 + a2 * r21, dZ02 = a0 * r02 + a2 * r22;
+                const float dZ10 = b1 * r10 + b2 * r20, dZ11 = b1 * r11 + b2 * r21, dZ12 = b1 * r12 + b2 * r22;
+                const float d00 = wv * (dZ00 * dZ00 + dZ10 * dZ10);
+                const float d10 = wv * (dZ01 * dZ00 + dZ11 * dZ10);
+                const float d11 = wv * (dZ01 * dZ01 + dZ11 * dZ11);
+                const float d20 = wv * (dZ02 * dZ00 + dZ12 * dZ10);
+                const float d21 = wv * (dZ02 * dZ01 + dZ12 * dZ11);
+                const float d22 = wv * (dZ02 * dZ02 + dZ12 * dZ12);
+                const float X0 = Bw.x, X1 = Bw.y, X2 = Bw.z;
+                const float v[27] = {
+                    X2 * (X2 * d11 - X1 * d21) + X1 * (X1 * d22 - X2 * d21),
+                    -X2 * (X2 * d10 - X0 * d21) - X1 * (X0 * d22 - X2 * d20),
+                    X1 * (X0 * d21 - X1 * d20) - X2 * (X0 * d11 - X1 * d10),
+                    X1 * d20 - X2 * d10,
+                    X1 * d21 - X2 * d11,
+                    X1 * d22 - X2 * d21,
+                    X2 * (X2 * d00 - X0 * d20) + X0 * (X0 * d22 - X2 * d20),
+                    -X2 * (X1 * d00 - X0 * d10) - X0 * (X0 * d21 - X1 * d20),
+                    X2 * d00 - X0 * d20,
+                    X2 * d10 - X0 * d21,
+                    X2 * d20 - X0 * d22,
+                    X1 * (X1 * d00 - X0 * d10) + X0 * (X0 * d11 - X1 * d10),
+                    X0 * d10 - X1 * d00,
+                    X0 * d11 - X1 * d10,
+                    X0 * d21 - X1 * d20,
+                    d00, d10, d20, d11, d21, d22,
+                    (wv * rx) * (X1 * dZ02 - X2 * dZ01) + (wv * ry) * (X1 * dZ12 - X2 * dZ11),
+                    -(wv * rx) * (X0 * dZ02 - X2 * dZ00) - (wv * ry) * (X0 * dZ12 - X2 * dZ10),
+                    (wv * rx) * (X0 * dZ01 - X1 * dZ00) + (wv * ry) * (X0 * dZ11 - X1 * dZ10),
+                    dZ00 * (wv * rx) + dZ10 * (wv * ry),
+                    dZ01 * (wv * rx) + dZ11 * (wv * ry),
+                    dZ02 * (wv * rx) + dZ12 * (wv * ry)};
+#pragma unroll
+                for (int k = 0; k < 27; ++k) kahan_add(S[k], Cc[k], v[k]);
+            }
+            double dv[27];
+#pragma unroll
+            for (int k = 0; k < 27; ++k) dv[k] = (double)S[k] - (double)Cc[k];
+            block_sum_d<27>(dv, scratch, red);
+            if (threadIdx.x == 0) {
+                // lower triangle in the reference's order: (0,0),(1,0)..(5,0),(1,1)..(5,1),...
+                const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
+                                        {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
+                                        {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
+                for (int k = 0; k < 36; ++k) sJ[k] = 0.0;
+                for (int k = 0; k < 21; ++k) sJ[idx[k][0] * 6 + idx[k][1]] = red[k];
+                double gn = 0.0;
+                for (int k = 0; k < 6; ++k) {
+                    sg[k] = red[21 + k];
+                    gn += sg[k] * sg[k];
+                }
+                grad_norm = sqrt(gn);
+                if (grad_norm < f.lm_grad_tol) brk = 1;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) {
+            for (int k = 0; k < 6; ++k) sJ[k * 7] += lambda;
+            // Cholesky solve (lm_utils.cuh:14-100), then the step (jaco.cuh:288-299).
+            double L[36];
+            for (int k = 0; k < 36; ++k) L[k] = 0.0;
+            for (int i = 0; i < 6; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    double sum = 0.0;
+                    for (int k = 0; k < j; ++k) sum += L[i * 6 + k] * L[j * 6 + k];
+                    if (i == j) {
+                        double val = sJ[i * 6 + i] - sum;
+                        if (val <= 0.0) val = 1e-15;
+                        L[i * 6 + j] = sqrt(val);
+                    } else {
+                        L[i * 6 + j] = (sJ[i * 6 + j] - sum) / L[j * 6 + j];
+                    }
+                }
+            double y[6], x[6];
+            for (int i = 0; i < 6; ++i) {
+                double sum = 0.0;
+                for (int j = 0; j < i; ++j) sum += L[i * 6 + j] * y[j];
+                y[i] = (sg[i] - sum) / L[i * 6 + i];
+            }
+            for (int i = 5; i >= 0; --i) {
+                double sum = 0.0;
+                for (int j = i + 1; j < 6; ++j) sum += L[j * 6 + i] * x[j];
+                x[i] = (y[i] - sum) / L[i * 6 + i];
+            }
+            double sn = 0.0;
+            for (int k = 0; k < 6; ++k) {
+                x[k] = -1 * x[k];
+                sn += x[k] * x[k];
+            }
+            step_norm = sqrt(sn);
+            if (step_norm < f.lm_step_tol) brk = 1;
+            quat_step_post(q, x, qn);
+            double dt[3];
+            quat_rotate(q, x[3], x[4], x[5], dt);
+            for (int k = 0; k < 3; ++k) tn[k] = t[k] + dt[k];
+        }
+        __syncthreads();
+        if (brk) break;
+        const double cn = lm_cost(P, base, n, qn, tn, cam, inv_sq_thr, scratch, red);
+        if (threadIdx.x == 0) {
+            if (cn < cost) {
+                for (int k = 0; k < 4; ++k) q[k] = qn[k];
+                for (int k = 0; k < 3; ++k) t[k] = tn[k];
+                lambda = fmax(f.lm_min_lambda, lambda / 10);
+                cost = cn;
+                recompute = 1;
+            } else {
+                ++invalid;
+                for (int k = 0; k < 6; ++k) sJ[k * 7] -= lambda;
+                lambda = fmin(f.lm_max_lambda, lambda * 10);
+                recompute = 0;
+            }
+            ++iters;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) res.q[k] = q[k];
+        for (int k = 0; k < 3; ++k) res.t[k] = t[k];
+        res.lm_iters = iters;
+        res.lm_invalid = invalid;
+        res.lm_cost = cost;
+        res.samples = f.samples_done;
+        res.rounds = f.rounds_done;
+        res.hypotheses = f.hyps_done;
+        res.ransac_inliers = f.found ? f.best_count : 0;
+        res.num_inliers = f.num_inliers;
+        res.model_score = f.found ? f.best_score : DBL_MAX;
+        res.best_sample = f.found ? f.best_sample : -1;
+        res.best_sol = f.found ? f.best_sol : -1;
+        res.steps = f.steps;
+        res.rescored = f.rescored;
+        res.overflow = f.overflow;
+        res.status = kDone;
+        f.status = kDone;
+    }
+}
+
+// ------------------------------------------------- standalone entry points --
+// get_inliers_mx (entry.cu:12-26) for a given pose over raw device arrays.
+__global__ void k_pose_mask(const double *xn, const double *X, int64_t n, const double *qt,
+                            double sq_thr, uint8_t *mask, unsigned long long *count) {
+    double R[9];
+    quat_to_rotmat(qt, R);
+    const double t0 = qt[4], t1 = qt[5], t2 = qt[6];
+    int c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double X0 = X[3 * i], X1 = X[3 * i + 1], X2 = X[3 * i + 2];
+        const double Z0 = R[0] * X0 + R[1] * X1 + R[2] * X2 + t0;
+        const double Z1 = R[3] * X0 + R[4] * X1 + R[5] * X2 + t1;
+        const double Z2 = R[6] * X0 + R[7] * X1 + R[8] * X2 + t2;
+        const double h0 = Z0 / Z2 - xn[2 * i], h1 = Z1 / Z2 - xn[2 * i + 1];
+        const int in = (h0 * h0 + h1 * h1 < sq_thr && Z2 > 0.0) ? 1 : 0;
+        mask[i] = (uint8_t)in;
+        c += in;
+    }
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
+
+// bundle_adjust_cuda input: the caller's (x, X) become the LM arrays as given
+// (ba.cu:41-62), with FP32 copies centred on the AABB midpoint.
+__global__ void k_lm_pack(Pools P) {
+    const int slot = P.active[0];
+    FrameDev &f = P.frames[slot];
+    const int64_t base = f.blk_off * kSub;
+    const double c0 = 0.5 * (ordered_to_dbl(f.bmin[0]) + ordered_to_dbl(f.bmax[0]));
+    const double c1 = 0.5 * (ordered_to_dbl(f.bmin[1]) + ordered_to_dbl(f.bmax[1]));
+    const double c2 = 0.5 * (ordered_to_dbl(f.bmin[2]) + ordered_to_dbl(f.bmax[2]));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        f.centre[0] = c0;
+        f.centre[1] = c1;
+        f.centre[2] = c2;
+        f.num_inliers = f.n;
+    }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < f.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t p = base + i;
+        const double u = P.uv64[2 * p], v = P.uv64[2 * p + 1];
+        const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
+        P.lx64[2 * p] = u;
+        P.lx64[2 * p + 1] = v;
+        P.lX64[3 * p] = X0;
+        P.lX64[3 * p + 1] = X1;
+        P.lX64[3 * p + 2] = X2;
+        P.lA32[p] = make_float4((float)(X0 - c0), (float)(X1 - c1), (float)(X2 - c2), (float)u);
+        P.lB32[p] = make_float4((float)X0, (float)X1, (float)X2, (float)v);
+    }
+}
+
+// ------------------------------------------------------------- debug -------
+// Per-hypothesis inlier counts decided in FP32 (same formula as k_score),
+// with pairs whose FP32 r^2/tau^2 lies within 2^-10 of 1 (or whose depth is
+// within 2^-20 of zero) re-decided with the FP64 reference formula.
+__global__ void k_debug_counts(Pools P) {
+    const int slot = P.active[0];
+    const FrameDev &f = P.frames[slot];
+    const int64_t base = f.blk_off * kSub;
+    for (int h = blockIdx.x; h < f.hyp_count; h += gridDim.x) {
+        const float *Q = P.hP32 + 12 * (f.hyp_base + h);
+        const double *M = P.hP64 + 12 * (f.hyp_base + h);
+        int cnt = 0;
+        for (int64_t i = threadIdx.x; i < f.n; i += blockDim.x) {
+            const float2 *blk = P.pts32 + (f.blk_off + i / kSub) * kBlockFloat2;
+            const int j = (int)(i % kSub);
+            const float X = blk[j].x, Y = blk[kSub + j].x, Z = blk[2 * kSub + j].x;
+            const float NX = blk[3 * kSub + j].x, NY = blk[4 * kSub + j].x;
+            const float z0 = fmaf(Q[0], X, fmaf(Q[1], Y, fmaf(Q[2], Z, Q[3])));
+            const float z1 = fmaf(Q[4], X, fmaf(Q[5], Y, fmaf(Q[6], Z, Q[7])));
+            const float z2 = fmaf(Q[8], X, fmaf(Q[9], Y, fmaf(Q[10], Z, Q[11])));
+            const float inv = rcp_approx(z2);
+            const float r0 = fmaf(z0, inv, NX), r1 = fmaf(z1, inv, NY);
+            const float qv = fmaf(r0, r0, r1 * r1);
+            int in;
+            if (fabsf(qv - 1.0f) < (1.0f / 1024.0f) || fabsf(z2) < 1e-6f || !(qv == qv)) {
+                const int64_t p = base + i;
+                const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
+                const double d0 = M[0] * X0 + M[1] * X1 + M[2] * X2 + M[3];
+                const double d1 = M[4] * X0 + M[5] * X1 + M[6] * X2 + M[7];
+                const double d2 = M[8] * X0 + M[9] * X1 + M[10] * X2 + M[11];
+                const double iv = 1.0 / d2;
+                const double e0 = d0 * iv - P.xn64[2 * p], e1 = d1 * iv - P.xn64[2 * p + 1];
+                in = (e0 * e0 + e1 * e1 < f.sq_thr && d2 > 0.0) ? 1 : 0;
+            } else {
+                in = (qv < 1.0f && z2 > 0.0f) ? 1 : 0;
+            }
+            cnt += in;
+        }
+        cnt = warp_sum(cnt);
+        __shared__ int sc[32];
+        if ((threadIdx.x & 31) == 0) sc[threadIdx.x >> 5] = cnt;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int s = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += sc[k];
+            P.dbg_counts[h] = s;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace tbr
