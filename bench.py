@@ -1,0 +1,332 @@
+#!/usr/bin/env python
+"""Headline benchmark: absolute-pose RANSAC frames/s on 1 B200 (replicas on N).
+
+Workload (one "step"): the batched configuration -- 256 synthetic frames of
+uneven size (N log-uniform in [500, 30000], inlier ratio U[0.10, 0.80], pixel
+noise U[0.5, 2] px, 4 px threshold, 1000 samples per round, the reference's
+adaptive stop rule, LM refinement) estimated in one CUDA-graph launch with the
+inputs resident in device memory. L2 is flushed (256 MiB write) before every
+timed step. Each rank of a multi-GPU run estimates its own 256 frames (frames
+are independent: replicas, no collective on the path).
+
+Also reported on the same frames: the end-to-end public call with host buffers
+(e2e), a loop of plain per-frame calls (the reference's calling pattern),
+success rate at 5 deg / 5 cm, per-kernel device times from CUDA events, the
+FP32 roofline of the scoring kernel, and the FP64 CPU oracle on the host cores.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "frames/s & p50/p99 ms at >=99% success: served-batched vs plain call, 1 B200"
+WORKLOAD = ("batched: 256 frames/GPU, N log-uniform [500,30000], inlier ratio U[0.10,0.80], "
+            "sigma U[0.5,2] px, 640x480 f=525, 4 px, 1000 samples/round, p=0.9999, LM")
+FLOP_PER_PAIR = 27  # projection 9 FMA, reciprocal, 2 residual FMA, r^2, score add
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--frames", type=int, default=256)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        backend = "nccl"
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(pg, v: float, device) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples every 200 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        try:
+            rows = [r.strip().split(", ") for r in open(self.path) if r.strip()]
+        except Exception:
+            rows = []
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(float(r[3]) for r in rows if len(r) > 3)}
+
+
+def success(results, frames):
+    from turboransac_b200 import scenes
+    ok = 0
+    for r, f in zip(results, frames):
+        ae, te = scenes.pose_error(scenes.quat_to_rotmat(r["q"]), r["t"], f.R_gt, f.t_gt)
+        ok += (ae < 5.0 and te < 5.0)
+    return ok / len(frames)
+
+
+def cpu_baseline(frames, seconds_target=15.0):
+    """FP64 oracle (same algorithm, same samples) over frames with all host threads."""
+    from oracle.oracle import Oracle
+    o = Oracle()
+    cores = os.cpu_count() or 1
+    # Calibrate on a few frames, then size the sample to ~seconds_target.
+    t0 = time.perf_counter()
+    o.estimate_batch(frames[:cores], threads=cores)
+    dt = time.perf_counter() - t0
+    per_frame_wall = dt / min(len(frames), cores)
+    m = int(max(cores, min(len(frames), seconds_target / max(per_frame_wall, 1e-6))))
+    m = min(m, len(frames))
+    sample = frames[:m]
+    t0 = time.perf_counter()
+    o.estimate_batch(sample, threads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": m / dt, "unit": "frames/s", "cores": cores, "kind": "port",
+            "sample": f"first {m} frames of the batched workload, FP64 oracle, {cores} threads over frames",
+            "seconds": dt}
+
+
+def run_reference(args, world, rank):
+    """--impl reference: the CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return
+    from turboransac_b200 import scenes
+    frames = scenes.batched_frames(args.frames)
+    from oracle.oracle import Oracle
+    o = Oracle()
+    cores = os.cpu_count() or 1
+    m = min(len(frames), max(cores, 16))
+    sample = frames[:m]
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        o.estimate_batch(sample, threads=cores)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            times.append(dt)
+    fps = m * len(times) / sum(times)
+    line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": m, "sample": f"first {m} frames"},
+            "impl": "reference",
+            "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
+                             "sample": f"first {m} frames of the batched workload per step, {cores} threads"},
+            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+
+    import numpy as np
+    import torch
+
+    from turboransac_b200 import (Batch, BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda,
+                                  estimate_batch, scenes)
+    from turboransac_b200 import build as tbuild
+    tbuild.build()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    frames = scenes.batched_frames(args.frames, first=rank * args.frames)
+    ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
+    ctx = Context(local, 6 << 30)
+    batch = Batch(ctx, frames, ro, hyp_per_thread=args.hr)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    for _ in range(args.warmup):
+        batch.run()
+        batch.sync()
+    res = batch.results()
+    steps_per_run = max(r["steps"] for r in res)
+
+    barrier(pg)
+    torch.cuda.synchronize()
+    dev_ms = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            batch.run()
+            batch.sync()
+            dev_ms.append(batch.results()[0]["gpu_ms"])
+    torch.cuda.synchronize()
+    barrier(pg)
+    total_ms = max_over_ranks(pg, sum(dev_ms), dev)
+    value = world * args.frames * args.steps / (total_ms / 1000.0)
+    res = batch.results()
+    succ = success(res, frames)
+
+    # Per-kernel device time (CUDA events on the launch stream) for the roofline.
+    prof, pairs = batch.profile()
+    score_ms, score_launches = prof["k_score"]
+    achieved = FLOP_PER_PAIR * pairs / (score_ms / 1000.0) / 1e12
+    peak_fp32 = fp32_peak_tflops(ctx)
+    nominal = 148 * 256 * 1965e6 / 1e12
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "k_score_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tj = json.load(open(tpath))
+            traffic = tj.get("bytes_per_launch_batched")
+        except Exception:
+            traffic = None
+
+    # e2e: public call, host buffers in, results out, every step.
+    e2e_t = []
+    for i in range(1 + max(1, args.steps // 2)):
+        t0 = time.perf_counter()
+        estimate_batch(ctx, frames, ro)
+        dt = time.perf_counter() - t0
+        if i:
+            e2e_t.append(dt)
+    e2e_fps = world * args.frames * len(e2e_t) / max_over_ranks(pg, sum(e2e_t), dev)
+    h2d = sum(40 * f.n for f in frames)
+    d2h = args.frames * 264
+
+    # Plain per-frame calls (the reference's calling pattern) on the same frames.
+    plain = None
+    if not args.no_plain:
+        lat = []
+        for f in frames:
+            cam = Camera_cuda(1, 640, 480, list(f.K))
+            t0 = time.perf_counter()
+            ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, BundleOptions_cuda(), seed=f.seed)
+            lat.append(1000.0 * (time.perf_counter() - t0))
+        plain = {"frames_per_s": len(lat) / (sum(lat) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
+                 "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(frames)
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 scoring / fp64 P3P, re-rank, LM solve",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": world * args.frames,
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "engine_steps_per_batch": steps_per_run, "parallelism": f"replicas x{world}"},
+            "success_rate": succ,
+            "pairs_scored_per_batch": pairs,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
+                         "frac": achieved / peak_fp32 if peak_fp32 else None, "traffic": traffic,
+                         "kernel": "k_score", "flop_per_pair": FLOP_PER_PAIR,
+                         "peak_source": "FP32 FMA peak measured in this run (packed-FMA kernel); "
+                                        f"nominal {nominal:.1f} TFLOP/s at 1965 MHz",
+                         "launch_ms_avg": score_ms / max(score_launches, 1)},
+            "kernels_ms_per_batch": {k: v[0] for k, v in prof.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "plain_call": plain,
+            "speedup_vs_plain": (value / plain["frames_per_s"]) if plain else None,
+            "gpu_launches": args.steps * (1 + 11 * steps_per_run),
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def fp32_peak_tflops(ctx) -> float | None:
+    import ctypes as C
+
+    from turboransac_b200 import _lib
+    L = _lib.lib()
+    if not hasattr(L, "tbr_measure_fp32_peak"):
+        return None
+    L.tbr_measure_fp32_peak.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    v = C.c_double()
+    if L.tbr_measure_fp32_peak(ctx.handle, C.byref(v)) != 0:
+        return None
+    return v.value
+
+
+if __name__ == "__main__":
+    main()

@@ -203,6 +203,23 @@ tbr_status tbr_batch_sync(tbr_batch *b);     /* waits; returns the first device 
 tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results);
 void tbr_batch_destroy(tbr_batch *b);
 
+/* Per-kernel device time of one batch run, stepped from the host with a CUDA
+ * event pair around every kernel launch on the context stream (slower than
+ * tbr_batch_run; for measurement only). pairs_scored = hypothesis x point
+ * pairs evaluated by the FP32 scoring kernel. */
+typedef struct tbr_kernel_profile {
+    char name[32];
+    double total_ms;
+    int64_t launches;
+} tbr_kernel_profile;
+tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max, int32_t *n_out,
+                             uint64_t *pairs_scored);
+
+/* Measured FP32 FMA throughput of the context's device (packed FP32x2 FMA
+ * chains on every SM, CUDA-event timed): the denominator of the scoring
+ * kernel's roofline. */
+tbr_status tbr_measure_fp32_peak(tbr_context *ctx, double *tflops);
+
 /* -------------------------------------------------------------- serving --
  * Continuous batching: a worker thread advances every admitted frame by one
  * engine step at a time; requests that arrive while others run are admitted

@@ -69,6 +69,10 @@ class FrameResultC(C.Structure):
                 ("pad", C.c_int32), ("stats", StatsC)]
 
 
+class KernelProfileC(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("total_ms", C.c_double), ("launches", C.c_int64)]
+
+
 class ServerConfigC(C.Structure):
     _fields_ = [("workspace_budget_bytes", C.c_uint64), ("max_slots", C.c_int32),
                 ("max_queue", C.c_int32), ("ransac", RansacOptionsC), ("ext", ExtOptionsC)]
@@ -87,7 +91,7 @@ EXPORTS = [
     "tbr_abi_version", "tbr_last_error", "tbr_default_ransac_options", "tbr_default_bundle_options",
     "tbr_context_create", "tbr_context_destroy", "tbr_estimate_absolute_pose", "tbr_get_inliers",
     "tbr_bundle_adjust", "tbr_estimate_batch", "tbr_batch_create", "tbr_batch_run", "tbr_batch_sync",
-    "tbr_batch_results", "tbr_batch_destroy", "tbr_server_create", "tbr_server_submit",
+    "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
     "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
     "tbr_debug_score_samples",
 ]
@@ -122,6 +126,9 @@ def lib() -> C.CDLL:
     L.tbr_batch_sync.argtypes = [vp]
     L.tbr_batch_results.argtypes = [vp, C.POINTER(FrameResultC)]
     L.tbr_batch_destroy.argtypes = [vp]
+    L.tbr_batch_profile.argtypes = [vp, C.POINTER(KernelProfileC), C.c_int32, C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_uint64)]
+    L.tbr_measure_fp32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.tbr_server_create.argtypes = [vp, C.POINTER(ServerConfigC), C.POINTER(vp)]
     L.tbr_server_submit.argtypes = [vp, C.POINTER(FrameDescC), C.POINTER(C.c_uint64)]
     L.tbr_server_poll.argtypes = [vp, C.POINTER(ServerResultC), C.c_int32, C.POINTER(C.c_int32)]

@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from ._lib import TbrError, check
 
-__all__ = ["RansacOptions_cuda", "BundleOptions_cuda", "RansacStats_cuda", "Camera_cuda",
+__all__ = ["Batch", "estimate_batch", "RansacOptions_cuda", "BundleOptions_cuda", "RansacStats_cuda", "Camera_cuda",
            "CameraPose_cuda", "Context", "estimate_absolute_pose_cuda", "get_inliers_mx",
            "bundle_adjust_cuda", "TbrError"]
 
@@ -288,3 +288,99 @@ def bundle_adjust_cuda(x, X, camera: Camera_cuda, pose: CameraPose_cuda, opt: Bu
                        weights=None):
     """ba.cuh:17-24: LM refinement; returns the refined CameraPose_cuda."""
     return default_context().bundle_adjust(x, X, camera, pose, opt, weights)[0]
+
+
+def _frame_descs(frames, seeds=None, max_reproj_error=0.0):
+    """Build tbr_frame_desc entries (keeps references to the float64 arrays)."""
+    keep = []
+    arr = (_lib.FrameDescC * len(frames))()
+    for i, fr in enumerate(frames):
+        uv = np.ascontiguousarray(fr.uv, np.float64)
+        X = np.ascontiguousarray(fr.xyz, np.float64)
+        keep += [uv, X]
+        arr[i].points2D = uv.ctypes.data
+        arr[i].points3D = X.ctypes.data
+        arr[i].n = uv.shape[0]
+        for k in range(4):
+            arr[i].K[k] = float(fr.K[k])
+        arr[i].seed = (fr.seed if seeds is None else seeds[i]) & 0xFFFFFFFFFFFFFFFF
+        arr[i].max_reproj_error = max_reproj_error or getattr(fr, "threshold_px", 0.0)
+    return arr, keep
+
+
+def _results(res, n):
+    out = []
+    for i in range(n):
+        r = res[i]
+        out.append({"q": np.array(r.q[:]), "t": np.array(r.t[:]), "status": r.status, **r.stats.as_dict()})
+    return out
+
+
+class Batch:
+    """Frames uploaded once; run() replays one captured CUDA graph (device loop
+    over engine steps) with the inputs resident in device memory."""
+
+    def __init__(self, ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None,
+                 hyp_per_thread: int = 0, chunk_points: int = 0):
+        self.ctx = ctx
+        self.n = len(frames)
+        arr, self._keep = _frame_descs(frames)
+        ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+        ext = _lib.ExtOptionsC()
+        ext.hyp_per_thread = hyp_per_thread
+        ext.chunk_points = chunk_points
+        h = C.c_void_p()
+        with ctx._lock:
+            check(_lib.lib().tbr_batch_create(ctx.handle, arr, self.n, C.byref(ro), C.byref(ext), C.byref(h)))
+        self._h = h
+
+    def run(self):
+        check(_lib.lib().tbr_batch_run(self._h))
+
+    def sync(self):
+        check(_lib.lib().tbr_batch_sync(self._h))
+
+    def results(self):
+        res = (_lib.FrameResultC * self.n)()
+        check(_lib.lib().tbr_batch_results(self._h, res))
+        return _results(res, self.n)
+
+    def profile(self):
+        """Per-kernel device ms of one host-stepped run (CUDA events) and pairs scored."""
+        out = (_lib.KernelProfileC * 16)()
+        n = C.c_int32()
+        pairs = C.c_uint64()
+        check(_lib.lib().tbr_batch_profile(self._h, out, 16, C.byref(n), C.byref(pairs)))
+        return {out[i].name.decode(): (out[i].total_ms, out[i].launches) for i in range(n.value)}, pairs.value
+
+    def close(self):
+        if self._h:
+            _lib.lib().tbr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, masks: bool = False):
+    """Host buffers in, results out, all frames in one call (tbr_estimate_batch)."""
+    arr, keep = _frame_descs(frames)
+    ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+    ext = _lib.ExtOptionsC()
+    res = (_lib.FrameResultC * len(frames))()
+    mbufs = None
+    mptrs = None
+    if masks:
+        mbufs = [np.zeros(f.n, np.uint8) for f in frames]
+        mptrs = (C.c_void_p * len(frames))(*[m.ctypes.data for m in mbufs])
+    with ctx._lock:
+        check(_lib.lib().tbr_estimate_batch(ctx.handle, arr, len(frames), C.byref(ro), C.byref(ext), res,
+                                            C.cast(mptrs, C.c_void_p) if masks else None))
+    out = _results(res, len(frames))
+    if masks:
+        for o, m in zip(out, mbufs):
+            o["inliers"] = m
+    return out

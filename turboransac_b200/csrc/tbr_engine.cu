@@ -189,10 +189,11 @@ class Engine {
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
         // Split: 30 % hypotheses, the rest points, after the per-frame state.
-        const size_t per_frame = sizeof(FrameDev) + sizeof(FrameResult) + sizeof(int32_t) +
-                                 (size_t)kMaxCand * (4 + 8 + 8 + 4) +
-                                 (size_t)kMaxCand * kMaxRChunks * 12 + 64;
-        const size_t fixed = (size_t)max_frames * per_frame + 3 * (kMaxActive + 1) * 8 + 4096 * 8;
+        const size_t per_frame = sizeof(FrameDev) + sizeof(FrameResult) + sizeof(int32_t) + 64;
+        P.cand_cap = std::max<int64_t>(16384, (int64_t)max_frames * 256);
+        const size_t per_cand = 4 + 8 + 8 + 4 + (size_t)kMaxRChunks * 12;
+        const size_t fixed = (size_t)max_frames * per_frame + (size_t)P.cand_cap * per_cand +
+                             3 * (kMaxActive + 1) * 8 + 4096 * 8;
         if (budget < fixed + (64ull << 20)) return fail(TBR_ERR_INVALID_ARG, "workspace too small");
         const size_t rest = budget - fixed;
         const size_t per_hyp = 96 + 48 + 8 + 4 + 4 * 32 + 4;
@@ -228,12 +229,12 @@ class Engine {
         add((void **)&P.hS32, 4 * P.max_hyps);
         add((void **)&P.part, 4 * P.max_parts);
         add((void **)&P.hb_arrive, 4 * P.max_hb);
-        add((void **)&P.cHyp, 4 * (size_t)max_frames * kMaxCand);
-        add((void **)&P.cS64, 8 * (size_t)max_frames * kMaxCand);
-        add((void **)&P.cCnt, 8 * (size_t)max_frames * kMaxCand);
-        add((void **)&P.cpS, 8 * (size_t)max_frames * kMaxCand * kMaxRChunks);
-        add((void **)&P.cpC, 4 * (size_t)max_frames * kMaxCand * kMaxRChunks);
-        add((void **)&P.c_arrive, 4 * (size_t)max_frames * kMaxCand);
+        add((void **)&P.cHyp, 4 * (size_t)P.cand_cap);
+        add((void **)&P.cS64, 8 * (size_t)P.cand_cap);
+        add((void **)&P.cCnt, 8 * (size_t)P.cand_cap);
+        add((void **)&P.cpS, 8 * (size_t)P.cand_cap * kMaxRChunks);
+        add((void **)&P.cpC, 4 * (size_t)P.cand_cap * kMaxRChunks);
+        add((void **)&P.c_arrive, 4 * (size_t)P.cand_cap);
         add((void **)&P.counters, 8 * kCNum);
         add((void **)&P.dbg_counts, 8 * P.max_hyps);
         size_t total = 0;
@@ -332,37 +333,60 @@ class Engine {
         return f;
     }
 
-    // Enqueue the step kernels for the current active list.
-    void launch_step(int n_active, int hr) {
-        k_plan<<<1, kMaxActive, 0, stream>>>(P);
-        k_sample_p3p<<<p3p_grid, 128, 0, stream>>>(P);
-        k_score_plan<<<1, kMaxActive, 0, stream>>>(P);
-        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, stream>>>(P);
-        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, stream>>>(P);
-        k_select<<<n_active, 256, 0, stream>>>(P);
-        k_rescore_plan<<<1, kMaxActive, 0, stream>>>(P);
-        k_rescore<<<rescore_grid, 256, 0, stream>>>(P);
-        k_finalize<<<(n_active + 127) / 128, 128, 0, stream>>>(P);
-        k_inliers<<<n_active, 1024, 0, stream>>>(P);
-        k_lm<<<n_active, kLMThreads, 0, stream>>>(P);
+    // Enqueue the step kernels for the active list of `Q`. With `prof`, every
+    // kernel is bracketed by CUDA events on this stream.
+    struct Profile {
+        cudaEvent_t ev[2 * 12] = {};
+        double ms[12] = {};
+        int64_t launches[12] = {};
+        bool armed = false;
+    };
+    static constexpr const char *kKernelNames[12] = {"k_plan", "k_sample_p3p", "k_score_plan", "k_score",
+                                                     "k_select", "k_rescore_plan", "k_rescore", "k_finalize",
+                                                     "k_inliers", "k_lm", "k_prep", "unused"};
+    void launch_step(const Pools &Q, int n_active, int hr, Profile *prof = nullptr) {
+        auto beg = [&](int k) { if (prof) cudaEventRecord(prof->ev[2 * k], stream); };
+        auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], stream); prof->launches[k]++; } };
+        beg(0); k_plan<<<1, kMaxActive, 0, stream>>>(Q); end(0);
+        beg(1); k_sample_p3p<<<p3p_grid, 128, 0, stream>>>(Q); end(1);
+        beg(2); k_score_plan<<<1, kMaxActive, 0, stream>>>(Q); end(2);
+        beg(3);
+        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, stream>>>(Q);
+        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, stream>>>(Q);
+        end(3);
+        beg(4); k_select<<<n_active, 256, 0, stream>>>(Q); end(4);
+        beg(5); k_rescore_plan<<<1, kMaxActive, 0, stream>>>(Q); end(5);
+        beg(6); k_rescore<<<rescore_grid, 256, 0, stream>>>(Q); end(6);
+        beg(7); k_finalize<<<n_active, 256, 0, stream>>>(Q); end(7);
+        beg(8); k_inliers<<<n_active, 1024, 0, stream>>>(Q); end(8);
+        beg(9); k_lm<<<n_active, kLMThreads, 0, stream>>>(Q); end(9);
     }
 
-    void launch_prep(int n_active, int64_t max_n) {
+    void launch_prep(const Pools &Q, int n_active, int64_t max_n) {
         const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024));
-        k_prep_bounds<<<dim3(bx, n_active), 256, 0, stream>>>(P);
-        k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(P);
+        k_prep_bounds<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
+        k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
     }
+    void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n); }
 
-    // Runs admitted frames (slots) to completion with one host check per step.
-    tbr_status run(const std::vector<int> &slots, int hr, int max_steps, int *steps_out) {
-        const int na = (int)slots.size();
+    // Runs the active frames of `Q` to completion with one host check per step.
+    tbr_status run(const Pools &Q, int na, int hr, int max_steps, int *steps_out, Profile *prof = nullptr) {
         int steps = 0;
+        if (prof && !prof->armed) {
+            for (auto &e : prof->ev) TBR_CUDA(cudaEventCreate(&e));
+            prof->armed = true;
+        }
         for (;;) {
-            TBR_CUDA(cudaMemsetAsync(P.counters + kCStillRansac, 0, 16, stream));
-            launch_step(na, hr);
+            launch_step(Q, na, hr, prof);
             TBR_CUDA(cudaGetLastError());
-            TBR_CUDA(cudaMemcpyAsync(h_counters, P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, stream));
+            TBR_CUDA(cudaMemcpyAsync(h_counters, Q.counters, 8 * kCNum, cudaMemcpyDeviceToHost, stream));
             TBR_CUDA(cudaStreamSynchronize(stream));
+            if (prof)
+                for (int k = 0; k < 10; ++k) {
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, prof->ev[2 * k], prof->ev[2 * k + 1]);
+                    prof->ms[k] += ms;
+                }
             ++steps;
             if (h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
             if (h_counters[kCStillRansac] == 0) break;
@@ -370,6 +394,9 @@ class Engine {
         }
         if (steps_out) *steps_out = steps;
         return TBR_OK;
+    }
+    tbr_status run(const std::vector<int> &slots, int hr, int max_steps, int *steps_out) {
+        return run(P, (int)slots.size(), hr, max_steps, steps_out);
     }
 };
 
@@ -757,17 +784,236 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     return TBR_OK;
 }
 
-// Placeholders until the graph-captured batch handle and the serving loop land.
-tbr_status tbr_batch_create(tbr_context *, const tbr_frame_desc *, int32_t, const tbr_ransac_options *,
-                            const tbr_ext_options *, tbr_batch **) {
-    return fail(TBR_ERR_INTERNAL, "tbr_batch_create: not available in this build");
+}  // extern "C"
+
+// --------------------------------------------------------------- batches --
+struct tbr_batch {
+    tbr_context *ctx = nullptr;
+    std::vector<int> slots;
+    std::vector<int64_t> ns, blk_off, n_blocks;
+    RunOptions o;
+    Pools Q{};
+    int32_t *d_active = nullptr;
+    FrameDev *d_init = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool launched = false;
+    Engine::Profile prof;
+};
+
+static void batch_free(tbr_batch *b) {
+    if (!b) return;
+    Engine &E = b->ctx->E;
+    cudaStreamSynchronize(E.stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->d_active) cudaFree(b->d_active);
+    if (b->d_init) cudaFree(b->d_init);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    for (auto &e : b->prof.ev)
+        if (e) cudaEventDestroy(e);
+    for (size_t i = 0; i < b->slots.size(); ++i) {
+        E.blocks.release(b->blk_off[i], b->n_blocks[i]);
+        E.free_slots.push_back(b->slots[i]);
+    }
+    delete b;
 }
-tbr_status tbr_batch_run(tbr_batch *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
-tbr_status tbr_batch_sync(tbr_batch *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
-tbr_status tbr_batch_results(tbr_batch *, tbr_frame_result *) {
-    return fail(TBR_ERR_INTERNAL, "not available in this build");
+
+extern "C" {
+
+tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                            const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext, tbr_batch **out) {
+    if (!ctx || !frames || n_frames < 1 || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    if (n_frames > kMaxActive) return fail(TBR_ERR_INVALID_ARG, "at most 1024 frames per batch");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations must be >= 1");
+    std::vector<FrameHost> fr;
+    for (int i = 0; i < n_frames; ++i) {
+        const tbr_frame_desc &d = frames[i];
+        if (d.n < 3 || !d.points2D || !d.points3D || !(d.K[0] > 0) || !(d.K[1] > 0))
+            return fail(TBR_ERR_INVALID_ARG, "bad frame");
+        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
+                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+    }
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    auto *b = new tbr_batch();
+    b->ctx = ctx;
+    b->o = make_run_options(&ro, nullptr, ext);
+    int64_t max_n = 0;
+    tbr_status st = admit_frames(E, fr, b->o, b->slots, max_n);
+    if (st) {
+        delete b;
+        return st;
+    }
+    // The batch keeps its own active list so that other calls on the context
+    // can run between its launches.
+    if (cudaMalloc(&b->d_active, 4 * n_frames) != cudaSuccess ||
+        cudaMalloc(&b->d_init, sizeof(FrameDev) * n_frames) != cudaSuccess) {
+        batch_free(b);
+        return fail(TBR_ERR_OOM, "batch allocation failed");
+    }
+    cudaMemcpyAsync(b->d_active, E.d_active, 4 * n_frames, cudaMemcpyDeviceToDevice, E.stream);
+    b->Q = E.P;
+    b->Q.active = b->d_active;
+    b->Q.n_active = n_frames;
+    E.launch_prep(b->Q, n_frames, max_n);
+    // Snapshot the prepared frame states (AABB centre included).
+    std::vector<FrameDev> hf(n_frames);
+    for (int i = 0; i < n_frames; ++i)
+        cudaMemcpyAsync(b->d_init + i, E.P.frames + b->slots[i], sizeof(FrameDev), cudaMemcpyDeviceToDevice, E.stream);
+    for (int i = 0; i < n_frames; ++i)
+        cudaMemcpyAsync(&hf[i], E.P.frames + b->slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream);
+    if (cudaStreamSynchronize(E.stream) != cudaSuccess) {
+        batch_free(b);
+        return fail(TBR_ERR_CUDA, "batch upload failed");
+    }
+    for (int i = 0; i < n_frames; ++i) {
+        b->ns.push_back(hf[i].n);
+        b->blk_off.push_back(hf[i].blk_off);
+        b->n_blocks.push_back(hf[i].n_blocks);
+    }
+    // Graph: reset -> while (any frame in RANSAC) { step; inliers + LM of finished frames }.
+    cudaGraphConditionalHandle h;
+    bool ok = cudaGraphCreate(&b->graph, 0) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&h, b->graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    cudaGraphNode_t reset_node = nullptr, loop_node = nullptr;
+    if (ok) {
+        cudaKernelNodeParams kp = {};
+        void *args[2] = {(void *)&b->Q, (void *)&b->d_init};
+        kp.func = (void *)k_reset_frames;
+        kp.gridDim = dim3(n_frames);
+        kp.blockDim = dim3(128);
+        kp.kernelParams = args;
+        ok = cudaGraphAddKernelNode(&reset_node, b->graph, nullptr, 0, &kp) == cudaSuccess;
+    }
+    cudaGraph_t body = nullptr;
+    if (ok) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        ok = cudaGraphAddNode(&loop_node, b->graph, &reset_node, 1, &cp) == cudaSuccess;
+        body = cp.conditional.phGraph_out[0];
+    }
+    if (ok) {
+        ok = cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+             cudaSuccess;
+        if (ok) {
+            E.launch_step(b->Q, n_frames, b->o.hr);
+            k_loop_ctl<<<1, 1, 0, E.stream>>>(b->Q, h, 100000ull);
+            ok = cudaStreamEndCapture(E.stream, &body) == cudaSuccess;
+        }
+    }
+    if (ok) ok = cudaGraphInstantiate(&b->exec, b->graph, 0) == cudaSuccess;
+    if (ok) ok = cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        batch_free(b);
+        return fail(TBR_ERR_CUDA, "graph capture failed");
+    }
+    *out = b;
+    return TBR_OK;
 }
-void tbr_batch_destroy(tbr_batch *) {}
+
+tbr_status tbr_batch_run(tbr_batch *b) {
+    if (!b) return fail(TBR_ERR_INVALID_ARG, "NULL batch");
+    Engine &E = b->ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    TBR_CUDA(cudaEventRecord(b->e0, E.stream));
+    TBR_CUDA(cudaGraphLaunch(b->exec, E.stream));
+    TBR_CUDA(cudaEventRecord(b->e1, E.stream));
+    b->launched = true;
+    return TBR_OK;
+}
+
+tbr_status tbr_batch_sync(tbr_batch *b) {
+    if (!b) return fail(TBR_ERR_INVALID_ARG, "NULL batch");
+    Engine &E = b->ctx->E;
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    TBR_CUDA(cudaMemcpy(E.h_counters, b->Q.counters, 8 * kCNum, cudaMemcpyDeviceToHost));
+    if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    if (E.h_counters[kCError] & kErrOverflow) return fail(TBR_ERR_INTERNAL, "step limit or capacity exceeded");
+    return TBR_OK;
+}
+
+tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results) {
+    if (!b || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = b->ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    float ms = 0.f;
+    if (b->launched) cudaEventElapsedTime(&ms, b->e0, b->e1);
+    std::vector<FrameResult> r(b->slots.size());
+    for (size_t i = 0; i < b->slots.size(); ++i)
+        TBR_CUDA(cudaMemcpyAsync(&r[i], E.P.results + b->slots[i], sizeof(FrameResult), cudaMemcpyDeviceToHost,
+                                 E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    for (size_t i = 0; i < b->slots.size(); ++i) {
+        for (int k = 0; k < 4; ++k) results[i].q[k] = r[i].q[k];
+        for (int k = 0; k < 3; ++k) results[i].t[k] = r[i].t[k];
+        results[i].status = r[i].status == kDone ? TBR_OK : TBR_ERR_INTERNAL;
+        fill_stats(r[i], b->ns[i], &results[i].stats, ms);
+    }
+    return TBR_OK;
+}
+
+tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max, int32_t *n_out,
+                             uint64_t *pairs_scored) {
+    if (!b || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = b->ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    Engine::Profile pr;
+    k_reset_frames<<<b->Q.n_active, 128, 0, E.stream>>>(b->Q, b->d_init);
+    int steps = 0;
+    tbr_status st = E.run(b->Q, b->Q.n_active, b->o.hr, 100000, &steps, &pr);
+    for (auto &e : pr.ev)
+        if (e) cudaEventDestroy(e);
+    if (st) return st;
+    if (pairs_scored) *pairs_scored = E.h_counters[kCPairsTotal];
+    int m = 0;
+    for (int k = 0; k < 10 && m < max; ++k, ++m) {
+        std::snprintf(out[m].name, sizeof(out[m].name), "%s", Engine::kKernelNames[k]);
+        out[m].total_ms = pr.ms[k];
+        out[m].launches = pr.launches[k];
+    }
+    if (n_out) *n_out = m;
+    return TBR_OK;
+}
+
+tbr_status tbr_measure_fp32_peak(tbr_context *ctx, double *tflops) {
+    if (!ctx || !tflops) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    const int blocks = E.num_sms * 8, threads = 256, iters = 1 << 14;
+    float *sink = (float *)E.P.hS32;  // never written (see k_fp32_peak)
+    k_fp32_peak<<<blocks, threads, 0, E.stream>>>(sink, 256, 0.999f, 1e-3f);  // warm-up
+    TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
+    for (int r = 0; r < 4; ++r) k_fp32_peak<<<blocks, threads, 0, E.stream>>>(sink, iters, 0.999f, 1e-3f);
+    TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    TBR_CUDA(cudaEventSynchronize(E.ev1));
+    float ms = 0.f;
+    TBR_CUDA(cudaEventElapsedTime(&ms, E.ev0, E.ev1));
+    const double flop = 4.0 * blocks * threads * (double)iters * 8 * 4;  // 8 f32x2 FMA = 32 FLOP
+    *tflops = flop / (ms * 1e-3) / 1e12;
+    return TBR_OK;
+}
+
+void tbr_batch_destroy(tbr_batch *b) {
+    if (!b) return;
+    std::lock_guard<std::mutex> lk(b->ctx->E.mu);
+    batch_free(b);
+}
+
 tbr_status tbr_server_create(tbr_context *, const tbr_server_config *, tbr_server **) {
     return fail(TBR_ERR_INTERNAL, "tbr_server_create: not available in this build");
 }
@@ -802,7 +1048,6 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, con
     tbr_status st = admit_frames(E, {fh}, o, slots, max_n);
     if (st) return st;
     E.launch_prep(1, max_n);
-    TBR_CUDA(cudaMemsetAsync(E.P.counters + kCStillRansac, 0, 16, E.stream));
     k_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
     k_sample_p3p<<<E.p3p_grid, 128, 0, E.stream>>>(E.P);
     k_score_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
