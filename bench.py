@@ -237,6 +237,8 @@ def main():
     value = world * args.frames * args.steps / (total_ms / 1000.0)
     res = batch.results()
     succ = success(res, frames)
+    print(f"[bench] batched: {value:.1f} frames/s, {total_ms / args.steps:.3f} ms/step, success {succ:.4f}",
+          file=sys.stderr, flush=True)
 
     # Per-kernel device time (CUDA events on the launch stream) for the roofline.
     prof, pairs = batch.profile()

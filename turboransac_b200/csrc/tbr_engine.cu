@@ -179,7 +179,7 @@ class Engine {
         if (stream) cudaStreamDestroy(stream);
     }
 
-    tbr_status init(int dev, uint64_t budget, int frames_cap = 256) {
+    tbr_status init(int dev, uint64_t budget, int frames_cap = kMaxActive) {
         device = dev;
         TBR_CUDA(cudaSetDevice(dev));
         TBR_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -402,15 +402,16 @@ class Engine {
 
 // Uploads frames into slots (host -> device through pinned staging).
 static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
-                               std::vector<int> &slots, int64_t &max_n) {
+                               std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
     if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
+    auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     size_t stage = 0;
     int64_t replay_total = 0;
     for (auto &f : fr) {
-        stage += (size_t)f.n * 40;
+        stage += r256(16 * (size_t)f.n) + r256(24 * (size_t)f.n);
         replay_total += f.replay ? f.replay_count : 0;
     }
-    stage += sizeof(FrameDev) * fr.size() + 4 * fr.size() + 256;
+    stage += fr.size() * r256(sizeof(FrameDev)) + r256(4 * fr.size()) + 256;
     tbr_status st = E.ensure_stage(stage);
     if (st) return st;
     if (replay_total) {
@@ -459,6 +460,7 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
     for (size_t i = 0; i < slots.size(); ++i) ha[i] = slots[i];
     TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * slots.size(), cudaMemcpyHostToDevice, E.stream));
     E.P.n_active = (int32_t)slots.size();
+    if (host_devs) *host_devs = devs;
     return TBR_OK;
 }
 
@@ -546,45 +548,36 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
                                   float *ms_out, int *steps_out) {
     Engine &E = ctx->E;
     std::vector<int> slots;
+    std::vector<FrameDev> devs;
     int64_t max_n = 0;
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
-    tbr_status st = admit_frames(E, fr, o, slots, max_n);
+    tbr_status st = admit_frames(E, fr, o, slots, max_n, &devs);
     if (st) return st;
-    std::vector<int64_t> offs;
     TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
     E.launch_prep((int)slots.size(), max_n);
     st = E.run(slots, o.hr, 100000, steps_out);
     TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    if (st == TBR_OK) st = E.ensure_stage(sizeof(FrameResult) * slots.size() + 256);
     if (st == TBR_OK) {
         res.resize(fr.size());
         FrameResult *hres = (FrameResult *)E.h_stage;
         for (size_t i = 0; i < slots.size(); ++i)
             TBR_CUDA(cudaMemcpyAsync(hres + i, E.P.results + slots[i], sizeof(FrameResult),
                                      cudaMemcpyDeviceToHost, E.stream));
-        // inlier masks go straight into the caller's buffers (pageable: copied synchronously
-        // with respect to the stream by the driver)
-        FrameDev fd;
-        for (size_t i = 0; i < slots.size(); ++i) {
-            if (i < masks.size() && masks[i]) {
-                TBR_CUDA(cudaMemcpyAsync(&fd, E.P.frames + slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream));
-                TBR_CUDA(cudaStreamSynchronize(E.stream));
-                TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + fd.blk_off * kSub, fr[i].n, cudaMemcpyDeviceToHost, E.stream));
-            }
-        }
+        for (size_t i = 0; i < slots.size(); ++i)
+            if (i < masks.size() && masks[i])
+                TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + devs[i].blk_off * kSub, fr[i].n,
+                                         cudaMemcpyDeviceToHost, E.stream));
         TBR_CUDA(cudaStreamSynchronize(E.stream));
         for (size_t i = 0; i < slots.size(); ++i) res[i] = hres[i];
         float ms = 0.f;
         cudaEventElapsedTime(&ms, E.ev0, E.ev1);
         if (ms_out) *ms_out = ms;
     }
-    // release
     cudaStreamSynchronize(E.stream);
-    std::vector<FrameDev> hd(slots.size());
-    for (size_t i = 0; i < slots.size(); ++i)
-        cudaMemcpy(&hd[i], E.P.frames + slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost);
     for (size_t i = 0; i < slots.size(); ++i) {
-        E.blocks.release(hd[i].blk_off, hd[i].n_blocks);
+        E.blocks.release(devs[i].blk_off, devs[i].n_blocks);
         E.free_slots.push_back(slots[i]);
     }
     return st;
