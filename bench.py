@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
+    ap.add_argument("--case", default="", choices=["", "scoring"],
+                    help="scoring: one N=20000 frame, exactly 4096 samples (small case for ncu)")
     return ap.parse_args()
 
 
@@ -98,7 +100,7 @@ class ClockSampler:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(self.gpu), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-i", str(self.gpu), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
         return self
@@ -190,8 +192,32 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_case_scoring(args):
+    """Scoring-bound single frame: N=20000, 15 % inliers, exactly 4096 samples."""
+    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda, scenes
+    f = scenes.scoring_frame(0)
+    ctx = Context(0, 2 << 30)
+    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
+    cam = Camera_cuda(1, 640, 480, list(f.K))
+    ms = []
+    for i in range(args.warmup + args.steps):
+        st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, BundleOptions_cuda(), seed=f.seed,
+                                                   force_samples=4096, hyp_per_thread=args.hr)
+        if i >= args.warmup:
+            ms.append(st.details["gpu_ms"])
+    d = st.details
+    pairs = d["hypotheses"] * f.n
+    print(json.dumps({"case": "scoring", "n": f.n, "samples": d["samples"], "hypotheses": d["hypotheses"],
+                      "pairs": pairs, "gpu_ms_per_call": statistics.mean(ms),
+                      "pairs_per_s_call": pairs / (statistics.mean(ms) / 1000.0)}), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.case == "scoring":
+        run_case_scoring(args)
+        return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -96,6 +96,12 @@ typedef struct tbr_ext_options {
     int64_t replay_count;
     int32_t hyp_per_thread;       /* scoring tile: 0 = auto, else 4 or 8 */
     int32_t chunk_points;         /* scoring tile: 0 = auto, else points per work item */
+    /* Stop rule K = ceil(3 log(1-p) / log(1-w^3)) beyond the int range: the
+     * reference's double->int assignment (turbo_ransac.cu:231) is undefined
+     * there and x86 yields INT_MIN, ending the loop after one round.
+     * 0 (default): saturate -- keep sampling up to the cap; 1: reproduce x86. */
+    int32_t stop_rule_x86_quirk;
+    int32_t reserved;
 } tbr_ext_options;
 
 /* Results of one estimate. The reference returns RansacStats_cuda unfilled except

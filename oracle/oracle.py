@@ -43,7 +43,8 @@ class RansacCfg(C.Structure):
     _fields_ = [("samples_per_round", C.c_int64), ("max_total_samples", C.c_int64),
                 ("success_prob", C.c_double), ("trials_mult", C.c_double),
                 ("force_samples", C.c_int64), ("seed", C.c_uint64),
-                ("replay", C.c_void_p), ("replay_count", C.c_int64), ("threads", C.c_int)]
+                ("replay", C.c_void_p), ("replay_count", C.c_int64), ("threads", C.c_int),
+                ("quirk", C.c_int)]
 
 
 class RansacOut(C.Structure):
@@ -70,8 +71,9 @@ class EstimateInfo(C.Structure):
 
 
 def _cfg(samples_per_round=1000, seed=0, force_samples=0, replay=None, threads=1,
-         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0):
+         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0, quirk=False):
     cfg = RansacCfg()
+    cfg.quirk = int(quirk)
     cfg.samples_per_round = samples_per_round
     cfg.max_total_samples = max_total_samples
     cfg.success_prob = success_prob

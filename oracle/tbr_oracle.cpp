@@ -652,16 +652,22 @@ void lm_impl(const LMProblem &pb, double *q, double *t, const orc_lm_opts &opt, 
     }
 }
 
-// Adaptive-termination sample count (turbo_ransac.cu:223-231). The double is
-// converted to int as the x86 conversion instruction does: out-of-range and
-// NaN give INT_MIN, which makes the round loop stop.
-inline int64_t needed_samples(int64_t inliers, int64_t n, double success_prob, double mult) {
+// Adaptive-termination sample count (turbo_ransac.cu:223-231). Beyond the int
+// range the reference's double->int assignment is undefined; quirk = 1 gives
+// what x86's conversion instruction returns (INT_MIN, which ends the loop),
+// quirk = 0 saturates (no inlier or K >= INT_MAX: keep sampling to the cap).
+inline int64_t needed_samples(int64_t inliers, int64_t n, double success_prob, double mult, int quirk) {
     double log_prob_missing_model = std::log(1.0 - success_prob);
     double inlier_ratio = (double)inliers / (double)n;
     double prob_outlier = 1.0 - std::pow(inlier_ratio, 3);
     double v = std::ceil(log_prob_missing_model / std::log(prob_outlier) * mult);
-    if (!(v >= -2147483648.0 && v < 2147483648.0)) return (int64_t)INT_MIN;
-    return (int64_t)(int)v;
+    if (quirk) {
+        if (!(v >= -2147483648.0 && v < 2147483648.0)) return (int64_t)INT_MIN;
+        return (int64_t)(int)v;
+    }
+    if (inliers <= 0 || !(v == v) || v >= 2147483647.0) return (int64_t)INT_MAX;
+    if (v <= -2147483648.0) return (int64_t)INT_MIN;
+    return (int64_t)v;
 }
 
 template <class F>
@@ -820,7 +826,8 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
         done += cnt;
         ++rounds;
         if (forced) break;
-        int64_t need = needed_samples(out->found ? out->count : 0, n, cfg->success_prob, cfg->trials_mult);
+        int64_t need = needed_samples(out->found ? out->count : 0, n, cfg->success_prob, cfg->trials_mult,
+                                      cfg->quirk);
         if (done > need) stop = true;
     }
     out->samples = done;

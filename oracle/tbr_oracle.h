@@ -67,6 +67,7 @@ typedef struct orc_ransac_cfg {
     const int32_t *replay;      /* optional replayed triples (count*3) */
     int64_t replay_count;
     int threads;                /* worker threads over samples (>=1) */
+    int quirk;                  /* 1: stop rule with the x86 int-conversion result (INT_MIN) */
 } orc_ransac_cfg;
 
 typedef struct orc_ransac_out {

@@ -153,3 +153,19 @@ def test_bundle_adjust_matches_reference_fixture(ctx):
                                      BundleOptions_cuda(loss_scale=float(d[f"scale{k}"])))
         assert quat_angle(pose.q, d[f"q1_{k}"]) < 1e-6
         assert np.abs(pose.t - d[f"t1_{k}"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("quirk", [False, True])
+def test_stop_rule_overflow_modes(ctx, oracle, quirk):
+    """A first round whose best has almost no inliers makes the stop bound
+    overflow int: the x86 quirk stops after one round, the default saturates."""
+    from turboransac_b200 import scenes as sc
+    f = sc.batched_frames(256)[169]
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                               stop_rule_x86_quirk=quirk)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8, quirk=quirk)
+    assert st.details["samples"] == o["info"].ransac.samples
+    assert st.details["best_sample"] == o["info"].ransac.best_sample
+    assert (o["info"].ransac.samples == 1000) == quirk
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6

@@ -118,3 +118,14 @@ def test_live_oracle_vs_reference_harness(oracle, ref_harness):
         a, b = oracle.p3p(x, X), ref_harness.p3p(x, X)
         assert a.shape == b.shape
         np.testing.assert_array_equal(a, b)
+
+
+def test_stop_rule_quirk_vs_saturation(oracle):
+    from turboransac_b200 import scenes
+    f = scenes.batched_frames(256)[223]
+    xn = np.ascontiguousarray(np.stack([(f.uv[:, 0] - f.K[2]) / f.K[0], (f.uv[:, 1] - f.K[3]) / f.K[1]], 1))
+    thr = 4.0 / 525.0
+    q = oracle.ransac(xn, f.xyz, thr * thr, seed=f.seed, samples_per_round=1000, quirk=True, threads=8)
+    s = oracle.ransac(xn, f.xyz, thr * thr, seed=f.seed, samples_per_round=1000, quirk=False, threads=8)
+    assert q["samples"] == 1000 and q["count"] < 10   # INT_MIN ends the loop after one round
+    assert s["samples"] > 1000 and s["count"] > 300   # saturating rule keeps sampling

@@ -43,7 +43,8 @@ class ExtOptionsC(C.Structure):
     _fields_ = [("honor_options", C.c_int32), ("skip_refine", C.c_int32),
                 ("force_samples", C.c_int64), ("max_total_samples", C.c_int64),
                 ("seed", C.c_uint64), ("replay_idx", C.c_void_p), ("replay_count", C.c_int64),
-                ("hyp_per_thread", C.c_int32), ("chunk_points", C.c_int32)]
+                ("hyp_per_thread", C.c_int32), ("chunk_points", C.c_int32),
+                ("stop_rule_x86_quirk", C.c_int32), ("reserved", C.c_int32)]
 
 
 class StatsC(C.Structure):

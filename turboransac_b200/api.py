@@ -170,7 +170,8 @@ class Context:
                                bundle_opt: BundleOptions_cuda | None = None, *, seed: int | None = None,
                                replay=None, force_samples: int = 0, skip_refine: bool = False,
                                honor_options: bool = False, hyp_per_thread: int = 0,
-                               chunk_points: int = 0, max_total_samples: int = 0):
+                               chunk_points: int = 0, max_total_samples: int = 0,
+                               stop_rule_x86_quirk: bool = False):
         """Returns (RansacStats_cuda, CameraPose_cuda, inliers uint8[N])."""
         x = _f64(points2D, 2)
         X = _f64(points3D, 3)
@@ -186,6 +187,7 @@ class Context:
         ext.seed = (seed or 0) & 0xFFFFFFFFFFFFFFFF
         ext.hyp_per_thread = hyp_per_thread
         ext.chunk_points = chunk_points
+        ext.stop_rule_x86_quirk = int(stop_rule_x86_quirk)
         rep = None
         if replay is not None:
             rep = np.ascontiguousarray(np.asarray(replay, np.int32).reshape(-1, 3))

@@ -107,6 +107,7 @@ struct RunOptions {
     double success_prob = 0.9999;
     double trials_mult = 3.0;
     int skip_refine = 0;
+    int quirk = 0;
     int hr = 8;
     int chunk_points = 0;
     // LM (compat: default BundleOptions_cuda with loss_scale = 1/f)
@@ -123,6 +124,7 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
     const bool honor = ext && ext->honor_options;
     if (ext) {
         o.skip_refine = ext->skip_refine;
+        o.quirk = ext->stop_rule_x86_quirk;
         o.force_samples = ext->force_samples;
         if (ext->max_total_samples > 0) o.max_total = ext->max_total_samples;
         if (ext->hyp_per_thread == 4 || ext->hyp_per_thread == 8) o.hr = ext->hyp_per_thread;
@@ -315,6 +317,7 @@ class Engine {
         f.log_missing = std::log(1.0 - o.success_prob);
         f.trials_mult = o.trials_mult;
         f.skip_refine = o.skip_refine;
+        f.quirk = o.quirk;
         f.hr = o.hr;
         f.chunk_points = o.chunk_points;
         f.lm_max_iter = o.lm_max_iter;
@@ -359,7 +362,7 @@ class Engine {
         beg(6); k_rescore<<<rescore_grid, 256, 0, stream>>>(Q); end(6);
         beg(7); k_finalize<<<n_active, 256, 0, stream>>>(Q); end(7);
         beg(8); k_inliers<<<n_active, 1024, 0, stream>>>(Q); end(8);
-        beg(9); k_lm<<<n_active, kLMThreads, 0, stream>>>(Q); end(9);
+        beg(9); k_lm<<<n_active * kLMCluster, kLMThreads, 0, stream>>>(Q); end(9);
     }
 
     void launch_prep(const Pools &Q, int n_active, int64_t max_n) {
@@ -756,7 +759,7 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (n + 1023) / 1024));
     k_prep_bounds<<<dim3(bx, 1), 256, 0, E.stream>>>(E.P);
     k_lm_pack<<<bx, 256, 0, E.stream>>>(E.P);
-    k_lm<<<1, kLMThreads, 0, E.stream>>>(E.P);
+    k_lm<<<kLMCluster, kLMThreads, 0, E.stream>>>(E.P);
     st = TBR_OK;
     if (cudaGetLastError() != cudaSuccess) st = fail(TBR_ERR_CUDA, "bundle_adjust launch failed");
     FrameResult res;

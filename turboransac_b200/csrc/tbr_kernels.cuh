@@ -16,6 +16,7 @@
 
 #include <cfloat>
 #include <climits>
+#include <cooperative_groups.h>
 #include <cstdint>
 
 #include "tbr_device.cuh"
@@ -84,6 +85,7 @@ struct __align__(16) FrameDev {
     int64_t force_samples;
     double log_missing, trials_mult;
     int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass
+    int32_t quirk, pad1;      // stop rule: 1 = x86 int-conversion quirk of the reference  // hr: hypotheses per lane in the scoring pass
     int64_t lm_max_iter;
     double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
     double lm_inv_sq_thr, lm_grad_tol, lm_step_tol, lm_lambda0, lm_min_lambda, lm_max_lambda;
@@ -152,15 +154,25 @@ struct Pools {
 };
 
 // ------------------------------------------------------------- helpers -----
+// Samples the stop rule requires (turbo_ransac.cu:223-231):
+//   K = ceil(log(1 - p) / log(1 - w^3) * mult),  w = best inlier count / n.
+// The reference assigns K to an int; for K beyond the int range (w below about
+// 0.0024, or no inlier at all) that conversion is undefined behaviour, which
+// x86 resolves to INT_MIN and the round loop stops after its first round.
+// quirk = 1 reproduces that; quirk = 0 (default) saturates, so a frame without
+// a usable model keeps sampling up to the sample cap.
 __device__ __forceinline__ int64_t needed_samples(int64_t inliers, int64_t n, double log_missing,
-                                                  double mult) {
-    // turbo_ransac.cu:223-231; the int conversion behaves like x86 cvttsd2si:
-    // NaN and out-of-range values give INT_MIN, which ends the round loop.
+                                                  double mult, int quirk) {
     const double w = (double)inliers / (double)n;
     const double prob_outlier = 1.0 - pow(w, 3.0);
     const double v = ceil(log_missing / log(prob_outlier) * mult);
-    if (!(v >= -2147483648.0 && v < 2147483648.0)) return (int64_t)INT_MIN;
-    return (int64_t)(int)v;
+    if (quirk) {
+        if (!(v >= -2147483648.0 && v < 2147483648.0)) return (int64_t)INT_MIN;
+        return (int64_t)(int)v;
+    }
+    if (inliers <= 0 || !(v == v) || v >= 2147483647.0) return (int64_t)INT_MAX;
+    if (v <= -2147483648.0) return (int64_t)INT_MIN;
+    return (int64_t)v;
 }
 
 template <typename T>
@@ -315,7 +327,7 @@ __global__ void k_plan(Pools P) {
                 int64_t r = 1;
                 if (f->rounds_done > 0) {
                     const int64_t need = needed_samples(f->found ? f->best_count : 0, f->n,
-                                                        f->log_missing, f->trials_mult);
+                                                        f->log_missing, f->trials_mult, f->quirk);
                     r = need / f->B + 1 - f->rounds_done;
                     if (need < 0 || r < 1) r = 1;
                 }
@@ -921,7 +933,7 @@ __global__ void __launch_bounds__(256) k_finalize(Pools P) {
         }
         if (forced) continue;
         const int64_t after = f.step_first + (r + 1) * f.B;
-        const int64_t need = needed_samples(f.found ? f.best_count : 0, f.n, f.log_missing, f.trials_mult);
+        const int64_t need = needed_samples(f.found ? f.best_count : 0, f.n, f.log_missing, f.trials_mult, f.quirk);
         if (after > need || after >= f.max_total) {
             stop = true;
             r_end = r + 1;
@@ -1023,9 +1035,10 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
     s = t;
 }
 
-// Block-wide FP64 sum of NV values per thread into out[] (thread 0 gets them).
+// Block-wide FP64 sum of NV values per thread; every thread gets the result in
+// out[] (shared). Uses 32*NV doubles of scratch.
 template <int NV>
-__device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch /*32*NV*/, double *out) {
+__device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, double *out) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
@@ -1041,11 +1054,24 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch /*3
     __syncthreads();
 }
 
-// FP64 Cauchy cost of (q, t) over the compacted inliers (jaco.cuh:31-104).
-__device__ double lm_cost(const Pools &P, int64_t base, int64_t n, const double *q, const double *t,
-                          const double *cam, double inv_sq_thr, double *scratch, double *red) {
+constexpr int kLMCluster = 8;  // CTAs cooperating on one frame's LM
+
+// Shared state of one LM cluster. Rank 0 owns the solver state; the other
+// ranks read it through distributed shared memory after each cluster barrier.
+struct LMShared {
+    double part[28];        // this CTA's partial sums (27 accumulators, or the cost in [0])
+    double q[4], t[3], qn[4], tn[3];
+    double cost, lambda;
+    double J[36], g[6];
+    int brk, recompute, iters, invalid;
+};
+
+// FP64 Cauchy cost of (q, t) over inliers [i0, i1) (jaco.cuh:31-104).
+__device__ double lm_cost_slice(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q,
+                                const double *t, const double *cam, double inv_sq_thr, double *scratch,
+                                double *red) {
     double acc[1] = {0.0};
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int64_t o = base + i;
         double Z[3];
         quat_rotate(q, P.lX64[3 * o], P.lX64[3 * o + 1], P.lX64[3 * o + 2], Z);
@@ -1067,49 +1093,64 @@ __device__ double lm_cost(const Pools &P, int64_t base, int64_t n, const double 
 
 // Levenberg-Marquardt with the control flow of lm.cuh:15-171 (damping, accept
 // rule, lambda schedule, the removal of damping after a rejected step, and both
-// stop tests). J^T W J (lower triangle, jaco.cuh:173-200) and J^T W r
+// stop tests), one frame per cluster of kLMCluster CTAs, each owning a slice of
+// the inliers. J^T W J (lower triangle, jaco.cuh:173-200) and J^T W r
 // (:202-209) are accumulated per thread in FP32 with Kahan compensation from
-// centred coordinates, then summed across the block in FP64; the 6x6 Cholesky
-// (lm_utils.cuh:14-100), the step and the cost used for acceptance are FP64.
-__global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
+// centred coordinates and summed across the block and cluster in FP64 in a
+// fixed order; the 6x6 Cholesky (lm_utils.cuh:14-100), the step and the cost
+// used for acceptance are FP64.
+__global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads) k_lm(Pools P) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
     __shared__ double scratch[32 * 27];
     __shared__ double red[27];
-    __shared__ double sJ[36], sg[6], q[4], t[3], qn[4], tn[3];
+    __shared__ LMShared S;
     __shared__ float R32[9], tc32[3];
-    __shared__ double cost, cost_new, lambda, grad_norm, step_norm;
-    __shared__ int brk, recompute, iters, invalid;
-    const int slot = P.active[blockIdx.x];
+    const int rank = (int)cluster.block_rank();
+    const int slot = P.active[blockIdx.x / kLMCluster];
     FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending) return;
+    if (f.status != kLMPending) return;  // uniform across the cluster
+    LMShared *L0 = cluster.map_shared_rank(&S, 0);
     FrameResult &res = P.results[slot];
     const int64_t base = f.blk_off * kSub;
     const int64_t n = f.num_inliers;
+    const int64_t i0 = n * rank / kLMCluster, i1 = n * (rank + 1) / kLMCluster;
     const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
     const float camf[4] = {(float)cam[0], (float)cam[1], (float)cam[2], (float)cam[3]};
     const double inv_sq_thr = f.lm_inv_sq_thr;
     const float inv_sq_thr_f = (float)inv_sq_thr;
+    const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
+    __shared__ double q[4], t[3], qn[4], tn[3];
     if (threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) q[k] = res.q[k];
         for (int k = 0; k < 3; ++k) t[k] = res.t[k];
     }
     __syncthreads();
-    double c0 = 0.0;
-    if (!f.skip_refine) c0 = lm_cost(P, base, n, q, t, cam, inv_sq_thr, scratch, red);
-    if (threadIdx.x == 0) {
-        cost = c0;
-        lambda = f.lm_lambda0;
-        recompute = 1;
-        iters = 0;
-        invalid = 0;
-        res.lm_cost0 = c0;
+    // initial cost
+    double c = 0.0;
+    if (max_it > 0) c = lm_cost_slice(P, base, i0, i1, q, t, cam, inv_sq_thr, scratch, red);
+    if (threadIdx.x == 0) S.part[0] = c;
+    cluster.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int r = 0; r < kLMCluster; ++r) tot += cluster.map_shared_rank(&S, r)->part[0];
+        S.cost = tot;
+        S.lambda = f.lm_lambda0;
+        S.recompute = 1;
+        S.iters = 0;
+        S.invalid = 0;
+        S.brk = 0;
+        for (int k = 0; k < 4; ++k) S.q[k] = q[k];
+        for (int k = 0; k < 3; ++k) S.t[k] = t[k];
+        res.lm_cost0 = tot;
     }
-    __syncthreads();
-    const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
+    cluster.sync();
     for (int64_t it = 0; it < max_it; ++it) {
-        if (threadIdx.x == 0) brk = 0;
-        if (recompute) {
+        if (L0->recompute) {
             if (threadIdx.x == 0) {
                 double R[9];
+                for (int k = 0; k < 4; ++k) q[k] = L0->q[k];
+                for (int k = 0; k < 3; ++k) t[k] = L0->t[k];
                 quat_to_rotmat(q, R);
                 for (int k = 0; k < 9; ++k) R32[k] = (float)R[k];
                 for (int r = 0; r < 3; ++r)
@@ -1117,16 +1158,17 @@ __global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
                                       R[3 * r + 2] * f.centre[2]);
             }
             __syncthreads();
-            float S[27], Cc[27];
+            float Sv[27], Cc[27];
 #pragma unroll
-            for (int k = 0; k < 27; ++k) S[k] = Cc[k] = 0.0f;
+            for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
             const float r00 = R32[0], r01 = R32[1], r02 = R32[2], r10 = R32[3], r11 = R32[4], r12 = R32[5],
                         r20 = R32[6], r21 = R32[7], r22 = R32[8];
-            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            const float t0 = tc32[0], t1 = tc32[1], t2 = tc32[2];
+            for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
                 const float4 A = P.lA32[base + i], Bw = P.lB32[base + i];
-                const float Z0 = r00 * A.x + r01 * A.y + r02 * A.z + tc32[0];
-                const float Z1 = r10 * A.x + r11 * A.y + r12 * A.z + tc32[1];
-                const float Z2 = r20 * A.x + r21 * A.y + r22 * A.z + tc32[2];
+                const float Z0 = r00 * A.x + r01 * A.y + r02 * A.z + t0;
+                const float Z1 = r10 * A.x + r11 * A.y + r12 * A.z + t1;
+                const float Z2 = r20 * A.x + r21 * A.y + r22 * A.z + t2;
                 const float iz = 1.0f / Z2;
                 const float z0 = Z0 * iz, z1 = Z1 * iz;
                 const float rx = (camf[0] * z0 + camf[2]) - A.w;
@@ -1147,6 +1189,7 @@ __global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
                 const float d21 = wv * (dZ02 * dZ01 + dZ12 * dZ11);
                 const float d22 = wv * (dZ02 * dZ02 + dZ12 * dZ12);
                 const float X0 = Bw.x, X1 = Bw.y, X2 = Bw.z;
+                const float wx = wv * rx, wy = wv * ry;
                 const float v[27] = {
                     X2 * (X2 * d11 - X1 * d21) + X1 * (X1 * d22 - X2 * d21),
                     -X2 * (X2 * d10 - X0 * d21) - X1 * (X0 * d22 - X2 * d20),
@@ -1164,102 +1207,117 @@ __global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
                     X0 * d11 - X1 * d10,
                     X0 * d21 - X1 * d20,
                     d00, d10, d20, d11, d21, d22,
-                    (wv * rx) * (X1 * dZ02 - X2 * dZ01) + (wv * ry) * (X1 * dZ12 - X2 * dZ11),
-                    -(wv * rx) * (X0 * dZ02 - X2 * dZ00) - (wv * ry) * (X0 * dZ12 - X2 * dZ10),
-                    (wv * rx) * (X0 * dZ01 - X1 * dZ00) + (wv * ry) * (X0 * dZ11 - X1 * dZ10),
-                    dZ00 * (wv * rx) + dZ10 * (wv * ry),
-                    dZ01 * (wv * rx) + dZ11 * (wv * ry),
-                    dZ02 * (wv * rx) + dZ12 * (wv * ry)};
+                    wx * (X1 * dZ02 - X2 * dZ01) + wy * (X1 * dZ12 - X2 * dZ11),
+                    -wx * (X0 * dZ02 - X2 * dZ00) - wy * (X0 * dZ12 - X2 * dZ10),
+                    wx * (X0 * dZ01 - X1 * dZ00) + wy * (X0 * dZ11 - X1 * dZ10),
+                    dZ00 * wx + dZ10 * wy,
+                    dZ01 * wx + dZ11 * wy,
+                    dZ02 * wx + dZ12 * wy};
 #pragma unroll
-                for (int k = 0; k < 27; ++k) kahan_add(S[k], Cc[k], v[k]);
+                for (int k = 0; k < 27; ++k) kahan_add(Sv[k], Cc[k], v[k]);
             }
             double dv[27];
 #pragma unroll
-            for (int k = 0; k < 27; ++k) dv[k] = (double)S[k] - (double)Cc[k];
+            for (int k = 0; k < 27; ++k) dv[k] = (double)Sv[k] - (double)Cc[k];
             block_sum_d<27>(dv, scratch, red);
-            if (threadIdx.x == 0) {
-                // lower triangle in the reference's order: (0,0),(1,0)..(5,0),(1,1)..(5,1),...
+            if (threadIdx.x < 27) S.part[threadIdx.x] = red[threadIdx.x];
+            cluster.sync();
+            if (rank == 0 && threadIdx.x == 0) {
+                double tot[27];
+                for (int k = 0; k < 27; ++k) tot[k] = 0.0;
+                for (int r = 0; r < kLMCluster; ++r) {
+                    const LMShared *Sr = cluster.map_shared_rank(&S, r);
+                    for (int k = 0; k < 27; ++k) tot[k] += Sr->part[k];
+                }
+                // lower triangle in the reference's order (0,0),(1,0)..(5,0),(1,1)..(5,1),...
                 const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
                                         {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
                                         {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
-                for (int k = 0; k < 36; ++k) sJ[k] = 0.0;
-                for (int k = 0; k < 21; ++k) sJ[idx[k][0] * 6 + idx[k][1]] = red[k];
+                for (int k = 0; k < 36; ++k) S.J[k] = 0.0;
+                for (int k = 0; k < 21; ++k) S.J[idx[k][0] * 6 + idx[k][1]] = tot[k];
                 double gn = 0.0;
                 for (int k = 0; k < 6; ++k) {
-                    sg[k] = red[21 + k];
-                    gn += sg[k] * sg[k];
+                    S.g[k] = tot[21 + k];
+                    gn += S.g[k] * S.g[k];
                 }
-                grad_norm = sqrt(gn);
-                if (grad_norm < f.lm_grad_tol) brk = 1;
+                S.brk = sqrt(gn) < f.lm_grad_tol ? 1 : 0;
             }
-            __syncthreads();
+        } else if (rank == 0 && threadIdx.x == 0) {
+            S.brk = 0;
         }
-        if (threadIdx.x == 0) {
-            for (int k = 0; k < 6; ++k) sJ[k * 7] += lambda;
-            // Cholesky solve (lm_utils.cuh:14-100), then the step (jaco.cuh:288-299).
-            double L[36];
-            for (int k = 0; k < 36; ++k) L[k] = 0.0;
+        if (rank == 0 && threadIdx.x == 0) {
+            for (int k = 0; k < 6; ++k) S.J[k * 7] += S.lambda;
+            double Lc[36];
+            for (int k = 0; k < 36; ++k) Lc[k] = 0.0;
             for (int i = 0; i < 6; ++i)
                 for (int j = 0; j <= i; ++j) {
                     double sum = 0.0;
-                    for (int k = 0; k < j; ++k) sum += L[i * 6 + k] * L[j * 6 + k];
+                    for (int k = 0; k < j; ++k) sum += Lc[i * 6 + k] * Lc[j * 6 + k];
                     if (i == j) {
-                        double val = sJ[i * 6 + i] - sum;
+                        double val = S.J[i * 6 + i] - sum;
                         if (val <= 0.0) val = 1e-15;
-                        L[i * 6 + j] = sqrt(val);
+                        Lc[i * 6 + j] = sqrt(val);
                     } else {
-                        L[i * 6 + j] = (sJ[i * 6 + j] - sum) / L[j * 6 + j];
+                        Lc[i * 6 + j] = (S.J[i * 6 + j] - sum) / Lc[j * 6 + j];
                     }
                 }
             double y[6], x[6];
             for (int i = 0; i < 6; ++i) {
                 double sum = 0.0;
-                for (int j = 0; j < i; ++j) sum += L[i * 6 + j] * y[j];
-                y[i] = (sg[i] - sum) / L[i * 6 + i];
+                for (int j = 0; j < i; ++j) sum += Lc[i * 6 + j] * y[j];
+                y[i] = (S.g[i] - sum) / Lc[i * 6 + i];
             }
             for (int i = 5; i >= 0; --i) {
                 double sum = 0.0;
-                for (int j = i + 1; j < 6; ++j) sum += L[j * 6 + i] * x[j];
-                x[i] = (y[i] - sum) / L[i * 6 + i];
+                for (int j = i + 1; j < 6; ++j) sum += Lc[j * 6 + i] * x[j];
+                x[i] = (y[i] - sum) / Lc[i * 6 + i];
             }
             double sn = 0.0;
             for (int k = 0; k < 6; ++k) {
                 x[k] = -1 * x[k];
                 sn += x[k] * x[k];
             }
-            step_norm = sqrt(sn);
-            if (step_norm < f.lm_step_tol) brk = 1;
-            quat_step_post(q, x, qn);
+            if (sqrt(sn) < f.lm_step_tol) S.brk = 1;
+            quat_step_post(S.q, x, S.qn);
             double dt[3];
-            quat_rotate(q, x[3], x[4], x[5], dt);
-            for (int k = 0; k < 3; ++k) tn[k] = t[k] + dt[k];
+            quat_rotate(S.q, x[3], x[4], x[5], dt);
+            for (int k = 0; k < 3; ++k) S.tn[k] = S.t[k] + dt[k];
         }
-        __syncthreads();
-        if (brk) break;
-        const double cn = lm_cost(P, base, n, qn, tn, cam, inv_sq_thr, scratch, red);
+        cluster.sync();
+        if (L0->brk) break;
         if (threadIdx.x == 0) {
-            if (cn < cost) {
-                for (int k = 0; k < 4; ++k) q[k] = qn[k];
-                for (int k = 0; k < 3; ++k) t[k] = tn[k];
-                lambda = fmax(f.lm_min_lambda, lambda / 10);
-                cost = cn;
-                recompute = 1;
-            } else {
-                ++invalid;
-                for (int k = 0; k < 6; ++k) sJ[k * 7] -= lambda;
-                lambda = fmin(f.lm_max_lambda, lambda * 10);
-                recompute = 0;
-            }
-            ++iters;
+            for (int k = 0; k < 4; ++k) qn[k] = L0->qn[k];
+            for (int k = 0; k < 3; ++k) tn[k] = L0->tn[k];
         }
         __syncthreads();
+        const double cs = lm_cost_slice(P, base, i0, i1, qn, tn, cam, inv_sq_thr, scratch, red);
+        if (threadIdx.x == 0) S.part[0] = cs;
+        cluster.sync();
+        if (rank == 0 && threadIdx.x == 0) {
+            double cn = 0.0;
+            for (int r = 0; r < kLMCluster; ++r) cn += cluster.map_shared_rank(&S, r)->part[0];
+            if (cn < S.cost) {
+                for (int k = 0; k < 4; ++k) S.q[k] = S.qn[k];
+                for (int k = 0; k < 3; ++k) S.t[k] = S.tn[k];
+                S.lambda = fmax(f.lm_min_lambda, S.lambda / 10);
+                S.cost = cn;
+                S.recompute = 1;
+            } else {
+                ++S.invalid;
+                for (int k = 0; k < 6; ++k) S.J[k * 7] -= S.lambda;
+                S.lambda = fmin(f.lm_max_lambda, S.lambda * 10);
+                S.recompute = 0;
+            }
+            ++S.iters;
+        }
+        cluster.sync();
     }
-    if (threadIdx.x == 0) {
-        for (int k = 0; k < 4; ++k) res.q[k] = q[k];
-        for (int k = 0; k < 3; ++k) res.t[k] = t[k];
-        res.lm_iters = iters;
-        res.lm_invalid = invalid;
-        res.lm_cost = cost;
+    if (rank == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) res.q[k] = S.q[k];
+        for (int k = 0; k < 3; ++k) res.t[k] = S.t[k];
+        res.lm_iters = S.iters;
+        res.lm_invalid = S.invalid;
+        res.lm_cost = S.cost;
         res.samples = f.samples_done;
         res.rounds = f.rounds_done;
         res.hypotheses = f.hyps_done;
@@ -1272,8 +1330,9 @@ __global__ void __launch_bounds__(kLMThreads) k_lm(Pools P) {
         res.rescored = f.rescored;
         res.overflow = f.overflow;
         res.status = kDone;
-        f.status = kDone;
     }
+    cluster.sync();  // no CTA leaves while rank 0 may still read its shared memory
+    if (rank == 0 && threadIdx.x == 0) f.status = kDone;
 }
 
 // ----------------------------------------------------------- loop control --
