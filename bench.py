@@ -162,6 +162,85 @@ def cpu_baseline(frames, seconds_target=15.0):
             "seconds": dt}
 
 
+def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
+    """Config 4: Poisson stream of independent frames (N log-uniform [300, 50000],
+    inlier ratio U[0.05, 0.70], 1 px noise) through the continuous-batching server."""
+    import threading
+
+    import numpy as np
+
+    from turboransac_b200 import Server, scenes
+    reqs = [scenes.serving_request(i) for i in range(pool)]
+    arrivals = scenes.poisson_arrivals(rate, seconds, seed=11)
+    srv = Server(ctx, budget_bytes=budget, max_slots=1024)
+    # warm the server (first steps pay one-time costs)
+    for r in reqs[:32]:
+        srv.submit(r)
+    srv.drain()
+    srv.poll()
+    done, lock = {}, threading.Lock()
+    stop = threading.Event()
+
+    def poller():
+        while not stop.is_set():
+            got = srv.poll()
+            if got:
+                t = time.perf_counter()
+                with lock:
+                    for g in got:
+                        done[g["id"]] = (g, t)
+            else:
+                time.sleep(0.0005)
+
+    th = threading.Thread(target=poller, daemon=True)
+    th.start()
+    ids = {}
+    t0 = time.perf_counter()
+    for k, ta in enumerate(arrivals):
+        while True:
+            dt = t0 + ta - time.perf_counter()
+            if dt <= 0:
+                break
+            time.sleep(min(dt, 0.001))
+        ids[srv.submit(reqs[k % pool])] = k % pool
+    srv.drain()
+    t_end = time.perf_counter()
+    time.sleep(0.01)
+    stop.set()
+    th.join()
+    for g in srv.poll():
+        done[g["id"]] = (g, t_end)
+    srv.close()
+    lat = np.array([g["latency_ms"] for g, _ in done.values()])
+    ok = 0
+    for rid, (g, _) in done.items():
+        f = reqs[ids[rid]]
+        ae, te = scenes.pose_error(scenes.quat_to_rotmat(g["q"]), g["t"], f.R_gt, f.t_gt)
+        ok += (g["status"] == 0 and ae < 5.0 and te < 5.0)
+    last = max(t for _, t in done.values())
+    return {"offered_rate_hz": rate, "seconds": seconds, "requests": len(arrivals), "completed": len(done),
+            "throughput_fps": len(done) / (last - t0), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "p999_ms": float(np.percentile(lat, 99.9)),
+            "success_rate": ok / max(len(done), 1), "budget_bytes": budget,
+            "workload": "N log-uniform [300,50000], w U[0.05,0.70], sigma 1 px, Poisson arrivals"}, reqs
+
+
+def run_plain_serving(ctx, reqs, count=200):
+    """The reference's calling pattern on the serving distribution: synchronous plain calls."""
+    import numpy as np
+
+    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, RansacOptions_cuda
+    ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
+    lat = []
+    for f in reqs[:count]:
+        t0 = time.perf_counter()
+        ctx.estimate_absolute_pose(f.uv, f.xyz, Camera_cuda(1, 640, 480, list(f.K)), ro, BundleOptions_cuda(),
+                                   seed=f.seed)
+        lat.append(1000.0 * (time.perf_counter() - t0))
+    return {"frames_per_s": len(lat) / (sum(lat) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU implementation of the path on the host cores."""
     if rank != 0:
@@ -309,6 +388,14 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(frames)
 
+    serving = None
+    if args.serve_seconds > 0:
+        serving, reqs = run_serving(ctx, args.serve_seconds)
+        serving["plain_call"] = run_plain_serving(ctx, reqs)
+        serving["throughput_vs_plain"] = serving["throughput_fps"] / serving["plain_call"]["frames_per_s"]
+        print(f"[bench] serving: {serving['throughput_fps']:.0f} frames/s p50 {serving['p50_ms']:.2f} ms "
+              f"p99 {serving['p99_ms']:.2f} ms success {serving['success_rate']:.4f}", file=sys.stderr, flush=True)
+
     if rank == 0:
         clocks = clk.summary()
         line = {
@@ -331,6 +418,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "plain_call": plain,
+            "serving": serving,
             "speedup_vs_plain": (value / plain["frames_per_s"]) if plain else None,
             "gpu_launches": args.steps * (1 + 11 * steps_per_run),
             "clocks": clocks,

@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from ._lib import TbrError, check
 
-__all__ = ["Batch", "estimate_batch", "RansacOptions_cuda", "BundleOptions_cuda", "RansacStats_cuda", "Camera_cuda",
+__all__ = ["Batch", "Server", "estimate_batch", "RansacOptions_cuda", "BundleOptions_cuda", "RansacStats_cuda", "Camera_cuda",
            "CameraPose_cuda", "Context", "estimate_absolute_pose_cuda", "get_inliers_mx",
            "bundle_adjust_cuda", "TbrError"]
 
@@ -386,3 +386,56 @@ def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None =
         for o, m in zip(out, mbufs):
             o["inliers"] = m
     return out
+
+
+class Server:
+    """Continuous-batching request loop (tbr_server_*): submit frames any time;
+    a worker advances every resident frame one engine step at a time and admits
+    new requests into free slots within the workspace budget."""
+
+    def __init__(self, ctx: Context, budget_bytes: int = 8 << 30, max_slots: int = 512, max_queue: int = 1 << 16,
+                 ransac_opt: RansacOptions_cuda | None = None):
+        cfg = _lib.ServerConfigC()
+        cfg.workspace_budget_bytes = budget_bytes
+        cfg.max_slots = max_slots
+        cfg.max_queue = max_queue
+        cfg.ransac = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+        h = C.c_void_p()
+        check(_lib.lib().tbr_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._buf = (_lib.ServerResultC * 1024)()
+
+    def submit(self, frame, seed: int | None = None, max_reproj_error: float = 0.0) -> int:
+        arr, keep = _frame_descs([frame], None if seed is None else [seed], max_reproj_error)
+        rid = C.c_uint64()
+        check(_lib.lib().tbr_server_submit(self._h, arr, C.byref(rid)))
+        return rid.value
+
+    def poll(self, max_results: int = 1024):
+        n = C.c_int32()
+        st = _lib.lib().tbr_server_poll(self._h, self._buf, min(max_results, 1024), C.byref(n))
+        if st not in (0, 6):
+            check(st)
+        out = []
+        for i in range(n.value):
+            r = self._buf[i]
+            out.append({"id": r.request_id, "status": r.status, "q": np.array(r.q[:]), "t": np.array(r.t[:]),
+                        "latency_ms": r.submit_to_done_ms, **r.stats.as_dict()})
+        return out
+
+    def cancel(self, request_id: int):
+        check(_lib.lib().tbr_server_cancel(self._h, request_id))
+
+    def drain(self):
+        check(_lib.lib().tbr_server_drain(self._h))
+
+    def close(self):
+        if self._h:
+            _lib.lib().tbr_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

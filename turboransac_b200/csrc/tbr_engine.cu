@@ -110,6 +110,7 @@ struct RunOptions {
     int quirk = 0;
     int hr = 8;
     int chunk_points = 0;
+    int max_rounds_step = 0;
     // LM (compat: default BundleOptions_cuda with loss_scale = 1/f)
     int64_t lm_max_iter = 100;
     double lm_loss_scale_px = 1.0;  // loss scale in pixels (multiplied by 1/f)
@@ -168,6 +169,8 @@ class Engine {
     int score_grid[2] = {0, 0};
     int rescore_grid = 0, p3p_grid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::mutex mu;  // one call at a time per context
 
     ~Engine() {
@@ -178,6 +181,9 @@ class Engine {
         if (d_replay) cudaFree(d_replay);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -188,6 +194,9 @@ class Engine {
         TBR_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         TBR_CUDA(cudaEventCreate(&ev0));
         TBR_CUDA(cudaEventCreate(&ev1));
+        TBR_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
         // Split: 30 % hypotheses, the rest points, after the per-frame state.
@@ -320,6 +329,7 @@ class Engine {
         f.quirk = o.quirk;
         f.hr = o.hr;
         f.chunk_points = o.chunk_points;
+        f.max_rounds_step = o.max_rounds_step;
         f.lm_max_iter = o.lm_max_iter;
         const double sc = 1.0 / f.focal;  // entry.cu:87,107-114: LM in pixel/f units
         for (int k = 0; k < 4; ++k) f.lm_cam[k] = fh.K[k] * sc;
@@ -347,22 +357,37 @@ class Engine {
     static constexpr const char *kKernelNames[12] = {"k_plan", "k_sample_p3p", "k_score_plan", "k_score",
                                                      "k_select", "k_rescore_plan", "k_rescore", "k_finalize",
                                                      "k_inliers", "k_lm", "k_prep", "unused"};
-    void launch_step(const Pools &Q, int n_active, int hr, Profile *prof = nullptr) {
-        auto beg = [&](int k) { if (prof) cudaEventRecord(prof->ev[2 * k], stream); };
-        auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], stream); prof->launches[k]++; } };
-        beg(0); k_plan<<<1, kMaxActive, 0, stream>>>(Q); end(0);
-        beg(1); k_sample_p3p<<<p3p_grid, 128, 0, stream>>>(Q); end(1);
-        beg(2); k_score_plan<<<1, kMaxActive, 0, stream>>>(Q); end(2);
+    // RANSAC part of a step (plan .. finalize).
+    void launch_ransac(const Pools &Q, int n_active, int hr, cudaStream_t st, Profile *prof = nullptr) {
+        auto beg = [&](int k) { if (prof) cudaEventRecord(prof->ev[2 * k], st); };
+        auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
+        beg(0); k_plan<<<1, kMaxActive, 0, st>>>(Q); end(0);
+        beg(1); k_sample_p3p<<<p3p_grid, 128, 0, st>>>(Q); end(1);
+        beg(2); k_score_plan<<<1, kMaxActive, 0, st>>>(Q); end(2);
         beg(3);
-        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, stream>>>(Q);
-        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, stream>>>(Q);
+        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, st>>>(Q);
+        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, st>>>(Q);
         end(3);
-        beg(4); k_select<<<n_active, 256, 0, stream>>>(Q); end(4);
-        beg(5); k_rescore_plan<<<1, kMaxActive, 0, stream>>>(Q); end(5);
-        beg(6); k_rescore<<<rescore_grid, 256, 0, stream>>>(Q); end(6);
-        beg(7); k_finalize<<<n_active, 256, 0, stream>>>(Q); end(7);
-        beg(8); k_inliers<<<n_active, 1024, 0, stream>>>(Q); end(8);
-        beg(9); k_lm<<<n_active * kLMCluster, kLMThreads, 0, stream>>>(Q); end(9);
+        beg(4); k_select<<<n_active, 256, 0, st>>>(Q); end(4);
+        beg(5); k_rescore_plan<<<1, kMaxActive, 0, st>>>(Q); end(5);
+        beg(6); k_rescore<<<rescore_grid, 256, 0, st>>>(Q); end(6);
+        beg(7); k_finalize<<<n_active, 256, 0, st>>>(Q); end(7);
+    }
+    // Refinement part: inliers + LM of frames whose RANSAC ended in an earlier step.
+    void launch_refine(const Pools &Q, int n_active, cudaStream_t st, Profile *prof = nullptr) {
+        auto beg = [&](int k) { if (prof) cudaEventRecord(prof->ev[2 * k], st); };
+        auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
+        beg(8); k_inliers<<<n_active, 1024, 0, st>>>(Q); end(8);
+        beg(9);
+        k_lm_small<<<n_active, kLMThreads, 0, st>>>(Q);
+        k_lm<<<n_active * kLMCluster, kLMThreads, 0, st>>>(Q);
+        end(9);
+    }
+    // Host-stepped: RANSAC, close the step, refine what finished.
+    void launch_step(const Pools &Q, int n_active, int hr, Profile *prof = nullptr) {
+        launch_ransac(Q, n_active, hr, stream, prof);
+        k_tick<<<1, 1, 0, stream>>>(Q);
+        launch_refine(Q, n_active, stream, prof);
     }
 
     void launch_prep(const Pools &Q, int n_active, int64_t max_n) {
@@ -395,6 +420,7 @@ class Engine {
             if (h_counters[kCStillRansac] == 0) break;
             if (steps >= max_steps) return fail(TBR_ERR_INTERNAL, "step limit reached");
         }
+        TBR_CUDA(cudaStreamSynchronize(stream));
         if (steps_out) *steps_out = steps;
         return TBR_OK;
     }
@@ -740,6 +766,7 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     TBR_CUDA(cudaMemcpyAsync(&fd, E.P.frames + slots[0], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream));
     TBR_CUDA(cudaStreamSynchronize(E.stream));
     fd.status = kLMPending;
+    fd.lm_force_cluster = 1;
     fd.focal = 1.0;
     for (int k = 0; k < 4; ++k) fd.lm_cam[k] = K[k];
     fd.lm_inv_sq_thr = 1.0 / (bo.loss_scale * bo.loss_scale);  // CauchyLoss_cuda(loss_scale)
@@ -899,13 +926,32 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
         body = cp.conditional.phGraph_out[0];
     }
     if (ok) {
+        // Body: RANSAC of this step beside the refinement of frames that
+        // finished in the previous step (disjoint frames), then the loop test.
         ok = cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
              cudaSuccess;
         if (ok) {
-            E.launch_step(b->Q, n_frames, b->o.hr);
+            cudaEventRecord(E.ev_fork, E.stream);
+            cudaStreamWaitEvent(E.stream2, E.ev_fork, 0);
+            E.launch_refine(b->Q, n_frames, E.stream2);
+            E.launch_ransac(b->Q, n_frames, b->o.hr, E.stream);
+            cudaEventRecord(E.ev_join, E.stream2);
+            cudaStreamWaitEvent(E.stream, E.ev_join, 0);
             k_loop_ctl<<<1, 1, 0, E.stream>>>(b->Q, h, 100000ull);
             ok = cudaStreamEndCapture(E.stream, &body) == cudaSuccess;
         }
+    }
+    if (ok) {
+        // After the loop: refinement of the frames that finished in the last step.
+        cudaGraph_t tail = nullptr;
+        ok = cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+        if (ok) {
+            E.launch_refine(b->Q, n_frames, E.stream);
+            ok = cudaStreamEndCapture(E.stream, &tail) == cudaSuccess;
+        }
+        cudaGraphNode_t tail_node;
+        if (ok) ok = cudaGraphAddChildGraphNode(&tail_node, b->graph, &loop_node, 1, tail) == cudaSuccess;
+        if (tail) cudaGraphDestroy(tail);
     }
     if (ok) ok = cudaGraphInstantiate(&b->exec, b->graph, 0) == cudaSuccess;
     if (ok) ok = cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess;
@@ -1010,18 +1056,333 @@ void tbr_batch_destroy(tbr_batch *b) {
     batch_free(b);
 }
 
-tbr_status tbr_server_create(tbr_context *, const tbr_server_config *, tbr_server **) {
-    return fail(TBR_ERR_INTERNAL, "tbr_server_create: not available in this build");
+}  // extern "C"
+
+// --------------------------------------------------------------- serving --
+// Continuous batching. A worker thread owns a dedicated Engine sized by the
+// workspace budget and loops:
+//   1. retire: frames whose LM finished -> results out, slot and blocks freed;
+//   2. admit: queued requests, in arrival order, while a slot and point blocks
+//      are free (the budget is the engine workspace), uploaded and prepared;
+//   3. one engine step over every resident frame (RANSAC of the frames still
+//      sampling, inliers + LM of the frames that finished).
+// A request that arrives while others run therefore joins the next step and
+// its work overlaps theirs on the device.
+struct ServerRequest {
+    uint64_t id;
+    std::vector<double> uv, xyz;
+    double K[4];
+    uint64_t seed;
+    double thr;
+    std::chrono::steady_clock::time_point t_submit;
+    bool cancelled = false;
+};
+
+struct Resident {
+    std::unique_ptr<ServerRequest> req;
+    int slot;
+    int64_t blk_off, n_blocks;
+};
+
+struct tbr_server {
+    Engine E;
+    RunOptions o;
+    tbr_ransac_options ro;
+    int max_queue = 1 << 16;
+    std::mutex mu;
+    std::condition_variable cv, cv_done;
+    std::deque<std::unique_ptr<ServerRequest>> queue;
+    std::vector<Resident> resident;
+    std::vector<tbr_server_result> done;
+    std::vector<uint64_t> cancel_ids;
+    uint64_t next_id = 1;
+    uint64_t in_flight = 0;  // submitted and not yet completed
+    bool stop = false;
+    std::thread worker;
+    int32_t *d_status = nullptr, *h_status = nullptr;
+    int32_t *d_prep = nullptr;
+    tbr_status error = TBR_OK;
+    std::string error_msg;
+};
+
+static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, tbr_status st) {
+    tbr_server_result out;
+    std::memset(&out, 0, sizeof(out));
+    out.request_id = r.req->id;
+    out.status = st;
+    if (res) {
+        for (int k = 0; k < 4; ++k) out.q[k] = res->q[k];
+        for (int k = 0; k < 3; ++k) out.t[k] = res->t[k];
+        fill_stats(*res, (int64_t)(r.req->uv.size() / 2), &out.stats, 0.f);
+    }
+    out.submit_to_done_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r.req->t_submit).count();
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->done.push_back(out);
+    s->in_flight--;
+    s->cv_done.notify_all();
 }
-tbr_status tbr_server_submit(tbr_server *, const tbr_frame_desc *, uint64_t *) {
-    return fail(TBR_ERR_INTERNAL, "not available in this build");
+
+static tbr_status server_step(tbr_server *s) {
+    Engine &E = s->E;
+    // ---- admit ----
+    std::vector<std::unique_ptr<ServerRequest>> newreq;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        while (!s->queue.empty() && (int)newreq.size() < (int)E.free_slots.size()) {
+            auto &q = s->queue.front();
+            if (q->cancelled) {
+                Resident tmp{std::move(q), -1, 0, 0};
+                s->queue.pop_front();
+                s->done.push_back({});
+                auto &o = s->done.back();
+                std::memset(&o, 0, sizeof(o));
+                o.request_id = tmp.req->id;
+                o.status = TBR_ERR_CANCELLED;
+                s->in_flight--;
+                s->cv_done.notify_all();
+                continue;
+            }
+            const int64_t need = (int64_t)(q->uv.size() / 2 + kSub - 1) / kSub;
+            if (E.blocks.capacity() - E.blocks.used() < need) break;  // budget: wait for frames to retire
+            newreq.push_back(std::move(q));
+            s->queue.pop_front();
+        }
+    }
+    if (!newreq.empty()) {
+        std::vector<FrameHost> fh;
+        for (auto &r : newreq)
+            fh.push_back({r->uv.data(), r->xyz.data(), (int64_t)(r->uv.size() / 2), {r->K[0], r->K[1], r->K[2], r->K[3]},
+                          r->seed, r->thr, nullptr, 0});
+        std::vector<int> slots;
+        std::vector<FrameDev> devs;
+        int64_t max_n = 0;
+        tbr_status st = admit_frames(E, fh, s->o, slots, max_n, &devs);
+        if (st == TBR_ERR_OOM) {  // fragmentation: requeue at the front and retry after retirements
+            std::lock_guard<std::mutex> lk(s->mu);
+            for (auto it = newreq.rbegin(); it != newreq.rend(); ++it) s->queue.push_front(std::move(*it));
+            newreq.clear();
+        } else if (st) {
+            return st;
+        } else {
+            // admit_frames wrote the new slots to d_active; prepare them (AABB, packing).
+            cudaMemcpyAsync(s->d_prep, E.d_active, 4 * slots.size(), cudaMemcpyDeviceToDevice, E.stream);
+            Pools Q = E.P;
+            Q.active = s->d_prep;
+            Q.n_active = (int32_t)slots.size();
+            E.launch_prep(Q, (int)slots.size(), max_n);
+            for (size_t i = 0; i < slots.size(); ++i)
+                s->resident.push_back({std::move(newreq[i]), slots[i], devs[i].blk_off, devs[i].n_blocks});
+        }
+    }
+    if (s->resident.empty()) return TBR_OK;
+    // ---- cancels of resident frames: retire them now ----
+    {
+        std::vector<uint64_t> ids;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            ids.swap(s->cancel_ids);
+        }
+        for (uint64_t id : ids)
+            for (size_t i = 0; i < s->resident.size(); ++i)
+                if (s->resident[i].req->id == id) {
+                    TBR_CUDA(cudaStreamSynchronize(E.stream));
+                    server_complete(s, s->resident[i], nullptr, TBR_ERR_CANCELLED);
+                    E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
+                    E.free_slots.push_back(s->resident[i].slot);
+                    s->resident.erase(s->resident.begin() + i);
+                    break;
+                }
+        if (s->resident.empty()) return TBR_OK;
+    }
+    // ---- one step over all resident frames ----
+    const int na = (int)s->resident.size();
+    int32_t *ha = (int32_t *)E.h_stage;
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    tbr_status st = E.ensure_stage(8 * na + 4096);
+    if (st) return st;
+    ha = (int32_t *)E.h_stage;
+    for (int i = 0; i < na; ++i) ha[i] = s->resident[i].slot;
+    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * na, cudaMemcpyHostToDevice, E.stream));
+    E.P.n_active = na;
+    E.launch_step(E.P, na, s->o.hr);
+    k_gather_status<<<(na + 255) / 256, 256, 0, E.stream>>>(E.P, s->d_status);
+    TBR_CUDA(cudaGetLastError());
+    TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    // ---- retire ----
+    std::vector<int> fin;
+    for (int i = 0; i < na; ++i)
+        if (s->h_status[i] == kDone) fin.push_back(i);
+    if (!fin.empty()) {
+        std::vector<FrameResult> res(fin.size());
+        for (size_t k = 0; k < fin.size(); ++k)
+            TBR_CUDA(cudaMemcpyAsync(&res[k], E.P.results + s->resident[fin[k]].slot, sizeof(FrameResult),
+                                     cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaStreamSynchronize(E.stream));
+        for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &res[k], TBR_OK);
+        std::vector<Resident> keep;
+        std::vector<bool> gone(na, false);
+        for (int i : fin) gone[i] = true;
+        for (int i = 0; i < na; ++i) {
+            if (gone[i]) {
+                E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
+                E.free_slots.push_back(s->resident[i].slot);
+            } else {
+                keep.push_back(std::move(s->resident[i]));
+            }
+        }
+        s->resident.swap(keep);
+    }
+    return TBR_OK;
 }
-tbr_status tbr_server_poll(tbr_server *, tbr_server_result *, int32_t, int32_t *) {
-    return fail(TBR_ERR_INTERNAL, "not available in this build");
+
+static void server_loop(tbr_server *s) {
+    cudaSetDevice(s->E.device);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait_for(lk, std::chrono::milliseconds(50),
+                           [&] { return s->stop || !s->queue.empty() || !s->resident.empty(); });
+            if (s->stop) break;
+            if (s->queue.empty() && s->resident.empty()) continue;
+        }
+        // the counters are per step; the step stamp is reset only when idle
+        tbr_status st = server_step(s);
+        if (st) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->error = st;
+            s->error_msg = g_last_error;
+            // fail everything outstanding
+            for (auto &r : s->resident) {
+                tbr_server_result o;
+                std::memset(&o, 0, sizeof(o));
+                o.request_id = r.req->id;
+                o.status = st;
+                s->done.push_back(o);
+            }
+            for (auto &q : s->queue) {
+                tbr_server_result o;
+                std::memset(&o, 0, sizeof(o));
+                o.request_id = q->id;
+                o.status = st;
+                s->done.push_back(o);
+            }
+            s->in_flight = 0;
+            s->resident.clear();
+            s->queue.clear();
+            s->cv_done.notify_all();
+            break;
+        }
+    }
 }
-tbr_status tbr_server_cancel(tbr_server *, uint64_t) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
-tbr_status tbr_server_drain(tbr_server *) { return fail(TBR_ERR_INTERNAL, "not available in this build"); }
-void tbr_server_destroy(tbr_server *) {}
+
+extern "C" {
+
+tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr_server **out) {
+    if (!ctx || !cfg || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    auto *s = new tbr_server();
+    const uint64_t budget = cfg->workspace_budget_bytes ? cfg->workspace_budget_bytes : (8ull << 30);
+    const int slots = cfg->max_slots > 0 ? std::min(cfg->max_slots, kMaxActive) : 512;
+    tbr_status st = s->E.init(ctx->E.device, budget, slots);
+    if (st) {
+        delete s;
+        return st;
+    }
+    s->ro = cfg->ransac;
+    if (s->ro.max_iterations < 1) {
+        delete s;
+        return fail(TBR_ERR_INVALID_ARG, "ransac.max_iterations must be >= 1");
+    }
+    s->o = make_run_options(&s->ro, nullptr, &cfg->ext);
+    // Serving: bounded rounds per step so that one heavy frame cannot hold a
+    // step (and the requests arriving meanwhile) for long.
+    s->o.max_rounds_step = 16;
+    if (cfg->max_queue > 0) s->max_queue = cfg->max_queue;
+    if (cudaMalloc(&s->d_status, 4 * kMaxActive) != cudaSuccess ||
+        cudaMalloc(&s->d_prep, 4 * kMaxActive) != cudaSuccess ||
+        cudaMallocHost(&s->h_status, 4 * kMaxActive) != cudaSuccess) {
+        delete s;
+        return fail(TBR_ERR_OOM, "server allocation failed");
+    }
+    cudaMemsetAsync(s->E.P.counters, 0, 8 * kCNum, s->E.stream);
+    cudaStreamSynchronize(s->E.stream);
+    s->worker = std::thread(server_loop, s);
+    *out = s;
+    return TBR_OK;
+}
+
+tbr_status tbr_server_submit(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id) {
+    if (!s || !frame || !frame->points2D || !frame->points3D || frame->n < 3)
+        return fail(TBR_ERR_INVALID_ARG, "bad frame");
+    if (!(frame->K[0] > 0) || !(frame->K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "bad camera");
+    auto r = std::make_unique<ServerRequest>();
+    r->uv.assign(frame->points2D, frame->points2D + 2 * frame->n);
+    r->xyz.assign(frame->points3D, frame->points3D + 3 * frame->n);
+    for (int k = 0; k < 4; ++k) r->K[k] = frame->K[k];
+    r->seed = frame->seed;
+    r->thr = frame->max_reproj_error > 0 ? frame->max_reproj_error : s->ro.max_reproj_error;
+    r->t_submit = std::chrono::steady_clock::now();
+    if ((frame->n + kSub - 1) / kSub > s->E.blocks.capacity())
+        return fail(TBR_ERR_CAPACITY, "frame larger than the serving budget");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->error) return fail(s->error, s->error_msg);
+    if ((int)s->queue.size() >= s->max_queue) return fail(TBR_ERR_CAPACITY, "queue full");
+    r->id = s->next_id++;
+    if (request_id) *request_id = r->id;
+    s->queue.push_back(std::move(r));
+    s->in_flight++;
+    s->cv.notify_one();
+    return TBR_OK;
+}
+
+tbr_status tbr_server_poll(tbr_server *s, tbr_server_result *out, int32_t max, int32_t *n_out) {
+    if (!s || !out || max < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const int m = std::min<int>(max, (int)s->done.size());
+    for (int i = 0; i < m; ++i) out[i] = s->done[i];
+    s->done.erase(s->done.begin(), s->done.begin() + m);
+    if (n_out) *n_out = m;
+    if (m == 0 && s->error) return fail(s->error, s->error_msg);
+    return m ? TBR_OK : TBR_ERR_NOT_READY;
+}
+
+tbr_status tbr_server_cancel(tbr_server *s, uint64_t request_id) {
+    if (!s) return fail(TBR_ERR_INVALID_ARG, "NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (auto &q : s->queue)
+        if (q->id == request_id) {
+            q->cancelled = true;
+            s->cv.notify_one();
+            return TBR_OK;
+        }
+    s->cancel_ids.push_back(request_id);
+    return TBR_OK;
+}
+
+tbr_status tbr_server_drain(tbr_server *s) {
+    if (!s) return fail(TBR_ERR_INVALID_ARG, "NULL server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_done.wait(lk, [&] { return s->in_flight == 0 || s->error; });
+    return s->error ? fail(s->error, s->error_msg) : TBR_OK;
+}
+
+void tbr_server_destroy(tbr_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+        s->cv.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    cudaStreamSynchronize(s->E.stream);
+    if (s->d_status) cudaFree(s->d_status);
+    if (s->d_prep) cudaFree(s->d_prep);
+    if (s->h_status) cudaFreeHost(s->h_status);
+    delete s;
+}
 
 tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, const double *points3D,
                                    int64_t n, const double K[4], double max_reproj_error,

@@ -35,7 +35,10 @@ constexpr uint32_t kMaxPolls = 1u << 26;          // bounded mbarrier waits (~se
 constexpr int kScoreWarps = 4;                    // warps per scoring CTA
 constexpr int kLMThreads = 256;
 
-enum FrameStatus : int32_t { kFree = 0, kRansac = 1, kLMPending = 2, kDone = 3, kFailed = 4 };
+// kLMReady: RANSAC finished in the step stamped in lm_epoch; k_inliers takes it
+// one step later (so that in the captured loop it can run beside the next
+// step's RANSAC kernels without racing them) and moves it to kLMPending.
+enum FrameStatus : int32_t { kFree = 0, kRansac = 1, kLMPending = 2, kDone = 3, kFailed = 4, kLMReady = 5 };
 
 enum Counter : int {
     kCScoreNext = 0,
@@ -89,7 +92,7 @@ struct __align__(16) FrameDev {
     int64_t lm_max_iter;
     double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
     double lm_inv_sq_thr, lm_grad_tol, lm_step_tol, lm_lambda0, lm_min_lambda, lm_max_lambda;
-    int32_t chunk_points, pad0;
+    int32_t chunk_points, max_rounds_step;  // max_rounds_step: 0 = kMaxRoundsPerStep
     // ---- RANSAC progress ----
     int64_t samples_done, rounds_done, hyps_done;
     int32_t steps, found;
@@ -110,6 +113,8 @@ struct __align__(16) FrameDev {
     int32_t round_hyps[kMaxRoundsPerStep];
     // ---- LM ----
     int64_t num_inliers;
+    int64_t lm_epoch;  // engine step in which RANSAC finished
+    int32_t lm_force_cluster, pad9;  // bundle_adjust path: always the cluster LM
 };
 
 struct Pools {
@@ -332,7 +337,7 @@ __global__ void k_plan(Pools P) {
                     if (need < 0 || r < 1) r = 1;
                 }
                 r = min(r, max_rounds - f->rounds_done);
-                r = min(r, (int64_t)kMaxRoundsPerStep);
+                r = min(r, (int64_t)(f->max_rounds_step > 0 ? f->max_rounds_step : kMaxRoundsPerStep));
                 if (r < 1) r = 1;
                 rounds = r;
                 samples = r * f->B;
@@ -954,7 +959,11 @@ __global__ void __launch_bounds__(256) k_finalize(Pools P) {
         f.rounds_done += r_end;
     }
     if (stop) {
-        f.status = kLMPending;
+        // Publish the best pose and the epoch before the status: k_inliers may
+        // run concurrently on another stream and reads them in reverse order.
+        f.lm_epoch = (int64_t)P.counters[kCSteps];
+        __threadfence();
+        *(volatile int32_t *)&f.status = kLMReady;
         atomicAdd(&P.counters[kCLMPending], 1ull);
     } else {
         atomicAdd(&P.counters[kCStillRansac], 1ull);
@@ -970,7 +979,16 @@ __global__ void __launch_bounds__(1024) k_inliers(Pools P) {
     __shared__ double sR[9], st[3], sq[4];
     const int slot = P.active[blockIdx.x];
     FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending) return;
+    __shared__ int take;
+    if (threadIdx.x == 0) {
+        const int32_t st0 = *(volatile int32_t *)&f.status;
+        __threadfence();
+        const int64_t ep = *(volatile int64_t *)&f.lm_epoch;
+        take = (st0 == kLMReady && ep < (int64_t)*(volatile unsigned long long *)&P.counters[kCSteps]) ? 1 : 0;
+        __threadfence();
+    }
+    __syncthreads();
+    if (!take) return;
     if (threadIdx.x == 0) {
         double R[9];
         for (int r = 0; r < 3; ++r) {
@@ -1021,6 +1039,7 @@ __global__ void __launch_bounds__(1024) k_inliers(Pools P) {
     }
     if (threadIdx.x == 0) {
         f.num_inliers = written;
+        f.status = kLMPending;
         FrameResult &res = P.results[slot];
         for (int k = 0; k < 4; ++k) res.q[k] = sq[k];
         for (int k = 0; k < 3; ++k) res.t[k] = st[k];
@@ -1093,13 +1112,14 @@ __device__ double lm_cost_slice(const Pools &P, int64_t base, int64_t i0, int64_
 
 // Levenberg-Marquardt with the control flow of lm.cuh:15-171 (damping, accept
 // rule, lambda schedule, the removal of damping after a rejected step, and both
-// stop tests), one frame per cluster of kLMCluster CTAs, each owning a slice of
+// stop tests), one frame per cluster of CL CTAs, each owning a slice of
 // the inliers. J^T W J (lower triangle, jaco.cuh:173-200) and J^T W r
 // (:202-209) are accumulated per thread in FP32 with Kahan compensation from
 // centred coordinates and summed across the block and cluster in FP64 in a
 // fixed order; the 6x6 Cholesky (lm_utils.cuh:14-100), the step and the cost
 // used for acceptance are FP64.
-__global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads) k_lm(Pools P) {
+template <int CL>
+__device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     __shared__ double scratch[32 * 27];
@@ -1107,14 +1127,12 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads)
     __shared__ LMShared S;
     __shared__ float R32[9], tc32[3];
     const int rank = (int)cluster.block_rank();
-    const int slot = P.active[blockIdx.x / kLMCluster];
     FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending) return;  // uniform across the cluster
     LMShared *L0 = cluster.map_shared_rank(&S, 0);
     FrameResult &res = P.results[slot];
     const int64_t base = f.blk_off * kSub;
     const int64_t n = f.num_inliers;
-    const int64_t i0 = n * rank / kLMCluster, i1 = n * (rank + 1) / kLMCluster;
+    const int64_t i0 = n * rank / CL, i1 = n * (rank + 1) / CL;
     const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
     const float camf[4] = {(float)cam[0], (float)cam[1], (float)cam[2], (float)cam[3]};
     const double inv_sq_thr = f.lm_inv_sq_thr;
@@ -1133,7 +1151,7 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads)
     cluster.sync();
     if (rank == 0 && threadIdx.x == 0) {
         double tot = 0.0;
-        for (int r = 0; r < kLMCluster; ++r) tot += cluster.map_shared_rank(&S, r)->part[0];
+        for (int r = 0; r < CL; ++r) tot += cluster.map_shared_rank(&S, r)->part[0];
         S.cost = tot;
         S.lambda = f.lm_lambda0;
         S.recompute = 1;
@@ -1225,7 +1243,7 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads)
             if (rank == 0 && threadIdx.x == 0) {
                 double tot[27];
                 for (int k = 0; k < 27; ++k) tot[k] = 0.0;
-                for (int r = 0; r < kLMCluster; ++r) {
+                for (int r = 0; r < CL; ++r) {
                     const LMShared *Sr = cluster.map_shared_rank(&S, r);
                     for (int k = 0; k < 27; ++k) tot[k] += Sr->part[k];
                 }
@@ -1295,7 +1313,7 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads)
         cluster.sync();
         if (rank == 0 && threadIdx.x == 0) {
             double cn = 0.0;
-            for (int r = 0; r < kLMCluster; ++r) cn += cluster.map_shared_rank(&S, r)->part[0];
+            for (int r = 0; r < CL; ++r) cn += cluster.map_shared_rank(&S, r)->part[0];
             if (cn < S.cost) {
                 for (int k = 0; k < 4; ++k) S.q[k] = S.qn[k];
                 for (int k = 0; k < 3; ++k) S.t[k] = S.tn[k];
@@ -1333,6 +1351,35 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads)
     }
     cluster.sync();  // no CTA leaves while rank 0 may still read its shared memory
     if (rank == 0 && threadIdx.x == 0) f.status = kDone;
+}
+
+// Frames with fewer inliers than this run their LM on one CTA; larger ones on
+// a cluster of kLMCluster CTAs (a single SM would serialise them).
+constexpr int64_t kLMClusterMin = 3000;
+
+__global__ void __launch_bounds__(kLMThreads) k_lm_small(Pools P) {
+    const int slot = P.active[blockIdx.x];
+    const FrameDev &f = P.frames[slot];
+    if (f.status != kLMPending || f.num_inliers >= kLMClusterMin || f.lm_force_cluster) return;
+    lm_frame<1>(P, slot);
+}
+
+__global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads) k_lm(Pools P) {
+    const int slot = P.active[blockIdx.x / kLMCluster];
+    const FrameDev &f = P.frames[slot];
+    // uniform across the cluster
+    if (f.status != kLMPending || (f.num_inliers < kLMClusterMin && !f.lm_force_cluster)) return;
+    lm_frame<kLMCluster>(P, slot);
+}
+
+// Host-stepped runs: close the step (stamp it) so that frames finished in it
+// are taken by k_inliers right away.
+__global__ void k_tick(Pools P) { P.counters[kCSteps] += 1; }
+
+// Serving: the status of every active frame in one array (one copy to the host).
+__global__ void k_gather_status(Pools P, int32_t *out) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.n_active; a += gridDim.x * blockDim.x)
+        out[a] = P.frames[P.active[a]].status;
 }
 
 // ----------------------------------------------------------- loop control --
