@@ -273,6 +273,26 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D,
                                    float *scores32, int64_t *counts, int64_t cap,
                                    int64_t *n_hyp);
 
+/* --------------------------------------------------------- no allocation --
+ * No counterpart in the reference. FP64 truncated-MSAC scores and inlier counts
+ * of n_poses poses (n_poses*12 doubles, [R | t] row-major) over n device-resident
+ * correspondences x_dev (n*2 normalized coordinates) and X_dev (n*3), written to
+ * scores_dev[n_poses] and counts_dev[n_poses], asynchronously on `stream`
+ * (a cudaStream_t; NULL = the legacy default stream).
+ * For callers that must not allocate device memory -- code running inside
+ * another runtime's memory pool or an allocation-free real-time loop: this
+ * call performs no cudaMalloc or other allocation. Its working memory is one
+ * fixed array of about 400 KB compiled into the library, which every GPU that
+ * loads the library keeps until the process exits. Limits and rules:
+ *  - at most 1024 poses per call (larger requests fail with TBR_ERR_INVALID_ARG);
+ *  - the first call on each device looks up the array's device address (with
+ *    that device current), so make that first call before any stream capture;
+ *  - all calls share the array: calls that overlap on the GPU (different
+ *    streams, or other threads) race -- order them on one stream or with events. */
+tbr_status tbr_msac_score_noalloc(const double *x_dev, const double *X_dev, int64_t n,
+                                  const double *poses_dev, int32_t n_poses, double sq_threshold,
+                                  double *scores_dev, int64_t *counts_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

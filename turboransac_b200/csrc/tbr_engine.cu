@@ -1449,3 +1449,126 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, con
 }
 
 }  // extern "C"
+
+// ======================================================= no-allocation path ==
+// An FP64 MSAC scorer for callers that cannot allocate device memory: code
+// that runs where cudaMalloc is unavailable or forbidden -- inside another
+// library's memory pool, in an allocation-free real-time loop, or under a
+// host runtime that owns every device allocation. The caller passes device
+// inputs and outputs; the only other memory it touches is the fixed scratch
+// array below, which every GPU that loads this library holds until exit.
+namespace tbr {
+
+constexpr int kNoAllocMaxPoses = 1024;   // poses per call
+constexpr int kNoAllocChunks = 32;       // point chunks per pose (partial sums)
+
+struct NoAllocScratch {
+    double part_s[kNoAllocMaxPoses][kNoAllocChunks];
+    int part_c[kNoAllocMaxPoses][kNoAllocChunks];
+    unsigned arrive[kNoAllocMaxPoses];   // cleared at the start of every call
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// One CTA per (pose, chunk): the per-point formula of msac.cuh:18-56, a block
+// sum into the scratch partials, and the last chunk of each pose adding the
+// partials in chunk order plus (n - count) * sq_thr (ransac.cuh:322).
+__global__ void __launch_bounds__(256) k_msac_noalloc(NoAllocScratch *sc, const double *xn, const double *X,
+                                                      int64_t n, const double *poses, double sq_thr,
+                                                      double *scores, int64_t *counts) {
+    __shared__ double ss[8];
+    __shared__ int scnt[8];
+    __shared__ unsigned prev;
+    const int p = blockIdx.y, ch = blockIdx.x;
+    const int64_t per = (n + kNoAllocChunks - 1) / kNoAllocChunks;
+    const int64_t i0 = (int64_t)ch * per, i1 = i0 + per < n ? i0 + per : n;
+    double M[12];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) M[e] = poses[12 * p + e];
+    double s = 0.0;
+    int c = 0;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const double X0 = X[3 * i], X1 = X[3 * i + 1], X2 = X[3 * i + 2];
+        const double z0 = M[0] * X0 + M[1] * X1 + M[2] * X2 + M[3];
+        const double z1 = M[4] * X0 + M[5] * X1 + M[6] * X2 + M[7];
+        const double z2 = M[8] * X0 + M[9] * X1 + M[10] * X2 + M[11];
+        const double inv_z2 = 1.0 / z2;
+        const double r0 = z0 * inv_z2 - xn[2 * i], r1 = z1 * inv_z2 - xn[2 * i + 1];
+        const double r_sq = r0 * r0 + r1 * r1;
+        if (r_sq < sq_thr && z2 > 0.0) {
+            s += r_sq;
+            ++c;
+        }
+    }
+    s = warp_sum(s);
+    c = warp_sum(c);
+    if ((threadIdx.x & 31) == 0) {
+        ss[threadIdx.x >> 5] = s;
+        scnt[threadIdx.x >> 5] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double S = 0.0;
+        int C = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            S += ss[k];
+            C += scnt[k];
+        }
+        sc->part_s[p][ch] = S;
+        sc->part_c[p][ch] = C;
+        __threadfence();
+        prev = atomicAdd(&sc->arrive[p], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && prev == (unsigned)(kNoAllocChunks - 1)) {
+        __threadfence();
+        double S = 0.0;
+        int64_t C = 0;
+        for (int q = 0; q < kNoAllocChunks; ++q) {
+            S += __ldcg(&sc->part_s[p][q]);
+            C += __ldcg(&sc->part_c[p][q]);
+        }
+        scores[p] = S + (double)(n - C) * sq_thr;
+        counts[p] = C;
+    }
+}
+
+// Device address of the scratch array, resolved once per device.
+static std::mutex g_noalloc_mu;
+static std::unordered_map<int, NoAllocScratch *> g_noalloc_ptr;
+
+}  // namespace tbr
+
+extern "C" tbr_status tbr_msac_score_noalloc(const double *x_dev, const double *X_dev, int64_t n,
+                                              const double *poses_dev, int32_t n_poses, double sq_threshold,
+                                              double *scores_dev, int64_t *counts_dev, void *stream) {
+    if (!x_dev || !X_dev || !poses_dev || !scores_dev || !counts_dev || n < 1 || n_poses < 0)
+        return fail(TBR_ERR_INVALID_ARG, "tbr_msac_score_noalloc: bad arguments");
+    if (n_poses > kNoAllocMaxPoses)
+        return fail(TBR_ERR_INVALID_ARG, "tbr_msac_score_noalloc: at most 1024 poses per call (fixed scratch size)");
+    if (n_poses == 0) return TBR_OK;
+    int dev = 0;
+    TBR_CUDA(cudaGetDevice(&dev));
+    NoAllocScratch *sc = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        auto it = g_noalloc_ptr.find(dev);
+        if (it == g_noalloc_ptr.end()) {
+            // First call on this device (the device is current): translate the
+            // symbol into a device address. Host code must not use the
+            // symbol's own name as a pointer; it is only a host-side stand-in.
+            void *ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess)
+                return fail(TBR_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            it = g_noalloc_ptr.emplace(dev, (NoAllocScratch *)ptr).first;
+        }
+        sc = it->second;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    TBR_CUDA(cudaMemsetAsync(sc->arrive, 0, sizeof(unsigned) * n_poses, st));
+    k_msac_noalloc<<<dim3(kNoAllocChunks, n_poses), 256, 0, st>>>(sc, x_dev, X_dev, n, poses_dev, sq_threshold,
+                                                                    scores_dev, counts_dev);
+    TBR_CUDA(cudaGetLastError());
+    return TBR_OK;
+}
