@@ -44,7 +44,7 @@ class ExtOptionsC(C.Structure):
                 ("force_samples", C.c_int64), ("max_total_samples", C.c_int64),
                 ("seed", C.c_uint64), ("replay_idx", C.c_void_p), ("replay_count", C.c_int64),
                 ("hyp_per_thread", C.c_int32), ("chunk_points", C.c_int32),
-                ("stop_rule_x86_quirk", C.c_int32), ("reserved", C.c_int32)]
+                ("stop_rule_x86_quirk", C.c_int32), ("points_per_iter", C.c_int32)]
 
 
 class StatsC(C.Structure):

@@ -323,7 +323,8 @@ class Batch:
     over engine steps) with the inputs resident in device memory."""
 
     def __init__(self, ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None,
-                 hyp_per_thread: int = 0, chunk_points: int = 0):
+                 hyp_per_thread: int = 0, chunk_points: int = 0, force_samples: int = 0,
+                 points_per_iter: int = 0):
         self.ctx = ctx
         self.n = len(frames)
         arr, self._keep = _frame_descs(frames)
@@ -331,6 +332,8 @@ class Batch:
         ext = _lib.ExtOptionsC()
         ext.hyp_per_thread = hyp_per_thread
         ext.chunk_points = chunk_points
+        ext.force_samples = force_samples
+        ext.points_per_iter = points_per_iter
         h = C.c_void_p()
         with ctx._lock:
             check(_lib.lib().tbr_batch_create(ctx.handle, arr, self.n, C.byref(ro), C.byref(ext), C.byref(h)))

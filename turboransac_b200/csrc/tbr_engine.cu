@@ -108,7 +108,8 @@ struct RunOptions {
     double trials_mult = 3.0;
     int skip_refine = 0;
     int quirk = 0;
-    int hr = 8;
+    int hr = 4;
+    int pp = 2;
     int chunk_points = 0;
     int max_rounds_step = 0;
     // LM (compat: default BundleOptions_cuda with loss_scale = 1/f)
@@ -128,7 +129,9 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
         o.quirk = ext->stop_rule_x86_quirk;
         o.force_samples = ext->force_samples;
         if (ext->max_total_samples > 0) o.max_total = ext->max_total_samples;
-        if (ext->hyp_per_thread == 4 || ext->hyp_per_thread == 8) o.hr = ext->hyp_per_thread;
+        if (ext->hyp_per_thread == 2 || ext->hyp_per_thread == 4 || ext->hyp_per_thread == 8)
+            o.hr = ext->hyp_per_thread;
+        if (ext->points_per_iter == 2 || ext->points_per_iter == 4) o.pp = ext->points_per_iter;
         o.chunk_points = ext->chunk_points;
     }
     if (honor && ro) {
@@ -166,7 +169,7 @@ class Engine {
     int32_t *d_active = nullptr;
     int32_t *d_replay = nullptr;
     int64_t d_replay_cap = 0;
-    int score_grid[2] = {0, 0};
+    int score_grid[4] = {0, 0, 0, 0};  // (HP, PP) = (1,4), (2,2), (2,4), (4,2)
     int rescore_grid = 0, p3p_grid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
@@ -212,7 +215,7 @@ class Engine {
         P.max_hyps = std::max<int64_t>(P.max_hyps, 4096);
         P.max_parts = P.max_hyps * 32;
         P.max_hb = P.max_hyps / 32 + kMaxActive;
-        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 16 + 16) + kBlockBytes;
+        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24) + kBlockBytes;
         max_blocks = (int64_t)((rest - (size_t)(P.max_hyps * per_hyp) - P.max_hb * 4) / per_block) - 1;
         if (max_blocks < 64) return fail(TBR_ERR_INVALID_ARG, "workspace too small for points");
         // One allocation, carved with 256-byte alignment.
@@ -228,8 +231,6 @@ class Engine {
         add((void **)&P.mask, np);
         add((void **)&P.lx64, 16 * np);
         add((void **)&P.lX64, 24 * np);
-        add((void **)&P.lA32, 16 * np);
-        add((void **)&P.lB32, 16 * np);
         add((void **)&P.pts32, (size_t)kBlockBytes * max_blocks);
         add((void **)&P.sample_prefix, 8 * (kMaxActive + 1));
         add((void **)&P.item_prefix, 8 * (kMaxActive + 1));
@@ -264,10 +265,12 @@ class Engine {
         blocks.reset(max_blocks);
         for (int i = max_frames - 1; i >= 0; --i) free_slots.push_back(i);
         int occ = 0;
-        TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_score<2>, kScoreWarps * 32, 0));
-        score_grid[0] = num_sms * std::max(occ, 1);
-        TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_score<4>, kScoreWarps * 32, 0));
-        score_grid[1] = num_sms * std::max(occ, 1);
+        const void *sk[4] = {(const void *)k_score<1, 4>, (const void *)k_score<2, 2>, (const void *)k_score<2, 4>,
+                             (const void *)k_score<4, 2>};
+        for (int v = 0; v < 4; ++v) {
+            TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sk[v], kScoreWarps * 32, 0));
+            score_grid[v] = num_sms * std::max(occ, 1);
+        }
         TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rescore, 256, 0));
         rescore_grid = num_sms * std::max(occ, 1);
         p3p_grid = num_sms * 8;
@@ -357,6 +360,16 @@ class Engine {
     static constexpr const char *kKernelNames[12] = {"k_plan", "k_sample_p3p", "k_score_plan", "k_score",
                                                      "k_select", "k_rescore_plan", "k_rescore", "k_finalize",
                                                      "k_inliers", "k_lm", "k_prep", "unused"};
+    // Scoring kernel variant: HR hypotheses per lane = 2*HP, PP points per iteration.
+    void launch_score(const Pools &Q, int hr, int pp, cudaStream_t st) {
+        const int threads = kScoreWarps * 32;
+        if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
+        else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
+        else if (pp == 4) k_score<2, 4><<<score_grid[2], threads, 0, st>>>(Q);
+        else k_score<2, 2><<<score_grid[1], threads, 0, st>>>(Q);
+    }
+    int pp = 2;  // points per iteration of the scoring kernel (HR = 4)
+
     // RANSAC part of a step (plan .. finalize).
     void launch_ransac(const Pools &Q, int n_active, int hr, cudaStream_t st, Profile *prof = nullptr) {
         auto beg = [&](int k) { if (prof) cudaEventRecord(prof->ev[2 * k], st); };
@@ -365,8 +378,7 @@ class Engine {
         beg(1); k_sample_p3p<<<p3p_grid, 128, 0, st>>>(Q); end(1);
         beg(2); k_score_plan<<<1, kMaxActive, 0, st>>>(Q); end(2);
         beg(3);
-        if (hr == 4) k_score<2><<<score_grid[0], kScoreWarps * 32, 0, st>>>(Q);
-        else k_score<4><<<score_grid[1], kScoreWarps * 32, 0, st>>>(Q);
+        launch_score(Q, hr, pp, st);
         end(3);
         beg(4); k_select<<<n_active, 256, 0, st>>>(Q); end(4);
         beg(5); k_rescore_plan<<<1, kMaxActive, 0, st>>>(Q); end(5);
@@ -585,6 +597,7 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
     if (st) return st;
     TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
     E.launch_prep((int)slots.size(), max_n);
+    E.pp = o.pp;
     st = E.run(slots, o.hr, 100000, steps_out);
     TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
     if (st == TBR_OK) st = E.ensure_stage(sizeof(FrameResult) * slots.size() + 256);
@@ -786,7 +799,9 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (n + 1023) / 1024));
     k_prep_bounds<<<dim3(bx, 1), 256, 0, E.stream>>>(E.P);
     k_lm_pack<<<bx, 256, 0, E.stream>>>(E.P);
+    cudaEventRecord(E.ev0, E.stream);
     k_lm<<<kLMCluster, kLMThreads, 0, E.stream>>>(E.P);
+    cudaEventRecord(E.ev1, E.stream);
     st = TBR_OK;
     if (cudaGetLastError() != cudaSuccess) st = fail(TBR_ERR_CUDA, "bundle_adjust launch failed");
     FrameResult res;
@@ -799,6 +814,9 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     for (int k = 0; k < 3; ++k) t[k] = res.t[k];
     if (stats) {
         std::memset(stats, 0, sizeof(*stats));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, E.ev0, E.ev1);
+        stats->gpu_ms = ms;
         stats->lm_iterations = res.lm_iters;
         stats->lm_invalid_steps = res.lm_invalid;
         stats->lm_initial_cost = res.lm_cost0;
@@ -931,6 +949,7 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
         ok = cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
              cudaSuccess;
         if (ok) {
+            E.pp = b->o.pp;
             cudaEventRecord(E.ev_fork, E.stream);
             cudaStreamWaitEvent(E.stream2, E.ev_fork, 0);
             E.launch_refine(b->Q, n_frames, E.stream2);
@@ -1016,6 +1035,7 @@ tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max,
     Engine::Profile pr;
     k_reset_frames<<<b->Q.n_active, 128, 0, E.stream>>>(b->Q, b->d_init);
     int steps = 0;
+    E.pp = b->o.pp;
     tbr_status st = E.run(b->Q, b->Q.n_active, b->o.hr, 100000, &steps, &pr);
     for (auto &e : pr.ev)
         if (e) cudaEventDestroy(e);
@@ -1300,6 +1320,7 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
     // Serving: bounded rounds per step so that one heavy frame cannot hold a
     // step (and the requests arriving meanwhile) for long.
     s->o.max_rounds_step = 16;
+    s->E.pp = s->o.pp;
     if (cfg->max_queue > 0) s->max_queue = cfg->max_queue;
     if (cudaMalloc(&s->d_status, 4 * kMaxActive) != cudaSuccess ||
         cudaMalloc(&s->d_prep, 4 * kMaxActive) != cudaSuccess ||
@@ -1408,8 +1429,7 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, con
     k_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
     k_sample_p3p<<<E.p3p_grid, 128, 0, E.stream>>>(E.P);
     k_score_plan<<<1, kMaxActive, 0, E.stream>>>(E.P);
-    if (o.hr == 4) k_score<2><<<E.score_grid[0], kScoreWarps * 32, 0, E.stream>>>(E.P);
-    else k_score<4><<<E.score_grid[1], kScoreWarps * 32, 0, E.stream>>>(E.P);
+    E.launch_score(E.P, o.hr, o.pp, E.stream);
     if (counts) k_debug_counts<<<E.num_sms * 4, 256, 0, E.stream>>>(E.P);
     TBR_CUDA(cudaGetLastError());
     FrameDev fd;

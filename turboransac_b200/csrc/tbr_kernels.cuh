@@ -29,7 +29,7 @@ constexpr uint32_t kBlockBytes = kBlockFloat2 * 8;  // 2560 B per block
 constexpr int kMaxRoundsPerStep = 128;
 constexpr int kMaxCandFrame = 4096;               // FP64 re-rank candidates per frame and step
 constexpr int kMaxRChunks = 32;                   // FP64 rescoring point chunks per frame
-constexpr int kMaxScoreChunks = 32;               // FP32 scoring point chunks per frame
+constexpr int kMaxScoreChunks = 64;               // FP32 scoring point chunks per frame
 constexpr int kMaxActive = 1024;                  // frames advanced by one step
 constexpr uint32_t kMaxPolls = 1u << 26;          // bounded mbarrier waits (~seconds)
 constexpr int kScoreWarps = 4;                    // warps per scoring CTA
@@ -87,7 +87,7 @@ struct __align__(16) FrameDev {
     int64_t max_total;
     int64_t force_samples;
     double log_missing, trials_mult;
-    int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass
+    int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass (2 * HP)
     int32_t quirk, pad1;      // stop rule: 1 = x86 int-conversion quirk of the reference  // hr: hypotheses per lane in the scoring pass
     int64_t lm_max_iter;
     double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
@@ -130,8 +130,6 @@ struct Pools {
     uint8_t *mask;       // final inlier mask (1/pt)
     double *lx64;        // LM: pixels / f (2/pt)
     double *lX64;        // LM: world points (3/pt)
-    float4 *lA32;        // LM: (Xc, Yc, Zc, u/f) centred, FP32
-    float4 *lB32;        // LM: (X, Y, Z, v/f) world, FP32
     float2 *pts32;       // staging blocks: [X|Y|Z|-x/tau|-y/tau] x kSub, each value duplicated
     // step prefixes (n_active + 1)
     int64_t *sample_prefix;
@@ -338,6 +336,10 @@ __global__ void k_plan(Pools P) {
                 }
                 r = min(r, max_rounds - f->rounds_done);
                 r = min(r, (int64_t)(f->max_rounds_step > 0 ? f->max_rounds_step : kMaxRoundsPerStep));
+                // Growth cap: the frame's s-th step runs at most 4 * 2^(s-1) rounds,
+                // so a stop bound that shrinks once a better model turns up wastes
+                // at most the last step's overshoot.
+                if (f->steps >= 1) r = min(r, (int64_t)4 << min(f->steps - 1, 5));
                 if (r < 1) r = 1;
                 rounds = r;
                 samples = r * f->B;
@@ -476,17 +478,30 @@ __global__ void k_score_plan(Pools P) {
     __syncthreads();
     if (act) atomicAdd(&pairs_total, (unsigned long long)f->hyp_count * (unsigned long long)f->n);
     __syncthreads();
+    __shared__ unsigned long long parts_total;
+    if (a == 0) parts_total = 0;
     int64_t items = 0, parts = 0, hbs = 0;
+    int HB = 32, nhb = 0, cb = 1;
     if (act) {
-        const int HB = 32 * f->hr;
-        const int nhb = (f->hyp_count + HB - 1) / HB;
-        // Target about 8 items per warp slot of the GPU, at least 4 blocks per item.
+        HB = 32 * f->hr;
+        nhb = (f->hyp_count + HB - 1) / HB;
+        // About 8 items per warp slot of the GPU; at least 2 staging blocks per item.
         const double target_items = 8.0 * P.num_sms * 16;
-        const double pairs_per_item = fmax((double)pairs_total / target_items, 4.0 * kSub * HB);
-        int cb = (int)ceil(pairs_per_item / ((double)HB * kSub));
+        const double pairs_per_item = fmax((double)pairs_total / target_items, 2.0 * kSub * HB);
+        cb = (int)ceil(pairs_per_item / ((double)HB * kSub));
         if (f->chunk_points > 0) cb = max(1, f->chunk_points / kSub);
         cb = max(cb, (f->n_blocks + kMaxScoreChunks - 1) / kMaxScoreChunks);
         cb = max(1, min(cb, f->n_blocks));
+        atomicAdd(&parts_total, (unsigned long long)f->hyp_count * ((f->n_blocks + cb - 1) / cb));
+    }
+    __syncthreads();
+    if (act) {
+        // Keep the chunk partials within their buffer.
+        const unsigned long long pt = parts_total;
+        if (pt > (unsigned long long)P.max_parts) {
+            const int scale = (int)((pt + P.max_parts - 1) / P.max_parts);
+            cb = min(f->n_blocks, cb * scale);
+        }
         const int nch = (f->n_blocks + cb - 1) / cb;
         f->n_hblocks = nhb;
         f->chunk_blocks = cb;
@@ -517,33 +532,50 @@ __global__ void k_score_plan(Pools P) {
     if (a == 0 && tot > P.max_hb) flag_error(P, kErrOverflow);
 }
 
-// One (hypothesis pair, point) update: returns nothing, accumulates
-// min(r^2 / tau^2, 1) into both halves of acc, counting a point with
-// non-positive depth as an outlier (msac.cuh:46 semantics). Division-free
-// sign test: the reciprocal of the depth carries its sign into the squared
-// residual's sign bit, and an unsigned min against 1.0f clamps NaN, +inf,
-// and any negative-signed value to 1.
-__device__ __forceinline__ void msac_pair(const uint64_t (&p)[12], uint64_t X, uint64_t Y, uint64_t Z,
-                                          uint64_t NX, uint64_t NY, uint64_t &acc) {
-    const uint64_t z0 = f2fma(p[0], X, f2fma(p[1], Y, f2fma(p[2], Z, p[3])));
-    const uint64_t z1 = f2fma(p[4], X, f2fma(p[5], Y, f2fma(p[6], Z, p[7])));
-    const uint64_t z2 = f2fma(p[8], X, f2fma(p[9], Y, f2fma(p[10], Z, p[11])));
-    float za, zb;
-    f2unpack(z2, za, zb);
-    const float ia = rcp_approx(za), ib = rcp_approx(zb);
-    const uint64_t inv = f2pack(ia, ib);
-    const uint64_t r0 = f2fma(z0, inv, NX);
-    const uint64_t r1 = f2fma(z1, inv, NY);
-    const uint64_t q = f2fma(r0, r0, f2mul(r1, r1));
-    float qa, qb;
-    f2unpack(q, qa, qb);
-    const uint32_t ca = min(__float_as_uint(qa) | (__float_as_uint(ia) & 0x80000000u), 0x3f800000u);
-    const uint32_t cb = min(__float_as_uint(qb) | (__float_as_uint(ib) & 0x80000000u), 0x3f800000u);
-    acc = f2add(acc, f2pack(__uint_as_float(ca), __uint_as_float(cb)));
+// Per (hypothesis, point) the FP32 filter accumulates min(r^2 / tau^2, 1),
+// counting a point with non-positive depth as an outlier (msac.cuh:46
+// semantics) without a division or a branch: the reciprocal of the depth
+// carries its sign into the squared residual's sign bit, and an unsigned min
+// against the bits of 1.0f clamps NaN, +inf and any negative-signed value to 1.
+// HP hypothesis pairs x PP points as independent packed-FP32 chains, staged so
+// that every depth and its reciprocal issue first and the MUFU latency is
+// covered by the other two rows: z2 -> rcp, then z0, z1, residuals, clamp, sum.
+template <int HP, int PP>
+__device__ __forceinline__ void msac_chains(const uint64_t (&c)[HP][12], const uint64_t (&X)[PP],
+                                            const uint64_t (&Y)[PP], const uint64_t (&Z)[PP],
+                                            const uint64_t (&NX)[PP], const uint64_t (&NY)[PP], uint64_t (&acc)[HP]) {
+    float ia[HP][PP], ib[HP][PP];
+#pragma unroll
+    for (int h = 0; h < HP; ++h)
+#pragma unroll
+        for (int p = 0; p < PP; ++p) {
+            const uint64_t z2 = f2fma(c[h][8], X[p], f2fma(c[h][9], Y[p], f2fma(c[h][10], Z[p], c[h][11])));
+            float za, zb;
+            f2unpack(z2, za, zb);
+            ia[h][p] = rcp_approx(za);
+            ib[h][p] = rcp_approx(zb);
+        }
+#pragma unroll
+    for (int h = 0; h < HP; ++h)
+#pragma unroll
+        for (int p = 0; p < PP; ++p) {
+            const uint64_t z0 = f2fma(c[h][0], X[p], f2fma(c[h][1], Y[p], f2fma(c[h][2], Z[p], c[h][3])));
+            const uint64_t z1 = f2fma(c[h][4], X[p], f2fma(c[h][5], Y[p], f2fma(c[h][6], Z[p], c[h][7])));
+            const uint64_t inv = f2pack(ia[h][p], ib[h][p]);
+            const uint64_t r0 = f2fma(z0, inv, NX[p]);
+            const uint64_t r1 = f2fma(z1, inv, NY[p]);
+            const uint64_t q = f2fma(r0, r0, f2mul(r1, r1));
+            float qa, qb;
+            f2unpack(q, qa, qb);
+            const uint32_t ca = min(__float_as_uint(qa) | (__float_as_uint(ia[h][p]) & 0x80000000u), 0x3f800000u);
+            const uint32_t cb = min(__float_as_uint(qb) | (__float_as_uint(ib[h][p]) & 0x80000000u), 0x3f800000u);
+            acc[h] = f2add(acc[h], f2pack(__uint_as_float(ca), __uint_as_float(cb)));
+        }
 }
 
-// One staging block (kSub points) against the lane's HP hypothesis pairs.
-template <int HP>
+// One staging block (kSub points) against the lane's HP hypothesis pairs,
+// PP points at a time (each 16-byte shared load carries two duplicated points).
+template <int HP, int PP>
 __device__ __forceinline__ void score_block(const float2 *blk, int valid, const uint64_t (&c)[HP][12],
                                             uint64_t (&acc)[HP]) {
     const ulonglong2 *sX = reinterpret_cast<const ulonglong2 *>(blk);
@@ -552,22 +584,26 @@ __device__ __forceinline__ void score_block(const float2 *blk, int valid, const 
     const ulonglong2 *sNX = sZ + kSub / 2;
     const ulonglong2 *sNY = sNX + kSub / 2;
     if (valid == kSub) {
-#pragma unroll 2
-        for (int j = 0; j < kSub / 2; ++j) {
-            const ulonglong2 X = sX[j], Y = sY[j], Z = sZ[j], NX = sNX[j], NY = sNY[j];
+#pragma unroll 1
+        for (int j = 0; j < kSub / 2; j += PP / 2) {
+            uint64_t X[PP], Y[PP], Z[PP], NX[PP], NY[PP];
 #pragma unroll
-            for (int h = 0; h < HP; ++h) {
-                msac_pair(c[h], X.x, Y.x, Z.x, NX.x, NY.x, acc[h]);
-                msac_pair(c[h], X.y, Y.y, Z.y, NX.y, NY.y, acc[h]);
+            for (int k = 0; k < PP / 2; ++k) {
+                const ulonglong2 x = sX[j + k], y = sY[j + k], z = sZ[j + k], nx = sNX[j + k], ny = sNY[j + k];
+                X[2 * k] = x.x; X[2 * k + 1] = x.y;
+                Y[2 * k] = y.x; Y[2 * k + 1] = y.y;
+                Z[2 * k] = z.x; Z[2 * k + 1] = z.y;
+                NX[2 * k] = nx.x; NX[2 * k + 1] = nx.y;
+                NY[2 * k] = ny.x; NY[2 * k + 1] = ny.y;
             }
+            msac_chains<HP, PP>(c, X, Y, Z, NX, NY, acc);
         }
     } else {
+        const uint64_t *u = reinterpret_cast<const uint64_t *>(blk);
         for (int j = 0; j < valid; ++j) {
-            const uint64_t *u = reinterpret_cast<const uint64_t *>(blk);
-            const uint64_t X = u[j], Y = u[kSub + j], Z = u[2 * kSub + j], NX = u[3 * kSub + j],
-                           NY = u[4 * kSub + j];
-#pragma unroll
-            for (int h = 0; h < HP; ++h) msac_pair(c[h], X, Y, Z, NX, NY, acc[h]);
+            uint64_t X[1] = {u[j]}, Y[1] = {u[kSub + j]}, Z[1] = {u[2 * kSub + j]}, NX[1] = {u[3 * kSub + j]},
+                     NY[1] = {u[4 * kSub + j]};
+            msac_chains<HP, 1>(c, X, Y, Z, NX, NY, acc);
         }
     }
 }
@@ -579,7 +615,7 @@ __device__ __forceinline__ void score_block(const float2 *blk, int valid, const 
 // as packed FP32x2 pairs. The warp that completes the last chunk of a
 // hypothesis block sums the chunk partials in fixed order and publishes the
 // per-round minimum as a packed (score, index) key.
-template <int HP>
+template <int HP, int PP>
 __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
     __shared__ __align__(128) float2 stage[kScoreWarps][2][kBlockFloat2];
     __shared__ __align__(8) uint64_t bars[kScoreWarps][2];
@@ -596,11 +632,29 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
     __syncwarp();
     uint32_t phase0 = 0, phase1 = 0;
     const int64_t total = (int64_t)P.counters[kCScoreTotal];
+    const int64_t warps_total = (int64_t)gridDim.x * kScoreWarps;
+    // Guided self-scheduling: a warp takes a run of consecutive items (chunks of
+    // one hypothesis block in order), long while much work remains and single
+    // items at the tail; hypotheses stay in registers while the run stays in
+    // one block.
+    int64_t run_next = 0, run_end = 0;
+    int cur_a = -1, cur_hb = -1;
+    uint64_t c[HP][12];
     for (;;) {
-        int64_t item = 0;
-        if (lane == 0) item = (int64_t)atomicAdd(&P.counters[kCScoreNext], 1ull);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= total) break;
+        if (run_next >= run_end) {
+            int64_t start = 0, len = 0;
+            if (lane == 0) {
+                const int64_t done = (int64_t)*(volatile unsigned long long *)&P.counters[kCScoreNext];
+                len = max((int64_t)1, min((int64_t)8, (total - done) / (4 * warps_total)));
+                start = (int64_t)atomicAdd(&P.counters[kCScoreNext], (unsigned long long)len);
+            }
+            start = __shfl_sync(0xffffffffu, start, 0);
+            len = __shfl_sync(0xffffffffu, len, 0);
+            if (start >= total) break;
+            run_next = start;
+            run_end = min(total, start + len);
+        }
+        const int64_t item = run_next++;
         const int a = find_segment(P.item_prefix, P.n_active, item);
         FrameDev &f = P.frames[P.active[a]];
         const int64_t local = item - P.item_prefix[a];
@@ -608,18 +662,22 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
         const int hb = (int)(local / nch), ch = (int)(local % nch);
         const int nh = f.hyp_count;
         const int64_t hbase = f.hyp_base;
-        // Hypotheses: lane owns HR consecutive ones.
-        uint64_t c[HP][12];
+        // Hypotheses: lane owns HR consecutive ones (reloaded when the block changes).
+        if (a != cur_a || hb != cur_hb) {
+#pragma unroll
+            for (int h = 0; h < HP; ++h) {
+                const int i0 = hb * HB + lane * HR + 2 * h, i1 = i0 + 1;
+                const float *A = P.hP32 + 12 * (hbase + i0), *Bp = P.hP32 + 12 * (hbase + i1);
+#pragma unroll
+                for (int e = 0; e < 12; ++e)
+                    c[h][e] = f2pack(i0 < nh ? __ldg(A + e) : 0.0f, i1 < nh ? __ldg(Bp + e) : 0.0f);
+            }
+            cur_a = a;
+            cur_hb = hb;
+        }
         uint64_t acc[HP];
 #pragma unroll
-        for (int h = 0; h < HP; ++h) {
-            const int i0 = hb * HB + lane * HR + 2 * h, i1 = i0 + 1;
-            const float *A = P.hP32 + 12 * (hbase + i0), *Bp = P.hP32 + 12 * (hbase + i1);
-#pragma unroll
-            for (int e = 0; e < 12; ++e)
-                c[h][e] = f2pack(i0 < nh ? __ldg(A + e) : 0.0f, i1 < nh ? __ldg(Bp + e) : 0.0f);
-            acc[h] = 0ull;
-        }
+        for (int h = 0; h < HP; ++h) acc[h] = 0ull;
         const int b0 = ch * f.chunk_blocks;
         const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
         const int nb = b1 - b0;
@@ -640,7 +698,7 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
             if (s) phase1 ^= 1u; else phase0 ^= 1u;
             const int64_t pt0 = (int64_t)(b0 + i) * kSub;
             const int valid = (int)(f.n - pt0 < kSub ? f.n - pt0 : kSub);
-            score_block<HP>(s ? st1 : st0, valid, c, acc);
+            score_block<HP, PP>(s ? st1 : st0, valid, c, acc);
             __syncwarp();
             if (lane == 0 && i + 2 < nb) {
                 fence_proxy_async();
@@ -1031,9 +1089,6 @@ __global__ void __launch_bounds__(1024) k_inliers(Pools P) {
             P.lX64[3 * o] = X0;
             P.lX64[3 * o + 1] = X1;
             P.lX64[3 * o + 2] = X2;
-            P.lA32[o] = make_float4((float)(X0 - f.centre[0]), (float)(X1 - f.centre[1]),
-                                    (float)(X2 - f.centre[2]), (float)u);
-            P.lB32[o] = make_float4((float)X0, (float)X1, (float)X2, (float)v);
         }
         written += tot;
     }
@@ -1075,267 +1130,262 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, do
 
 constexpr int kLMCluster = 8;  // CTAs cooperating on one frame's LM
 
-// Shared state of one LM cluster. Rank 0 owns the solver state; the other
-// ranks read it through distributed shared memory after each cluster barrier.
-struct LMShared {
-    double part[28];        // this CTA's partial sums (27 accumulators, or the cost in [0])
-    double q[4], t[3], qn[4], tn[3];
-    double cost, lambda;
-    double J[36], g[6];
-    int brk, recompute, iters, invalid;
-};
+// Relative resolution of a gradient component accumulated in FP32: a few ulps
+// of the sum of the magnitudes of its terms.
+constexpr double kGradNoiseUlps = 8.0 * 5.9604644775390625e-08;  // 8 * 2^-24
 
-// FP64 Cauchy cost of (q, t) over inliers [i0, i1) (jaco.cuh:31-104).
-__device__ double lm_cost_slice(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q,
-                                const double *t, const double *cam, double inv_sq_thr, double *scratch,
-                                double *red) {
-    double acc[1] = {0.0};
+// One pass over inliers [i0, i1) at pose (q, t): the FP64 Cauchy cost
+// (jaco.cuh:31-104) and, from the same FP64 residuals, the J^T W J lower
+// triangle (jaco.cuh:173-200) and J^T W r (:202-209) accumulated in FP32 with
+// Kahan compensation, plus the magnitude sums of the J^T W r terms. The
+// Jacobian uses the world coordinates of the reference's parameterisation
+// (rotation post-multiplied, translation t + R dt). out[0] = cost,
+// out[1..27] = accumulators, out[28..33] = magnitude sums (block totals).
+__device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q, const double *t,
+                        const double *cam, double inv_sq_thr, double *scratch, double *out) {
+    double R[9];
+    quat_to_rotmat(q, R);
+    const float r00 = (float)R[0], r01 = (float)R[1], r02 = (float)R[2], r10 = (float)R[3], r11 = (float)R[4],
+                r12 = (float)R[5], r20 = (float)R[6], r21 = (float)R[7], r22 = (float)R[8];
+    const float fx = (float)cam[0], fy = (float)cam[1];
+    const float isq = (float)inv_sq_thr;
+    double cost = 0.0;
+    float Sv[27], Cc[27], Ab[6];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) Ab[k] = 0.0f;
     for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int64_t o = base + i;
-        double Z[3];
-        quat_rotate(q, P.lX64[3 * o], P.lX64[3 * o + 1], P.lX64[3 * o + 2], Z);
-        Z[0] += t[0];
-        Z[1] += t[1];
-        Z[2] += t[2];
-        const bool valid = Z[2] >= 0.0;
-        const double inv_z = valid ? 1.0 / Z[2] : 0.0;
-        double p0 = Z[0] * inv_z, p1 = Z[1] * inv_z;
-        p0 = cam[0] * p0 + cam[2];
-        p1 = cam[1] * p1 + cam[3];
-        const double r0 = p0 - P.lx64[2 * o], r1 = p1 - P.lx64[2 * o + 1];
+        const double X0d = P.lX64[3 * o], X1d = P.lX64[3 * o + 1], X2d = P.lX64[3 * o + 2];
+        const double Z0 = R[0] * X0d + R[1] * X1d + R[2] * X2d + t[0];
+        const double Z1 = R[3] * X0d + R[4] * X1d + R[5] * X2d + t[1];
+        const double Z2 = R[6] * X0d + R[7] * X1d + R[8] * X2d + t[2];
+        const bool valid = Z2 >= 0.0;
+        const double inv_z = 1.0 / Z2;
+        const double z0d = Z0 * inv_z, z1d = Z1 * inv_z;
+        const double r0 = (cam[0] * z0d + cam[2]) - P.lx64[2 * o];
+        const double r1 = (cam[1] * z1d + cam[3]) - P.lx64[2 * o + 1];
         const double r_squared = r0 * r0 + r1 * r1;
-        acc[0] += valid ? log1p(r_squared * inv_sq_thr) : 0.0;
+        cost += valid ? log1p(r_squared * inv_sq_thr) : 0.0;
+        // FP32 Jacobian from the FP64 projection and residual.
+        const float iz = (float)inv_z, z0 = (float)z0d, z1 = (float)z1d;
+        const float rx = (float)r0, ry = (float)r1;
+        const float r2 = (float)r_squared;
+        float wgt = isq / (1.0f + r2 * isq);
+        wgt = fmaxf(wgt, FLT_MIN);
+        const float wv = valid ? wgt : 0.0f;
+        const float a0 = fx * iz, a2 = -fx * z0 * iz;
+        const float b1 = fy * iz, b2 = -fy * z1 * iz;
+        const float dZ00 = a0 * r00 + a2 * r20, dZ01 = a0 * r01 + a2 * r21, dZ02 = a0 * r02 + a2 * r22;
+        const float dZ10 = b1 * r10 + b2 * r20, dZ11 = b1 * r11 + b2 * r21, dZ12 = b1 * r12 + b2 * r22;
+        const float d00 = wv * (dZ00 * dZ00 + dZ10 * dZ10);
+        const float d10 = wv * (dZ01 * dZ00 + dZ11 * dZ10);
+        const float d11 = wv * (dZ01 * dZ01 + dZ11 * dZ11);
+        const float d20 = wv * (dZ02 * dZ00 + dZ12 * dZ10);
+        const float d21 = wv * (dZ02 * dZ01 + dZ12 * dZ11);
+        const float d22 = wv * (dZ02 * dZ02 + dZ12 * dZ12);
+        const float X0 = (float)X0d, X1 = (float)X1d, X2 = (float)X2d;
+        const float wx = wv * rx, wy = wv * ry;
+        const float v[27] = {
+            X2 * (X2 * d11 - X1 * d21) + X1 * (X1 * d22 - X2 * d21),
+            -X2 * (X2 * d10 - X0 * d21) - X1 * (X0 * d22 - X2 * d20),
+            X1 * (X0 * d21 - X1 * d20) - X2 * (X0 * d11 - X1 * d10),
+            X1 * d20 - X2 * d10,
+            X1 * d21 - X2 * d11,
+            X1 * d22 - X2 * d21,
+            X2 * (X2 * d00 - X0 * d20) + X0 * (X0 * d22 - X2 * d20),
+            -X2 * (X1 * d00 - X0 * d10) - X0 * (X0 * d21 - X1 * d20),
+            X2 * d00 - X0 * d20,
+            X2 * d10 - X0 * d21,
+            X2 * d20 - X0 * d22,
+            X1 * (X1 * d00 - X0 * d10) + X0 * (X0 * d11 - X1 * d10),
+            X0 * d10 - X1 * d00,
+            X0 * d11 - X1 * d10,
+            X0 * d21 - X1 * d20,
+            d00, d10, d20, d11, d21, d22,
+            wx * (X1 * dZ02 - X2 * dZ01) + wy * (X1 * dZ12 - X2 * dZ11),
+            -wx * (X0 * dZ02 - X2 * dZ00) - wy * (X0 * dZ12 - X2 * dZ10),
+            wx * (X0 * dZ01 - X1 * dZ00) + wy * (X0 * dZ11 - X1 * dZ10),
+            dZ00 * wx + dZ10 * wy,
+            dZ01 * wx + dZ11 * wy,
+            dZ02 * wx + dZ12 * wy};
+#pragma unroll
+        for (int k = 0; k < 27; ++k) kahan_add(Sv[k], Cc[k], v[k]);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) Ab[k] += fabsf(v[21 + k]);
     }
-    block_sum_d<1>(acc, scratch, red);
-    return red[0];
+    double dv[34];
+    dv[0] = cost;
+#pragma unroll
+    for (int k = 0; k < 27; ++k) dv[1 + k] = (double)Sv[k] - (double)Cc[k];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) dv[28 + k] = (double)Ab[k];
+    block_sum_d<34>(dv, scratch, out);
 }
 
-// Levenberg-Marquardt with the control flow of lm.cuh:15-171 (damping, accept
-// rule, lambda schedule, the removal of damping after a rejected step, and both
-// stop tests), one frame per cluster of CL CTAs, each owning a slice of
-// the inliers. J^T W J (lower triangle, jaco.cuh:173-200) and J^T W r
-// (:202-209) are accumulated per thread in FP32 with Kahan compensation from
-// centred coordinates and summed across the block and cluster in FP64 in a
-// fixed order; the 6x6 Cholesky (lm_utils.cuh:14-100), the step and the cost
-// used for acceptance are FP64.
+// 6x6 Cholesky solve of the damped normal equations (lm_utils.cuh:14-100),
+// non-positive pivots replaced by 1e-15 as there, with reciprocal pivots.
+__device__ __forceinline__ void cholesky_solve6(const double *A, const double *b, double *x) {
+    double L[36], inv[6], y[6];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j <= i; ++j) {
+            double sum = 0.0;
+            for (int k = 0; k < j; ++k) sum += L[i * 6 + k] * L[j * 6 + k];
+            if (i == j) {
+                double val = A[i * 6 + i] - sum;
+                if (val <= 0.0) val = 1e-15;
+                L[i * 6 + i] = sqrt(val);
+                inv[i] = 1.0 / L[i * 6 + i];
+            } else {
+                L[i * 6 + j] = (A[i * 6 + j] - sum) * inv[j];
+            }
+        }
+    for (int i = 0; i < 6; ++i) {
+        double sum = 0.0;
+        for (int j = 0; j < i; ++j) sum += L[i * 6 + j] * y[j];
+        y[i] = (b[i] - sum) * inv[i];
+    }
+    for (int i = 5; i >= 0; --i) {
+        double sum = 0.0;
+        for (int j = i + 1; j < 6; ++j) sum += L[j * 6 + i] * x[j];
+        x[i] = (y[i] - sum) * inv[i];
+    }
+}
+
+// Levenberg-Marquardt with the control flow of lm.cuh:15-171 -- damping, the
+// accept rule, the lambda schedule, the removal of damping after a rejected
+// step, and both stop tests -- one frame per cluster of CL CTAs, each owning a
+// slice of the inliers. Every candidate pose gets one fused pass (cost and, for
+// the case it is accepted, the normal equations at it), so an iteration costs
+// one pass and two cluster barriers. Sums cross the block and cluster in FP64 in
+// a fixed order; the solve, the step and the acceptance test are FP64.
 template <int CL>
 __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    __shared__ double scratch[32 * 27];
-    __shared__ double red[27];
-    __shared__ LMShared S;
-    __shared__ float R32[9], tc32[3];
+    __shared__ double scratch[32 * 34];
+    __shared__ double part[34];   // this CTA's pass totals
+    __shared__ double tot[34];    // rank 0: cluster totals
+    __shared__ double J[36], g[6], Jc[28], q[4], t[3], qn[4], tn[3];
+    __shared__ double cost, lambda;
+    __shared__ int brk, recompute, iters, invalid;
+    __shared__ double pq[4], pt[3];  // the pose every CTA evaluates next
+    __shared__ int pbrk;
     const int rank = (int)cluster.block_rank();
     FrameDev &f = P.frames[slot];
-    LMShared *L0 = cluster.map_shared_rank(&S, 0);
     FrameResult &res = P.results[slot];
     const int64_t base = f.blk_off * kSub;
     const int64_t n = f.num_inliers;
     const int64_t i0 = n * rank / CL, i1 = n * (rank + 1) / CL;
     const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
-    const float camf[4] = {(float)cam[0], (float)cam[1], (float)cam[2], (float)cam[3]};
     const double inv_sq_thr = f.lm_inv_sq_thr;
-    const float inv_sq_thr_f = (float)inv_sq_thr;
     const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
-    __shared__ double q[4], t[3], qn[4], tn[3];
+
+    auto cluster_totals = [&]() {  // after lm_pass: every CTA's part -> rank 0's tot
+        cluster.sync();
+        if (rank == 0 && threadIdx.x < 34) {
+            double acc = 0.0;
+            for (int r = 0; r < CL; ++r) acc += cluster.map_shared_rank(part, r)[threadIdx.x];
+            tot[threadIdx.x] = acc;
+        }
+        __syncthreads();
+    };
+
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 4; ++k) q[k] = res.q[k];
-        for (int k = 0; k < 3; ++k) t[k] = res.t[k];
+        for (int k = 0; k < 4; ++k) pq[k] = res.q[k];
+        for (int k = 0; k < 3; ++k) pt[k] = res.t[k];
     }
     __syncthreads();
-    // initial cost
-    double c = 0.0;
-    if (max_it > 0) c = lm_cost_slice(P, base, i0, i1, q, t, cam, inv_sq_thr, scratch, red);
-    if (threadIdx.x == 0) S.part[0] = c;
-    cluster.sync();
+    if (max_it > 0) lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, scratch, part);
+    else if (threadIdx.x < 34) part[threadIdx.x] = 0.0;
+    __syncthreads();
+    cluster_totals();
     if (rank == 0 && threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int r = 0; r < CL; ++r) tot += cluster.map_shared_rank(&S, r)->part[0];
-        S.cost = tot;
-        S.lambda = f.lm_lambda0;
-        S.recompute = 1;
-        S.iters = 0;
-        S.invalid = 0;
-        S.brk = 0;
-        for (int k = 0; k < 4; ++k) S.q[k] = q[k];
-        for (int k = 0; k < 3; ++k) S.t[k] = t[k];
-        res.lm_cost0 = tot;
+        for (int k = 0; k < 4; ++k) q[k] = pq[k];
+        for (int k = 0; k < 3; ++k) t[k] = pt[k];
+        cost = tot[0];
+        for (int k = 0; k < 27; ++k) Jc[k] = tot[1 + k];
+        Jc[27] = 0.0;
+        lambda = f.lm_lambda0;
+        recompute = 1;
+        iters = 0;
+        invalid = 0;
+        res.lm_cost0 = cost;
     }
-    cluster.sync();
     for (int64_t it = 0; it < max_it; ++it) {
-        if (L0->recompute) {
-            if (threadIdx.x == 0) {
-                double R[9];
-                for (int k = 0; k < 4; ++k) q[k] = L0->q[k];
-                for (int k = 0; k < 3; ++k) t[k] = L0->t[k];
-                quat_to_rotmat(q, R);
-                for (int k = 0; k < 9; ++k) R32[k] = (float)R[k];
-                for (int r = 0; r < 3; ++r)
-                    tc32[r] = (float)(t[r] + R[3 * r] * f.centre[0] + R[3 * r + 1] * f.centre[1] +
-                                      R[3 * r + 2] * f.centre[2]);
-            }
-            __syncthreads();
-            float Sv[27], Cc[27];
-#pragma unroll
-            for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
-            const float r00 = R32[0], r01 = R32[1], r02 = R32[2], r10 = R32[3], r11 = R32[4], r12 = R32[5],
-                        r20 = R32[6], r21 = R32[7], r22 = R32[8];
-            const float t0 = tc32[0], t1 = tc32[1], t2 = tc32[2];
-            for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-                const float4 A = P.lA32[base + i], Bw = P.lB32[base + i];
-                const float Z0 = r00 * A.x + r01 * A.y + r02 * A.z + t0;
-                const float Z1 = r10 * A.x + r11 * A.y + r12 * A.z + t1;
-                const float Z2 = r20 * A.x + r21 * A.y + r22 * A.z + t2;
-                const float iz = 1.0f / Z2;
-                const float z0 = Z0 * iz, z1 = Z1 * iz;
-                const float rx = (camf[0] * z0 + camf[2]) - A.w;
-                const float ry = (camf[1] * z1 + camf[3]) - Bw.w;
-                const float r2 = rx * rx + ry * ry;
-                float wgt = inv_sq_thr_f / (1.0f + r2 * inv_sq_thr_f);
-                wgt = fmaxf(wgt, FLT_MIN);
-                const float wv = (Z2 >= 0.0f) ? wgt : 0.0f;
-                // dZ = (1/Z2) [fx 0 -fx z0; 0 fy -fy z1] R
-                const float a0 = camf[0] * iz, a2 = -camf[0] * z0 * iz;
-                const float b1 = camf[1] * iz, b2 = -camf[1] * z1 * iz;
-                const float dZ00 = a0 * r00 + a2 * r20, dZ01 = a0 * r01 + a2 * r21, dZ02 = a0 * r02 + a2 * r22;
-                const float dZ10 = b1 * r10 + b2 * r20, dZ11 = b1 * r11 + b2 * r21, dZ12 = b1 * r12 + b2 * r22;
-                const float d00 = wv * (dZ00 * dZ00 + dZ10 * dZ10);
-                const float d10 = wv * (dZ01 * dZ00 + dZ11 * dZ10);
-                const float d11 = wv * (dZ01 * dZ01 + dZ11 * dZ11);
-                const float d20 = wv * (dZ02 * dZ00 + dZ12 * dZ10);
-                const float d21 = wv * (dZ02 * dZ01 + dZ12 * dZ11);
-                const float d22 = wv * (dZ02 * dZ02 + dZ12 * dZ12);
-                const float X0 = Bw.x, X1 = Bw.y, X2 = Bw.z;
-                const float wx = wv * rx, wy = wv * ry;
-                const float v[27] = {
-                    X2 * (X2 * d11 - X1 * d21) + X1 * (X1 * d22 - X2 * d21),
-                    -X2 * (X2 * d10 - X0 * d21) - X1 * (X0 * d22 - X2 * d20),
-                    X1 * (X0 * d21 - X1 * d20) - X2 * (X0 * d11 - X1 * d10),
-                    X1 * d20 - X2 * d10,
-                    X1 * d21 - X2 * d11,
-                    X1 * d22 - X2 * d21,
-                    X2 * (X2 * d00 - X0 * d20) + X0 * (X0 * d22 - X2 * d20),
-                    -X2 * (X1 * d00 - X0 * d10) - X0 * (X0 * d21 - X1 * d20),
-                    X2 * d00 - X0 * d20,
-                    X2 * d10 - X0 * d21,
-                    X2 * d20 - X0 * d22,
-                    X1 * (X1 * d00 - X0 * d10) + X0 * (X0 * d11 - X1 * d10),
-                    X0 * d10 - X1 * d00,
-                    X0 * d11 - X1 * d10,
-                    X0 * d21 - X1 * d20,
-                    d00, d10, d20, d11, d21, d22,
-                    wx * (X1 * dZ02 - X2 * dZ01) + wy * (X1 * dZ12 - X2 * dZ11),
-                    -wx * (X0 * dZ02 - X2 * dZ00) - wy * (X0 * dZ12 - X2 * dZ10),
-                    wx * (X0 * dZ01 - X1 * dZ00) + wy * (X0 * dZ11 - X1 * dZ10),
-                    dZ00 * wx + dZ10 * wy,
-                    dZ01 * wx + dZ11 * wy,
-                    dZ02 * wx + dZ12 * wy};
-#pragma unroll
-                for (int k = 0; k < 27; ++k) kahan_add(Sv[k], Cc[k], v[k]);
-            }
-            double dv[27];
-#pragma unroll
-            for (int k = 0; k < 27; ++k) dv[k] = (double)Sv[k] - (double)Cc[k];
-            block_sum_d<27>(dv, scratch, red);
-            if (threadIdx.x < 27) S.part[threadIdx.x] = red[threadIdx.x];
-            cluster.sync();
-            if (rank == 0 && threadIdx.x == 0) {
-                double tot[27];
-                for (int k = 0; k < 27; ++k) tot[k] = 0.0;
-                for (int r = 0; r < CL; ++r) {
-                    const LMShared *Sr = cluster.map_shared_rank(&S, r);
-                    for (int k = 0; k < 27; ++k) tot[k] += Sr->part[k];
-                }
-                // lower triangle in the reference's order (0,0),(1,0)..(5,0),(1,1)..(5,1),...
+        if (rank == 0 && threadIdx.x == 0) {
+            brk = 0;
+            if (recompute) {
+                // J from the pass at the current pose (lower triangle in the
+                // reference's order); gradient test of lm.cuh:243-248, which with
+                // J^T r summed in FP32 also accepts a gradient within the
+                // rounding of its terms.
                 const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
                                         {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
                                         {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
-                for (int k = 0; k < 36; ++k) S.J[k] = 0.0;
-                for (int k = 0; k < 21; ++k) S.J[idx[k][0] * 6 + idx[k][1]] = tot[k];
-                double gn = 0.0;
+                for (int k = 0; k < 36; ++k) J[k] = 0.0;
+                for (int k = 0; k < 21; ++k) J[idx[k][0] * 6 + idx[k][1]] = Jc[k];
+                double gn = 0.0, noise = 0.0;
                 for (int k = 0; k < 6; ++k) {
-                    S.g[k] = tot[21 + k];
-                    gn += S.g[k] * S.g[k];
+                    g[k] = Jc[21 + k];
+                    gn += g[k] * g[k];
                 }
-                S.brk = sqrt(gn) < f.lm_grad_tol ? 1 : 0;
-            }
-        } else if (rank == 0 && threadIdx.x == 0) {
-            S.brk = 0;
-        }
-        if (rank == 0 && threadIdx.x == 0) {
-            for (int k = 0; k < 6; ++k) S.J[k * 7] += S.lambda;
-            double Lc[36];
-            for (int k = 0; k < 36; ++k) Lc[k] = 0.0;
-            for (int i = 0; i < 6; ++i)
-                for (int j = 0; j <= i; ++j) {
-                    double sum = 0.0;
-                    for (int k = 0; k < j; ++k) sum += Lc[i * 6 + k] * Lc[j * 6 + k];
-                    if (i == j) {
-                        double val = S.J[i * 6 + i] - sum;
-                        if (val <= 0.0) val = 1e-15;
-                        Lc[i * 6 + j] = sqrt(val);
-                    } else {
-                        Lc[i * 6 + j] = (S.J[i * 6 + j] - sum) / Lc[j * 6 + j];
-                    }
+                for (int k = 0; k < 6; ++k) {
+                    const double e = kGradNoiseUlps * tot[28 + k];
+                    noise += e * e;
                 }
-            double y[6], x[6];
-            for (int i = 0; i < 6; ++i) {
-                double sum = 0.0;
-                for (int j = 0; j < i; ++j) sum += Lc[i * 6 + j] * y[j];
-                y[i] = (S.g[i] - sum) / Lc[i * 6 + i];
+                if (sqrt(gn) < f.lm_grad_tol || sqrt(gn) <= sqrt(noise)) brk = 1;
             }
-            for (int i = 5; i >= 0; --i) {
-                double sum = 0.0;
-                for (int j = i + 1; j < 6; ++j) sum += Lc[j * 6 + i] * x[j];
-                x[i] = (y[i] - sum) / Lc[i * 6 + i];
-            }
+            for (int k = 0; k < 6; ++k) J[k * 7] += lambda;
+            double x[6];
+            cholesky_solve6(J, g, x);
             double sn = 0.0;
             for (int k = 0; k < 6; ++k) {
                 x[k] = -1 * x[k];
                 sn += x[k] * x[k];
             }
-            if (sqrt(sn) < f.lm_step_tol) S.brk = 1;
-            quat_step_post(S.q, x, S.qn);
+            if (sqrt(sn) < f.lm_step_tol) brk = 1;
+            quat_step_post(q, x, qn);  // jaco.cuh:288-299
             double dt[3];
-            quat_rotate(S.q, x[3], x[4], x[5], dt);
-            for (int k = 0; k < 3; ++k) S.tn[k] = S.t[k] + dt[k];
+            quat_rotate(q, x[3], x[4], x[5], dt);
+            for (int k = 0; k < 3; ++k) tn[k] = t[k] + dt[k];
         }
         cluster.sync();
-        if (L0->brk) break;
         if (threadIdx.x == 0) {
-            for (int k = 0; k < 4; ++k) qn[k] = L0->qn[k];
-            for (int k = 0; k < 3; ++k) tn[k] = L0->tn[k];
+            pbrk = cluster.map_shared_rank(&brk, 0)[0];
+            const double *rq = cluster.map_shared_rank(qn, 0), *rt = cluster.map_shared_rank(tn, 0);
+            for (int k = 0; k < 4; ++k) pq[k] = rq[k];
+            for (int k = 0; k < 3; ++k) pt[k] = rt[k];
         }
         __syncthreads();
-        const double cs = lm_cost_slice(P, base, i0, i1, qn, tn, cam, inv_sq_thr, scratch, red);
-        if (threadIdx.x == 0) S.part[0] = cs;
-        cluster.sync();
+        if (pbrk) break;
+        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, scratch, part);
+        __syncthreads();
+        cluster_totals();
         if (rank == 0 && threadIdx.x == 0) {
-            double cn = 0.0;
-            for (int r = 0; r < CL; ++r) cn += cluster.map_shared_rank(&S, r)->part[0];
-            if (cn < S.cost) {
-                for (int k = 0; k < 4; ++k) S.q[k] = S.qn[k];
-                for (int k = 0; k < 3; ++k) S.t[k] = S.tn[k];
-                S.lambda = fmax(f.lm_min_lambda, S.lambda / 10);
-                S.cost = cn;
-                S.recompute = 1;
+            if (tot[0] < cost) {
+                for (int k = 0; k < 4; ++k) q[k] = qn[k];
+                for (int k = 0; k < 3; ++k) t[k] = tn[k];
+                lambda = fmax(f.lm_min_lambda, lambda / 10);
+                cost = tot[0];
+                for (int k = 0; k < 27; ++k) Jc[k] = tot[1 + k];
+                recompute = 1;
             } else {
-                ++S.invalid;
-                for (int k = 0; k < 6; ++k) S.J[k * 7] -= S.lambda;
-                S.lambda = fmin(f.lm_max_lambda, S.lambda * 10);
-                S.recompute = 0;
+                ++invalid;
+                for (int k = 0; k < 6; ++k) J[k * 7] -= lambda;
+                lambda = fmin(f.lm_max_lambda, lambda * 10);
+                recompute = 0;
             }
-            ++S.iters;
+            ++iters;
         }
-        cluster.sync();
     }
     if (rank == 0 && threadIdx.x == 0) {
-        for (int k = 0; k < 4; ++k) res.q[k] = S.q[k];
-        for (int k = 0; k < 3; ++k) res.t[k] = S.t[k];
-        res.lm_iters = S.iters;
-        res.lm_invalid = S.invalid;
-        res.lm_cost = S.cost;
+        for (int k = 0; k < 4; ++k) res.q[k] = q[k];
+        for (int k = 0; k < 3; ++k) res.t[k] = t[k];
+        res.lm_iters = iters;
+        res.lm_invalid = invalid;
+        res.lm_cost = cost;
         res.samples = f.samples_done;
         res.rounds = f.rounds_done;
         res.hypotheses = f.hyps_done;
@@ -1452,8 +1502,6 @@ __global__ void k_lm_pack(Pools P) {
         P.lX64[3 * p] = X0;
         P.lX64[3 * p + 1] = X1;
         P.lX64[3 * p + 2] = X2;
-        P.lA32[p] = make_float4((float)(X0 - c0), (float)(X1 - c1), (float)(X2 - c2), (float)u);
-        P.lB32[p] = make_float4((float)X0, (float)X1, (float)X2, (float)v);
     }
 }
 
