@@ -47,8 +47,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
-    ap.add_argument("--case", default="", choices=["", "scoring"],
-                    help="scoring: one N=20000 frame, exactly 4096 samples (small case for ncu)")
+    ap.add_argument("--case", default="", choices=["", "scoring", "batch64"],
+                    help="scoring: one N=20000 frame, exactly 4096 samples; batch64: the batched workload's "
+                         "first 64 frames in one graph (small cases for ncu)")
     return ap.parse_args()
 
 
@@ -292,10 +293,35 @@ def run_case_scoring(args):
     ctx.close()
 
 
+def run_case_batch64(args):
+    """First 64 frames of the batched workload, one captured graph per step."""
+    from turboransac_b200 import Batch, Context, RansacOptions_cuda, scenes
+    frames = scenes.batched_frames(64)
+    ctx = Context(0, 2 << 30)
+    b = Batch(ctx, frames, RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0))
+    ms = []
+    for i in range(args.warmup + args.steps):
+        b.run()
+        b.sync()
+        if i >= args.warmup:
+            ms.append(b.results()[0]["gpu_ms"])
+    # One host-stepped run (the kernels of the captured graph, launched one by
+    # one): per-kernel CUDA-event times, and launches a profiler can attach to.
+    prof, pairs = b.profile()
+    print(json.dumps({"case": "batch64", "frames": 64, "ms_per_batch": statistics.mean(ms),
+                      "frames_per_s": 64 / (statistics.mean(ms) / 1000.0), "pairs": pairs,
+                      "kernels_ms": {k: v[0] for k, v in prof.items()}}), flush=True)
+    b.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.case == "scoring":
         run_case_scoring(args)
+        return
+    if args.case == "batch64":
+        run_case_batch64(args)
         return
     world, rank, local, pg = dist_setup(args)
     if args.impl == "reference":
