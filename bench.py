@@ -261,6 +261,7 @@ def run_reference(args, world, rank):
         if i >= args.warmup:
             times.append(dt)
     fps = m * len(times) / sum(times)
+    rcuda = reference_cuda_build(frames, args)
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
@@ -268,8 +269,36 @@ def run_reference(args, world, rank):
             "impl": "reference",
             "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
                              "sample": f"first {m} frames of the batched workload per step, {cores} threads"},
-            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_cuda": rcuda}
     print(json.dumps(line), flush=True)
+
+
+def reference_cuda_build(frames, args):
+    """The reference's own CUDA build (its src/*.cu for sm_100a) on this GPU: one
+    estimate_absolute_pose_cuda call per frame, as its evaluator loops, on the
+    batched workload and on plain single frames (N=2000, 40 % inliers)."""
+    import numpy as np
+    import torch
+
+    from oracle import refcuda
+    from turboransac_b200 import scenes
+    if not refcuda.available():
+        return {"unavailable": "oracle/_ref/tbr_refcuda not built (make -C oracle refcuda needs the reference tree)"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+
+    def measure(fr):
+        r = refcuda.run(fr, warmup=8)
+        ok = [scenes.pose_error(scenes.quat_to_rotmat(q), t, f.R_gt, f.t_gt) for f, q, t in zip(fr, r["q"], r["t"])]
+        return {"frames": len(fr), "frames_per_s": len(fr) / (float(r["ms"].sum()) / 1000.0),
+                "p50_ms": float(np.percentile(r["ms"], 50)), "p99_ms": float(np.percentile(r["ms"], 99)),
+                "success_rate": float(np.mean([a < 5.0 and b < 5.0 for a, b in ok]))}
+
+    return {"build": "reference src/entry.cu, turbo_ransac.cu, ba.cu, nvcc sm_100a -O3 -rdc=true",
+            "timing": "host clock around each call; the reference's stdout sent to /dev/null",
+            "batched_workload": measure(frames),
+            "plain_frame": measure([scenes.plain_frame(i) for i in range(64)])}
 
 
 def run_case_scoring(args):

@@ -36,7 +36,7 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REF_SRC)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "refcuda"], check=True)
 
 
 class RansacCfg(C.Structure):
