@@ -167,6 +167,9 @@ class Engine {
     size_t h_stage_bytes = 0;
     unsigned long long *h_counters = nullptr;
     int32_t *d_active = nullptr;
+    FrameDev *d_admit = nullptr;         // admission staging (device side)
+    FrameResult *d_res_stage = nullptr;  // packed results of one download
+    int32_t *d_res_slots = nullptr;      // slot list of that download
     int32_t *d_replay = nullptr;
     int64_t d_replay_cap = 0;
     int score_grid[4] = {0, 0, 0, 0};  // (HP, PP) = (1,4), (2,2), (2,4), (4,2)
@@ -203,7 +206,7 @@ class Engine {
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
         // Split: 30 % hypotheses, the rest points, after the per-frame state.
-        const size_t per_frame = sizeof(FrameDev) + sizeof(FrameResult) + sizeof(int32_t) + 64;
+        const size_t per_frame = 2 * (sizeof(FrameDev) + sizeof(FrameResult)) + sizeof(int32_t) + 64;
         P.cand_cap = std::max<int64_t>(16384, (int64_t)max_frames * 256);
         const size_t per_cand = 4 + 8 + 8 + 4 + (size_t)kMaxRChunks * 12;
         const size_t fixed = (size_t)max_frames * per_frame + (size_t)P.cand_cap * per_cand +
@@ -225,6 +228,9 @@ class Engine {
         add((void **)&P.frames, sizeof(FrameDev) * max_frames);
         add((void **)&P.results, sizeof(FrameResult) * max_frames);
         add((void **)&d_active, sizeof(int32_t) * kMaxActive);
+        add((void **)&d_admit, sizeof(FrameDev) * kMaxActive);
+        add((void **)&d_res_stage, sizeof(FrameResult) * kMaxActive);
+        add((void **)&d_res_slots, sizeof(int32_t) * kMaxActive);
         add((void **)&P.uv64, 16 * np);
         add((void **)&P.X64, 24 * np);
         add((void **)&P.xn64, 16 * np);
@@ -441,7 +447,43 @@ class Engine {
     }
 };
 
-// Uploads frames into slots (host -> device through pinned staging).
+// Host copies into pinned staging, split over threads when the batch is large
+// (a single core's memcpy bandwidth is well below the link's).
+struct CopyJob {
+    void *dst;
+    const void *src;
+    size_t bytes;
+};
+static void parallel_copy(const std::vector<CopyJob> &jobs) {
+    constexpr size_t kChunk = 1 << 20;
+    size_t total = 0;
+    for (auto &j : jobs) total += j.bytes;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::min<size_t>(std::min(8u, hw), total / (4 * kChunk));
+    if (T <= 1) {
+        for (auto &j : jobs) std::memcpy(j.dst, j.src, j.bytes);
+        return;
+    }
+    std::vector<CopyJob> pieces;
+    for (auto &j : jobs)
+        for (size_t o = 0; o < j.bytes; o += kChunk)
+            pieces.push_back({(char *)j.dst + o, (const char *)j.src + o, std::min(kChunk, j.bytes - o)});
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < pieces.size();)
+            std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < T; ++t) th.emplace_back(work);
+    work();
+    for (auto &x : th) x.join();
+}
+
+// Uploads frames into slots (host -> device through pinned staging). Frames
+// whose point blocks are adjacent in the pool form one run; the staging area
+// mirrors the pool's layout inside a run, so a run costs one copy per array.
+// The frame records go up as one array and are scattered by one kernel; on
+// return d_active[0..n) holds the new slots.
 static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
                                std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
     if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
@@ -449,18 +491,19 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
     size_t stage = 0;
     int64_t replay_total = 0;
     for (auto &f : fr) {
-        stage += r256(16 * (size_t)f.n) + r256(24 * (size_t)f.n);
+        const size_t pts = (size_t)((f.n + kSub - 1) / kSub) * kSub;
+        stage += r256(16 * pts) + r256(24 * pts);
         replay_total += f.replay ? f.replay_count : 0;
     }
-    stage += fr.size() * r256(sizeof(FrameDev)) + r256(4 * fr.size()) + 256;
+    stage += r256(sizeof(FrameDev) * fr.size()) + r256(4 * fr.size()) + 256;
     tbr_status st = E.ensure_stage(stage);
     if (st) return st;
     if (replay_total) {
         st = E.ensure_replay(replay_total);
         if (st) return st;
     }
-    char *h = (char *)E.h_stage;
     std::vector<FrameDev> devs;
+    std::vector<int64_t> offs;
     int64_t rep_off = 0;
     max_n = 0;
     for (auto &f : fr) {
@@ -475,6 +518,7 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         const int slot = E.free_slots.back();
         E.free_slots.pop_back();
         slots.push_back(slot);
+        offs.push_back(off);
         const int32_t *d_rep = nullptr;
         if (f.replay) {
             d_rep = E.d_replay + 3 * rep_off;
@@ -482,26 +526,78 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
             rep_off += f.replay_count;
         }
         devs.push_back(E.make_frame(f, off, o, d_rep));
-        const int64_t p0 = off * kSub;
-        std::memcpy(h, f.uv, 16 * f.n);
-        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), h, 16 * f.n, cudaMemcpyHostToDevice, E.stream));
-        h += (16 * f.n + 255) & ~int64_t(255);
-        std::memcpy(h, f.xyz, 24 * f.n);
-        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), h, 24 * f.n, cudaMemcpyHostToDevice, E.stream));
-        h += (24 * f.n + 255) & ~int64_t(255);
         max_n = std::max(max_n, f.n);
     }
-    for (size_t i = 0; i < slots.size(); ++i) {
-        FrameDev *hd = (FrameDev *)h;
-        *hd = devs[i];
-        TBR_CUDA(cudaMemcpyAsync(E.P.frames + slots[i], hd, sizeof(FrameDev), cudaMemcpyHostToDevice, E.stream));
-        h += (sizeof(FrameDev) + 255) & ~size_t(255);
+    // Runs of adjacent frames: [first frame, last frame], block range [b0, b1).
+    struct Run {
+        size_t f0, f1;
+        int64_t b0, b1;
+        char *huv, *hxyz;
+    };
+    std::vector<Run> runs;
+    for (size_t i = 0; i < fr.size(); ++i) {
+        const int64_t nb = devs[i].n_blocks;
+        if (!runs.empty() && runs.back().b1 == offs[i]) {
+            runs.back().f1 = i;
+            runs.back().b1 += nb;
+        } else {
+            runs.push_back({i, i, offs[i], offs[i] + nb, nullptr, nullptr});
+        }
     }
+    char *h = (char *)E.h_stage;
+    std::vector<CopyJob> jobs;
+    for (auto &r : runs) {
+        const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
+        r.huv = h;
+        h += r256(16 * pts);
+        r.hxyz = h;
+        h += r256(24 * pts);
+        for (size_t i = r.f0; i <= r.f1; ++i) {
+            const size_t p = (size_t)(offs[i] - r.b0) * kSub;
+            jobs.push_back({r.huv + 16 * p, fr[i].uv, 16 * (size_t)fr[i].n});
+            jobs.push_back({r.hxyz + 24 * p, fr[i].xyz, 24 * (size_t)fr[i].n});
+        }
+    }
+    FrameDev *hd = (FrameDev *)h;
+    h += r256(sizeof(FrameDev) * fr.size());
     int32_t *ha = (int32_t *)h;
-    for (size_t i = 0; i < slots.size(); ++i) ha[i] = slots[i];
-    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * slots.size(), cudaMemcpyHostToDevice, E.stream));
+    for (size_t i = 0; i < fr.size(); ++i) {
+        hd[i] = devs[i];
+        ha[i] = slots[i];
+    }
+    parallel_copy(jobs);
+    for (auto &r : runs) {
+        const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
+        const size_t p0 = (size_t)r.b0 * kSub;
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), r.huv, 16 * pts, cudaMemcpyHostToDevice, E.stream));
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), r.hxyz, 24 * pts, cudaMemcpyHostToDevice, E.stream));
+    }
+    TBR_CUDA(cudaMemcpyAsync(E.d_admit, hd, sizeof(FrameDev) * fr.size(), cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * fr.size(), cudaMemcpyHostToDevice, E.stream));
+    k_admit_frames<<<(int)fr.size(), 128, 0, E.stream>>>(E.P.frames, E.d_admit, E.d_active, (int)fr.size());
+    TBR_CUDA(cudaGetLastError());
     E.P.n_active = (int32_t)slots.size();
     if (host_devs) *host_devs = devs;
+    return TBR_OK;
+}
+
+// Results of `slots` into `out` (host), through one packed download.
+static tbr_status fetch_results(Engine &E, const std::vector<int> &slots, FrameResult *out) {
+    const size_t n = slots.size();
+    if (n == 0) return TBR_OK;
+    tbr_status st = E.ensure_stage(sizeof(FrameResult) * n + 4 * n + 512);
+    if (st) return st;
+    FrameResult *hres = (FrameResult *)E.h_stage;
+    int32_t *hs = (int32_t *)((char *)E.h_stage + ((sizeof(FrameResult) * n + 255) & ~size_t(255)));
+    for (size_t i = 0; i < n; ++i) hs[i] = slots[i];
+    int32_t *ds = E.d_res_slots;
+    TBR_CUDA(cudaMemcpyAsync(ds, hs, 4 * n, cudaMemcpyHostToDevice, E.stream));
+    k_gather_results<<<(int)std::min<size_t>(1024, (n * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0, E.stream>>>(
+        E.P.results, ds, (int)n, E.d_res_stage);
+    TBR_CUDA(cudaGetLastError());
+    TBR_CUDA(cudaMemcpyAsync(hres, E.d_res_stage, sizeof(FrameResult) * n, cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    std::memcpy(out, hres, sizeof(FrameResult) * n);
     return TBR_OK;
 }
 
@@ -600,19 +696,15 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
     E.pp = o.pp;
     st = E.run(slots, o.hr, 100000, steps_out);
     TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
-    if (st == TBR_OK) st = E.ensure_stage(sizeof(FrameResult) * slots.size() + 256);
     if (st == TBR_OK) {
         res.resize(fr.size());
-        FrameResult *hres = (FrameResult *)E.h_stage;
-        for (size_t i = 0; i < slots.size(); ++i)
-            TBR_CUDA(cudaMemcpyAsync(hres + i, E.P.results + slots[i], sizeof(FrameResult),
-                                     cudaMemcpyDeviceToHost, E.stream));
         for (size_t i = 0; i < slots.size(); ++i)
             if (i < masks.size() && masks[i])
                 TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + devs[i].blk_off * kSub, fr[i].n,
                                          cudaMemcpyDeviceToHost, E.stream));
-        TBR_CUDA(cudaStreamSynchronize(E.stream));
-        for (size_t i = 0; i < slots.size(); ++i) res[i] = hres[i];
+        st = fetch_results(E, slots, res.data());
+    }
+    if (st == TBR_OK) {
         float ms = 0.f;
         cudaEventElapsedTime(&ms, E.ev0, E.ev1);
         if (ms_out) *ms_out = ms;
@@ -1013,10 +1105,8 @@ tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results) {
     float ms = 0.f;
     if (b->launched) cudaEventElapsedTime(&ms, b->e0, b->e1);
     std::vector<FrameResult> r(b->slots.size());
-    for (size_t i = 0; i < b->slots.size(); ++i)
-        TBR_CUDA(cudaMemcpyAsync(&r[i], E.P.results + b->slots[i], sizeof(FrameResult), cudaMemcpyDeviceToHost,
-                                 E.stream));
-    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    tbr_status st = fetch_results(E, b->slots, r.data());
+    if (st) return st;
     for (size_t i = 0; i < b->slots.size(); ++i) {
         for (int k = 0; k < 4; ++k) results[i].q[k] = r[i].q[k];
         for (int k = 0; k < 3; ++k) results[i].t[k] = r[i].t[k];
@@ -1238,10 +1328,10 @@ static tbr_status server_step(tbr_server *s) {
         if (s->h_status[i] == kDone) fin.push_back(i);
     if (!fin.empty()) {
         std::vector<FrameResult> res(fin.size());
-        for (size_t k = 0; k < fin.size(); ++k)
-            TBR_CUDA(cudaMemcpyAsync(&res[k], E.P.results + s->resident[fin[k]].slot, sizeof(FrameResult),
-                                     cudaMemcpyDeviceToHost, E.stream));
-        TBR_CUDA(cudaStreamSynchronize(E.stream));
+        std::vector<int> fslots(fin.size());
+        for (size_t k = 0; k < fin.size(); ++k) fslots[k] = s->resident[fin[k]].slot;
+        tbr_status fst = fetch_results(E, fslots, res.data());
+        if (fst) return fst;
         for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &res[k], TBR_OK);
         std::vector<Resident> keep;
         std::vector<bool> gone(na, false);

@@ -1441,6 +1441,27 @@ __global__ void k_reset_frames(Pools P, const FrameDev *init) {
     if (a == 0 && threadIdx.x < kCNum) P.counters[threadIdx.x] = 0;
 }
 
+// Admission: staged[a] -> frames[slots[a]] (one upload for a whole batch).
+__global__ void k_admit_frames(FrameDev *frames, const FrameDev *staged, const int32_t *slots, int n) {
+    const int a = blockIdx.x;
+    if (a >= n) return;
+    const int4 *src = reinterpret_cast<const int4 *>(staged + a);
+    int4 *dst = reinterpret_cast<int4 *>(frames + slots[a]);
+    for (int i = threadIdx.x; i < (int)(sizeof(FrameDev) / 16); i += blockDim.x) dst[i] = src[i];
+}
+
+// Results of the frames in slots[0..n) packed into one array (one download).
+static_assert(sizeof(FrameResult) % 8 == 0, "FrameResult is copied in 8-byte words");
+__global__ void k_gather_results(const FrameResult *results, const int32_t *slots, int n, FrameResult *out) {
+    constexpr int W = (int)(sizeof(FrameResult) / 8);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)n * W;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int a = (int)(i / W), w = (int)(i % W);
+        reinterpret_cast<unsigned long long *>(out + a)[w] =
+            reinterpret_cast<const unsigned long long *>(results + slots[a])[w];
+    }
+}
+
 // ------------------------------------------------- standalone entry points --
 // get_inliers_mx (entry.cu:12-26) for a given pose over raw device arrays.
 __global__ void k_pose_mask(const double *xn, const double *X, int64_t n, const double *qt,
