@@ -171,6 +171,7 @@ def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
     import numpy as np
 
     from turboransac_b200 import Server, scenes
+    from turboransac_b200._lib import TbrError
     reqs = [scenes.serving_request(i) for i in range(pool)]
     arrivals = scenes.poisson_arrivals(rate, seconds, seed=11)
     srv = Server(ctx, budget_bytes=budget, max_slots=1024)
@@ -203,7 +204,14 @@ def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
             if dt <= 0:
                 break
             time.sleep(min(dt, 0.001))
-        ids[srv.submit(reqs[k % pool])] = k % pool
+        while True:
+            try:
+                ids[srv.submit(reqs[k % pool])] = k % pool
+                break
+            except TbrError as e:  # queue full: back off until the server drains
+                if "CAPACITY" not in str(e):
+                    raise
+                time.sleep(0.001)
     srv.drain()
     t_end = time.perf_counter()
     time.sleep(0.01)
@@ -211,6 +219,7 @@ def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
     th.join()
     for g in srv.poll():
         done[g["id"]] = (g, t_end)
+    sst = srv.stats()
     srv.close()
     lat = np.array([g["latency_ms"] for g, _ in done.values()])
     ok = 0
@@ -223,6 +232,9 @@ def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
             "throughput_fps": len(done) / (last - t0), "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "p999_ms": float(np.percentile(lat, 99.9)),
             "success_rate": ok / max(len(done), 1), "budget_bytes": budget,
+            "mean_resident": sst["resident_sum"] / max(sst["steps"], 1), "steps": sst["steps"],
+            "device_wait_ms": sst["device_wait_ms"], "host_ms": sst["host_stage_ms"] + sst["host_retire_ms"]
+            + sst["host_launch_ms"],
             "workload": "N log-uniform [300,50000], w U[0.05,0.70], sigma 1 px, Poisson arrivals"}, reqs
 
 

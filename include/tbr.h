@@ -249,9 +249,26 @@ typedef struct tbr_server_result {
     double submit_to_done_ms;         /* host wall clock from submit to completion */
 } tbr_server_result;
 
+/* Counters of the request loop since creation. The loop overlaps staging of
+ * new requests (host copies into pinned memory) with the step running on the
+ * device; device_wait_ms is the time it waited for steps to finish. */
+typedef struct tbr_server_stats {
+    int64_t submitted, admitted, completed;
+    int64_t steps;          /* engine steps launched */
+    int64_t resident_sum;   /* sum over steps of resident frames (mean = /steps) */
+    double host_stage_ms;   /* picking and copying admissions */
+    double device_wait_ms;  /* waiting for the step in flight */
+    double host_retire_ms;  /* downloading and publishing results */
+    double host_launch_ms;  /* uploads and step launches */
+} tbr_server_stats;
+
 tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr_server **out);
 /* Copies the frame's host arrays; returns immediately. */
 tbr_status tbr_server_submit(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id);
+/* Does not copy: the frame's arrays are read when the request is admitted, so
+ * they must stay valid and unchanged until its result has been polled. */
+tbr_status tbr_server_submit_nocopy(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id);
+tbr_status tbr_server_get_stats(tbr_server *s, tbr_server_stats *out);
 /* Moves up to max completed results into out; *n_out = number written. */
 tbr_status tbr_server_poll(tbr_server *s, tbr_server_result *out, int32_t max, int32_t *n_out);
 tbr_status tbr_server_cancel(tbr_server *s, uint64_t request_id);

@@ -85,6 +85,15 @@ class ServerResultC(C.Structure):
                 ("submit_to_done_ms", C.c_double)]
 
 
+class ServerStatsC(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("steps", C.c_int64), ("resident_sum", C.c_int64), ("host_stage_ms", C.c_double),
+                ("device_wait_ms", C.c_double), ("host_retire_ms", C.c_double), ("host_launch_ms", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _lib = None
 
 # Every entry point declared in include/tbr.h.
@@ -93,7 +102,7 @@ EXPORTS = [
     "tbr_context_create", "tbr_context_destroy", "tbr_estimate_absolute_pose", "tbr_get_inliers",
     "tbr_bundle_adjust", "tbr_estimate_batch", "tbr_batch_create", "tbr_batch_run", "tbr_batch_sync",
     "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
-    "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
+    "tbr_server_submit_nocopy", "tbr_server_get_stats", "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
     "tbr_debug_score_samples", "tbr_msac_score_noalloc",
 ]
 
@@ -132,6 +141,8 @@ def lib() -> C.CDLL:
     L.tbr_measure_fp32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.tbr_server_create.argtypes = [vp, C.POINTER(ServerConfigC), C.POINTER(vp)]
     L.tbr_server_submit.argtypes = [vp, C.POINTER(FrameDescC), C.POINTER(C.c_uint64)]
+    L.tbr_server_submit_nocopy.argtypes = [vp, C.POINTER(FrameDescC), C.POINTER(C.c_uint64)]
+    L.tbr_server_get_stats.argtypes = [vp, C.POINTER(ServerStatsC)]
     L.tbr_server_poll.argtypes = [vp, C.POINTER(ServerResultC), C.c_int32, C.POINTER(C.c_int32)]
     L.tbr_server_cancel.argtypes = [vp, C.c_uint64]
     L.tbr_server_drain.argtypes = [vp]

@@ -394,10 +394,15 @@ def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None =
 class Server:
     """Continuous-batching request loop (tbr_server_*): submit frames any time;
     a worker advances every resident frame one engine step at a time and admits
-    new requests into free slots within the workspace budget."""
+    new requests into free slots within the workspace budget.
+
+    With copy=False (default) a submitted frame's arrays are read when the
+    request is admitted (tbr_server_submit_nocopy): this object keeps them alive
+    until poll() returns the request, and they must not be modified meanwhile.
+    copy=True copies them at submit (tbr_server_submit)."""
 
     def __init__(self, ctx: Context, budget_bytes: int = 8 << 30, max_slots: int = 512, max_queue: int = 1 << 16,
-                 ransac_opt: RansacOptions_cuda | None = None):
+                 ransac_opt: RansacOptions_cuda | None = None, copy: bool = False):
         cfg = _lib.ServerConfigC()
         cfg.workspace_budget_bytes = budget_bytes
         cfg.max_slots = max_slots
@@ -407,12 +412,23 @@ class Server:
         check(_lib.lib().tbr_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self._h = h
         self._buf = (_lib.ServerResultC * 1024)()
+        self._copy = copy
+        self._keep = {}
 
     def submit(self, frame, seed: int | None = None, max_reproj_error: float = 0.0) -> int:
         arr, keep = _frame_descs([frame], None if seed is None else [seed], max_reproj_error)
         rid = C.c_uint64()
-        check(_lib.lib().tbr_server_submit(self._h, arr, C.byref(rid)))
+        if self._copy:
+            check(_lib.lib().tbr_server_submit(self._h, arr, C.byref(rid)))
+        else:
+            check(_lib.lib().tbr_server_submit_nocopy(self._h, arr, C.byref(rid)))
+            self._keep[rid.value] = keep
         return rid.value
+
+    def stats(self) -> dict:
+        st = _lib.ServerStatsC()
+        check(_lib.lib().tbr_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
 
     def poll(self, max_results: int = 1024):
         n = C.c_int32()
@@ -422,6 +438,7 @@ class Server:
         out = []
         for i in range(n.value):
             r = self._buf[i]
+            self._keep.pop(r.request_id, None)
             out.append({"id": r.request_id, "status": r.status, "q": np.array(r.q[:]), "t": np.array(r.t[:]),
                         "latency_ms": r.submit_to_done_ms, **r.stats.as_dict()})
         return out
@@ -436,6 +453,7 @@ class Server:
         if self._h:
             _lib.lib().tbr_server_destroy(self._h)
             self._h = None
+            self._keep.clear()
 
     def __del__(self):
         try:

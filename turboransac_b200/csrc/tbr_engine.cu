@@ -479,45 +479,62 @@ static void parallel_copy(const std::vector<CopyJob> &jobs) {
     for (auto &x : th) x.join();
 }
 
-// Uploads frames into slots (host -> device through pinned staging). Frames
-// whose point blocks are adjacent in the pool form one run; the staging area
-// mirrors the pool's layout inside a run, so a run costs one copy per array.
-// The frame records go up as one array and are scattered by one kernel; on
-// return d_active[0..n) holds the new slots.
-static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
-                               std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
-    if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
+// Admission in two halves. stage_frames (host only) takes slots and point
+// blocks and copies the frames into pinned staging; upload_staged enqueues the
+// device side. Frames whose point blocks are adjacent in the pool form one run;
+// the staging area mirrors the pool's layout inside a run, so a run costs one
+// copy per array. The frame records go up as one array and are scattered by
+// one kernel; after the upload d_active[0..n) holds the new slots.
+struct StagedAdmission {
+    struct Run {
+        int64_t b0, b1;  // block range in the pool
+        char *huv, *hxyz;
+    };
+    std::vector<int> slots;
+    std::vector<FrameDev> devs;
+    std::vector<Run> runs;
+    FrameDev *hd = nullptr;
+    int32_t *ha = nullptr;
+    int64_t max_n = 0;
+};
+
+static size_t stage_bytes(const std::vector<FrameHost> &fr) {
     auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     size_t stage = 0;
-    int64_t replay_total = 0;
     for (auto &f : fr) {
         const size_t pts = (size_t)((f.n + kSub - 1) / kSub) * kSub;
         stage += r256(16 * pts) + r256(24 * pts);
-        replay_total += f.replay ? f.replay_count : 0;
     }
-    stage += r256(sizeof(FrameDev) * fr.size()) + r256(4 * fr.size()) + 256;
-    tbr_status st = E.ensure_stage(stage);
-    if (st) return st;
+    return stage + r256(sizeof(FrameDev) * fr.size()) + r256(4 * fr.size()) + 256;
+}
+
+// `stage` holds at least stage_bytes(fr) bytes of pinned memory that no copy in
+// flight reads.
+static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o, char *stage,
+                               StagedAdmission &A) {
+    if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
+    auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+    int64_t replay_total = 0;
+    for (auto &f : fr) replay_total += f.replay ? f.replay_count : 0;
     if (replay_total) {
-        st = E.ensure_replay(replay_total);
+        tbr_status st = E.ensure_replay(replay_total);
         if (st) return st;
     }
-    std::vector<FrameDev> devs;
+    A = StagedAdmission();
     std::vector<int64_t> offs;
     int64_t rep_off = 0;
-    max_n = 0;
     for (auto &f : fr) {
         const int64_t nb = (f.n + kSub - 1) / kSub;
         const int64_t off = E.blocks.alloc(nb);
         if (off < 0) {
-            for (size_t i = 0; i < slots.size(); ++i) E.blocks.release(devs[i].blk_off, devs[i].n_blocks);
-            for (int s : slots) E.free_slots.push_back(s);
-            slots.clear();
+            for (size_t i = 0; i < A.slots.size(); ++i) E.blocks.release(A.devs[i].blk_off, A.devs[i].n_blocks);
+            for (int s : A.slots) E.free_slots.push_back(s);
+            A.slots.clear();
             return fail(TBR_ERR_OOM, "point workspace exhausted");
         }
         const int slot = E.free_slots.back();
         E.free_slots.pop_back();
-        slots.push_back(slot);
+        A.slots.push_back(slot);
         offs.push_back(off);
         const int32_t *d_rep = nullptr;
         if (f.replay) {
@@ -525,59 +542,77 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
             TBR_CUDA(cudaMemcpyAsync((void *)d_rep, f.replay, 12 * f.replay_count, cudaMemcpyHostToDevice, E.stream));
             rep_off += f.replay_count;
         }
-        devs.push_back(E.make_frame(f, off, o, d_rep));
-        max_n = std::max(max_n, f.n);
+        A.devs.push_back(E.make_frame(f, off, o, d_rep));
+        A.max_n = std::max(A.max_n, f.n);
     }
-    // Runs of adjacent frames: [first frame, last frame], block range [b0, b1).
-    struct Run {
-        size_t f0, f1;
-        int64_t b0, b1;
-        char *huv, *hxyz;
-    };
-    std::vector<Run> runs;
+    // Runs of adjacent frames.
+    std::vector<std::pair<size_t, size_t>> span;  // first, last frame of each run
     for (size_t i = 0; i < fr.size(); ++i) {
-        const int64_t nb = devs[i].n_blocks;
-        if (!runs.empty() && runs.back().b1 == offs[i]) {
-            runs.back().f1 = i;
-            runs.back().b1 += nb;
+        const int64_t nb = A.devs[i].n_blocks;
+        if (!A.runs.empty() && A.runs.back().b1 == offs[i]) {
+            A.runs.back().b1 += nb;
+            span.back().second = i;
         } else {
-            runs.push_back({i, i, offs[i], offs[i] + nb, nullptr, nullptr});
+            A.runs.push_back({offs[i], offs[i] + nb, nullptr, nullptr});
+            span.push_back({i, i});
         }
     }
-    char *h = (char *)E.h_stage;
+    char *h = stage;
     std::vector<CopyJob> jobs;
-    for (auto &r : runs) {
-        const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
-        r.huv = h;
+    for (size_t r = 0; r < A.runs.size(); ++r) {
+        auto &run = A.runs[r];
+        const size_t pts = (size_t)(run.b1 - run.b0) * kSub;
+        run.huv = h;
         h += r256(16 * pts);
-        r.hxyz = h;
+        run.hxyz = h;
         h += r256(24 * pts);
-        for (size_t i = r.f0; i <= r.f1; ++i) {
-            const size_t p = (size_t)(offs[i] - r.b0) * kSub;
-            jobs.push_back({r.huv + 16 * p, fr[i].uv, 16 * (size_t)fr[i].n});
-            jobs.push_back({r.hxyz + 24 * p, fr[i].xyz, 24 * (size_t)fr[i].n});
+        for (size_t i = span[r].first; i <= span[r].second; ++i) {
+            const size_t p = (size_t)(offs[i] - run.b0) * kSub;
+            jobs.push_back({run.huv + 16 * p, fr[i].uv, 16 * (size_t)fr[i].n});
+            jobs.push_back({run.hxyz + 24 * p, fr[i].xyz, 24 * (size_t)fr[i].n});
         }
     }
-    FrameDev *hd = (FrameDev *)h;
+    A.hd = (FrameDev *)h;
     h += r256(sizeof(FrameDev) * fr.size());
-    int32_t *ha = (int32_t *)h;
+    A.ha = (int32_t *)h;
     for (size_t i = 0; i < fr.size(); ++i) {
-        hd[i] = devs[i];
-        ha[i] = slots[i];
+        A.hd[i] = A.devs[i];
+        A.ha[i] = A.slots[i];
     }
     parallel_copy(jobs);
-    for (auto &r : runs) {
+    return TBR_OK;
+}
+
+static tbr_status upload_staged(Engine &E, const StagedAdmission &A) {
+    const size_t n = A.slots.size();
+    if (n == 0) return TBR_OK;
+    for (auto &r : A.runs) {
         const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
         const size_t p0 = (size_t)r.b0 * kSub;
         TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), r.huv, 16 * pts, cudaMemcpyHostToDevice, E.stream));
         TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), r.hxyz, 24 * pts, cudaMemcpyHostToDevice, E.stream));
     }
-    TBR_CUDA(cudaMemcpyAsync(E.d_admit, hd, sizeof(FrameDev) * fr.size(), cudaMemcpyHostToDevice, E.stream));
-    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * fr.size(), cudaMemcpyHostToDevice, E.stream));
-    k_admit_frames<<<(int)fr.size(), 128, 0, E.stream>>>(E.P.frames, E.d_admit, E.d_active, (int)fr.size());
+    TBR_CUDA(cudaMemcpyAsync(E.d_admit, A.hd, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.d_active, A.ha, 4 * n, cudaMemcpyHostToDevice, E.stream));
+    k_admit_frames<<<(int)n, 128, 0, E.stream>>>(E.P.frames, E.d_admit, E.d_active, (int)n);
     TBR_CUDA(cudaGetLastError());
-    E.P.n_active = (int32_t)slots.size();
-    if (host_devs) *host_devs = devs;
+    E.P.n_active = (int32_t)n;
+    return TBR_OK;
+}
+
+// Both halves through the context's own staging buffer.
+static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
+                               std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
+    tbr_status st = E.ensure_stage(stage_bytes(fr));
+    if (st) return st;
+    StagedAdmission A;
+    st = stage_frames(E, fr, o, (char *)E.h_stage, A);
+    if (st) return st;
+    st = upload_staged(E, A);
+    if (st) return st;
+    slots = A.slots;
+    max_n = A.max_n;
+    if (host_devs) *host_devs = A.devs;
     return TBR_OK;
 }
 
@@ -1180,18 +1215,42 @@ void tbr_batch_destroy(tbr_batch *b) {
 // its work overlaps theirs on the device.
 struct ServerRequest {
     uint64_t id;
-    std::vector<double> uv, xyz;
+    std::vector<double> uv, xyz;            // owned copies (tbr_server_submit)
+    const double *ext_uv = nullptr, *ext_xyz = nullptr;  // caller's arrays (tbr_server_submit_nocopy)
+    int64_t n = 0;
     double K[4];
     uint64_t seed;
     double thr;
     std::chrono::steady_clock::time_point t_submit;
     bool cancelled = false;
+    const double *U() const { return ext_uv ? ext_uv : uv.data(); }
+    const double *Xw() const { return ext_xyz ? ext_xyz : xyz.data(); }
 };
 
 struct Resident {
     std::unique_ptr<ServerRequest> req;
     int slot;
     int64_t blk_off, n_blocks;
+};
+
+struct PinnedBuffer {
+    void *p = nullptr;
+    size_t bytes = 0;
+    // Grows geometrically: pinning is slow and freeing pinned memory
+    // synchronizes the device.
+    tbr_status ensure(size_t b) {
+        if (b <= bytes) return TBR_OK;
+        const size_t nb = std::max(b, 2 * bytes);
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        TBR_CUDA(cudaMallocHost(&p, nb));
+        bytes = nb;
+        return TBR_OK;
+    }
+    ~PinnedBuffer() {
+        if (p) cudaFreeHost(p);
+    }
 };
 
 struct tbr_server {
@@ -1211,9 +1270,18 @@ struct tbr_server {
     std::thread worker;
     int32_t *d_status = nullptr, *h_status = nullptr;
     int32_t *d_prep = nullptr;
+    PinnedBuffer stage[2];   // admission staging, alternating between steps
+    int cur = 0;
+    bool step_in_flight = false;
+    tbr_server_stats stats{};  // guarded by mu
+    tbr_server_stats ws{};     // the worker's own counters, published into stats after each step
     tbr_status error = TBR_OK;
     std::string error_msg;
 };
+
+static double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
 
 static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, tbr_status st) {
     tbr_server_result out;
@@ -1223,70 +1291,110 @@ static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, 
     if (res) {
         for (int k = 0; k < 4; ++k) out.q[k] = res->q[k];
         for (int k = 0; k < 3; ++k) out.t[k] = res->t[k];
-        fill_stats(*res, (int64_t)(r.req->uv.size() / 2), &out.stats, 0.f);
+        fill_stats(*res, r.req->n, &out.stats, 0.f);
     }
-    out.submit_to_done_ms =
-        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r.req->t_submit).count();
+    out.submit_to_done_ms = ms_since(r.req->t_submit);
     std::lock_guard<std::mutex> lk(s->mu);
     s->done.push_back(out);
     s->in_flight--;
+    s->stats.completed++;
     s->cv_done.notify_all();
 }
 
+// One iteration of the request loop, pipelined with the device:
+//   A. while the previous step runs, take queued requests that fit the free
+//      slots and point blocks and copy them into pinned staging;
+//   B. wait for that step, retire the frames it finished;
+//   C. upload the staged frames, prepare them, and launch the next step over
+//      every resident frame without waiting for it.
 static tbr_status server_step(tbr_server *s) {
     Engine &E = s->E;
-    // ---- admit ----
+    // ---- A: stage admissions ----
+    auto t0 = std::chrono::steady_clock::now();
     std::vector<std::unique_ptr<ServerRequest>> newreq;
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        int64_t free_blocks = E.blocks.capacity() - E.blocks.used();
+        // One step admits at most a staging buffer's worth (always at least one
+        // request), so that staging keeps overlapping the device's steps.
+        size_t staged = 0;
+        const size_t stage_cap = s->stage[s->cur].bytes;
         while (!s->queue.empty() && (int)newreq.size() < (int)E.free_slots.size()) {
             auto &q = s->queue.front();
             if (q->cancelled) {
-                Resident tmp{std::move(q), -1, 0, 0};
-                s->queue.pop_front();
-                s->done.push_back({});
-                auto &o = s->done.back();
+                tbr_server_result o;
                 std::memset(&o, 0, sizeof(o));
-                o.request_id = tmp.req->id;
+                o.request_id = q->id;
                 o.status = TBR_ERR_CANCELLED;
+                s->done.push_back(o);
+                s->queue.pop_front();
                 s->in_flight--;
                 s->cv_done.notify_all();
                 continue;
             }
-            const int64_t need = (int64_t)(q->uv.size() / 2 + kSub - 1) / kSub;
-            if (E.blocks.capacity() - E.blocks.used() < need) break;  // budget: wait for frames to retire
+            const int64_t need = (q->n + kSub - 1) / kSub;
+            if (free_blocks < need) break;  // budget: wait for frames to retire
+            const size_t bytes = (size_t)need * kSub * 40 + 2 * sizeof(FrameDev) + 1024;
+            if (!newreq.empty() && staged + bytes > stage_cap) break;
+            staged += bytes;
+            free_blocks -= need;
             newreq.push_back(std::move(q));
             s->queue.pop_front();
         }
     }
+    StagedAdmission A;
     if (!newreq.empty()) {
         std::vector<FrameHost> fh;
         for (auto &r : newreq)
-            fh.push_back({r->uv.data(), r->xyz.data(), (int64_t)(r->uv.size() / 2), {r->K[0], r->K[1], r->K[2], r->K[3]},
-                          r->seed, r->thr, nullptr, 0});
-        std::vector<int> slots;
-        std::vector<FrameDev> devs;
-        int64_t max_n = 0;
-        tbr_status st = admit_frames(E, fh, s->o, slots, max_n, &devs);
+            fh.push_back({r->U(), r->Xw(), r->n, {r->K[0], r->K[1], r->K[2], r->K[3]}, r->seed, r->thr, nullptr, 0});
+        PinnedBuffer &buf = s->stage[s->cur];
+        tbr_status st = buf.ensure(stage_bytes(fh));
+        if (st) return st;
+        st = stage_frames(E, fh, s->o, (char *)buf.p, A);
         if (st == TBR_ERR_OOM) {  // fragmentation: requeue at the front and retry after retirements
             std::lock_guard<std::mutex> lk(s->mu);
             for (auto it = newreq.rbegin(); it != newreq.rend(); ++it) s->queue.push_front(std::move(*it));
             newreq.clear();
         } else if (st) {
             return st;
-        } else {
-            // admit_frames wrote the new slots to d_active; prepare them (AABB, packing).
-            cudaMemcpyAsync(s->d_prep, E.d_active, 4 * slots.size(), cudaMemcpyDeviceToDevice, E.stream);
-            Pools Q = E.P;
-            Q.active = s->d_prep;
-            Q.n_active = (int32_t)slots.size();
-            E.launch_prep(Q, (int)slots.size(), max_n);
-            for (size_t i = 0; i < slots.size(); ++i)
-                s->resident.push_back({std::move(newreq[i]), slots[i], devs[i].blk_off, devs[i].n_blocks});
         }
     }
-    if (s->resident.empty()) return TBR_OK;
-    // ---- cancels of resident frames: retire them now ----
+    s->ws.host_stage_ms += ms_since(t0);
+    // ---- B: finish the step in flight ----
+    if (s->step_in_flight) {
+        t0 = std::chrono::steady_clock::now();
+        TBR_CUDA(cudaStreamSynchronize(E.stream));
+        s->step_in_flight = false;
+        s->ws.device_wait_ms += ms_since(t0);
+        if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+        t0 = std::chrono::steady_clock::now();
+        const int na = (int)s->resident.size();
+        std::vector<int> fin;
+        for (int i = 0; i < na; ++i)
+            if (s->h_status[i] == kDone) fin.push_back(i);
+        if (!fin.empty()) {
+            std::vector<FrameResult> res(fin.size());
+            std::vector<int> fslots(fin.size());
+            for (size_t k = 0; k < fin.size(); ++k) fslots[k] = s->resident[fin[k]].slot;
+            tbr_status fst = fetch_results(E, fslots, res.data());
+            if (fst) return fst;
+            for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &res[k], TBR_OK);
+            std::vector<Resident> keep;
+            std::vector<bool> gone(na, false);
+            for (int i : fin) gone[i] = true;
+            for (int i = 0; i < na; ++i) {
+                if (gone[i]) {
+                    E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
+                    E.free_slots.push_back(s->resident[i].slot);
+                } else {
+                    keep.push_back(std::move(s->resident[i]));
+                }
+            }
+            s->resident.swap(keep);
+        }
+        s->ws.host_retire_ms += ms_since(t0);
+    }
+    // ---- cancels of resident frames (no step in flight here) ----
     {
         std::vector<uint64_t> ids;
         {
@@ -1296,56 +1404,55 @@ static tbr_status server_step(tbr_server *s) {
         for (uint64_t id : ids)
             for (size_t i = 0; i < s->resident.size(); ++i)
                 if (s->resident[i].req->id == id) {
-                    TBR_CUDA(cudaStreamSynchronize(E.stream));
                     server_complete(s, s->resident[i], nullptr, TBR_ERR_CANCELLED);
                     E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
                     E.free_slots.push_back(s->resident[i].slot);
                     s->resident.erase(s->resident.begin() + i);
                     break;
                 }
-        if (s->resident.empty()) return TBR_OK;
     }
-    // ---- one step over all resident frames ----
-    const int na = (int)s->resident.size();
-    int32_t *ha = (int32_t *)E.h_stage;
-    TBR_CUDA(cudaStreamSynchronize(E.stream));
-    tbr_status st = E.ensure_stage(8 * na + 4096);
-    if (st) return st;
-    ha = (int32_t *)E.h_stage;
-    for (int i = 0; i < na; ++i) ha[i] = s->resident[i].slot;
-    TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * na, cudaMemcpyHostToDevice, E.stream));
-    E.P.n_active = na;
-    E.launch_step(E.P, na, s->o.hr);
-    k_gather_status<<<(na + 255) / 256, 256, 0, E.stream>>>(E.P, s->d_status);
-    TBR_CUDA(cudaGetLastError());
-    TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
-    TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
-    TBR_CUDA(cudaStreamSynchronize(E.stream));
-    if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
-    // ---- retire ----
-    std::vector<int> fin;
-    for (int i = 0; i < na; ++i)
-        if (s->h_status[i] == kDone) fin.push_back(i);
-    if (!fin.empty()) {
-        std::vector<FrameResult> res(fin.size());
-        std::vector<int> fslots(fin.size());
-        for (size_t k = 0; k < fin.size(); ++k) fslots[k] = s->resident[fin[k]].slot;
-        tbr_status fst = fetch_results(E, fslots, res.data());
-        if (fst) return fst;
-        for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &res[k], TBR_OK);
-        std::vector<Resident> keep;
-        std::vector<bool> gone(na, false);
-        for (int i : fin) gone[i] = true;
-        for (int i = 0; i < na; ++i) {
-            if (gone[i]) {
-                E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
-                E.free_slots.push_back(s->resident[i].slot);
-            } else {
-                keep.push_back(std::move(s->resident[i]));
-            }
-        }
-        s->resident.swap(keep);
+    // ---- C: upload admissions, launch the next step ----
+    t0 = std::chrono::steady_clock::now();
+    if (!A.slots.empty()) {
+        tbr_status st = upload_staged(E, A);
+        if (st) return st;
+        // upload_staged wrote the new slots to d_active; prepare them (AABB, packing).
+        TBR_CUDA(cudaMemcpyAsync(s->d_prep, E.d_active, 4 * A.slots.size(), cudaMemcpyDeviceToDevice, E.stream));
+        Pools Q = E.P;
+        Q.active = s->d_prep;
+        Q.n_active = (int32_t)A.slots.size();
+        E.launch_prep(Q, (int)A.slots.size(), A.max_n);
+        for (size_t i = 0; i < A.slots.size(); ++i)
+            s->resident.push_back({std::move(newreq[i]), A.slots[i], A.devs[i].blk_off, A.devs[i].n_blocks});
+        s->ws.admitted += (int64_t)A.slots.size();
+        s->cur ^= 1;
     }
+    if (!s->resident.empty()) {
+        const int na = (int)s->resident.size();
+        tbr_status st = E.ensure_stage(8 * na + 4096);
+        if (st) return st;
+        int32_t *ha = (int32_t *)E.h_stage;
+        for (int i = 0; i < na; ++i) ha[i] = s->resident[i].slot;
+        TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * na, cudaMemcpyHostToDevice, E.stream));
+        E.P.n_active = na;
+        E.launch_step(E.P, na, s->o.hr);
+        k_gather_status<<<(na + 255) / 256, 256, 0, E.stream>>>(E.P, s->d_status);
+        TBR_CUDA(cudaGetLastError());
+        TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+        s->step_in_flight = true;
+        s->ws.steps++;
+        s->ws.resident_sum += na;
+    }
+    s->ws.host_launch_ms += ms_since(t0);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.steps = s->ws.steps;
+    s->stats.admitted = s->ws.admitted;
+    s->stats.resident_sum = s->ws.resident_sum;
+    s->stats.host_stage_ms = s->ws.host_stage_ms;
+    s->stats.device_wait_ms = s->ws.device_wait_ms;
+    s->stats.host_retire_ms = s->ws.host_retire_ms;
+    s->stats.host_launch_ms = s->ws.host_launch_ms;
     return TBR_OK;
 }
 
@@ -1354,14 +1461,19 @@ static void server_loop(tbr_server *s) {
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            s->cv.wait_for(lk, std::chrono::milliseconds(50),
-                           [&] { return s->stop || !s->queue.empty() || !s->resident.empty(); });
+            s->cv.wait_for(lk, std::chrono::milliseconds(50), [&] {
+                return s->stop || !s->queue.empty() || !s->resident.empty() || !s->cancel_ids.empty();
+            });
             if (s->stop) break;
-            if (s->queue.empty() && s->resident.empty()) continue;
+            if (s->queue.empty() && s->resident.empty() && !s->step_in_flight) {
+                s->cancel_ids.clear();  // nothing resident to cancel
+                continue;
+            }
         }
-        // the counters are per step; the step stamp is reset only when idle
         tbr_status st = server_step(s);
         if (st) {
+            cudaStreamSynchronize(s->E.stream);
+            s->step_in_flight = false;
             std::lock_guard<std::mutex> lk(s->mu);
             s->error = st;
             s->error_msg = g_last_error;
@@ -1387,6 +1499,7 @@ static void server_loop(tbr_server *s) {
             break;
         }
     }
+    cudaStreamSynchronize(s->E.stream);
 }
 
 extern "C" {
@@ -1418,6 +1531,16 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
         delete s;
         return fail(TBR_ERR_OOM, "server allocation failed");
     }
+    // Staging for one step's admissions, sized up front (64 MiB each).
+    for (auto &b : s->stage)
+        if (b.ensure(64ull << 20) != TBR_OK) {
+            delete s;
+            return fail(TBR_ERR_OOM, "server staging allocation failed");
+        }
+    if (s->E.ensure_stage(1 << 20) != TBR_OK) {
+        delete s;
+        return fail(TBR_ERR_OOM, "server staging allocation failed");
+    }
     cudaMemsetAsync(s->E.P.counters, 0, 8 * kCNum, s->E.stream);
     cudaStreamSynchronize(s->E.stream);
     s->worker = std::thread(server_loop, s);
@@ -1425,13 +1548,9 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
     return TBR_OK;
 }
 
-tbr_status tbr_server_submit(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id) {
-    if (!s || !frame || !frame->points2D || !frame->points3D || frame->n < 3)
-        return fail(TBR_ERR_INVALID_ARG, "bad frame");
-    if (!(frame->K[0] > 0) || !(frame->K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "bad camera");
-    auto r = std::make_unique<ServerRequest>();
-    r->uv.assign(frame->points2D, frame->points2D + 2 * frame->n);
-    r->xyz.assign(frame->points3D, frame->points3D + 3 * frame->n);
+static tbr_status server_enqueue(tbr_server *s, std::unique_ptr<ServerRequest> r, const tbr_frame_desc *frame,
+                                 uint64_t *request_id) {
+    r->n = frame->n;
     for (int k = 0; k < 4; ++k) r->K[k] = frame->K[k];
     r->seed = frame->seed;
     r->thr = frame->max_reproj_error > 0 ? frame->max_reproj_error : s->ro.max_reproj_error;
@@ -1445,7 +1564,37 @@ tbr_status tbr_server_submit(tbr_server *s, const tbr_frame_desc *frame, uint64_
     if (request_id) *request_id = r->id;
     s->queue.push_back(std::move(r));
     s->in_flight++;
+    s->stats.submitted++;
     s->cv.notify_one();
+    return TBR_OK;
+}
+
+static bool bad_request(const tbr_server *s, const tbr_frame_desc *frame) {
+    return !s || !frame || !frame->points2D || !frame->points3D || frame->n < 3;
+}
+
+tbr_status tbr_server_submit(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id) {
+    if (bad_request(s, frame)) return fail(TBR_ERR_INVALID_ARG, "bad frame");
+    if (!(frame->K[0] > 0) || !(frame->K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "bad camera");
+    auto r = std::make_unique<ServerRequest>();
+    r->uv.assign(frame->points2D, frame->points2D + 2 * frame->n);
+    r->xyz.assign(frame->points3D, frame->points3D + 3 * frame->n);
+    return server_enqueue(s, std::move(r), frame, request_id);
+}
+
+tbr_status tbr_server_submit_nocopy(tbr_server *s, const tbr_frame_desc *frame, uint64_t *request_id) {
+    if (bad_request(s, frame)) return fail(TBR_ERR_INVALID_ARG, "bad frame");
+    if (!(frame->K[0] > 0) || !(frame->K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "bad camera");
+    auto r = std::make_unique<ServerRequest>();
+    r->ext_uv = frame->points2D;
+    r->ext_xyz = frame->points3D;
+    return server_enqueue(s, std::move(r), frame, request_id);
+}
+
+tbr_status tbr_server_get_stats(tbr_server *s, tbr_server_stats *out) {
+    if (!s || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
     return TBR_OK;
 }
 

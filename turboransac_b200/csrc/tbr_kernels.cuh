@@ -1392,14 +1392,14 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
 // a cluster of kLMCluster CTAs (a single SM would serialise them).
 constexpr int64_t kLMClusterMin = 3000;
 
-__global__ void __launch_bounds__(kLMThreads) k_lm_small(Pools P) {
+__global__ void __launch_bounds__(kLMThreads, 2) k_lm_small(Pools P) {
     const int slot = P.active[blockIdx.x];
     const FrameDev &f = P.frames[slot];
     if (f.status != kLMPending || f.num_inliers >= kLMClusterMin || f.lm_force_cluster) return;
     lm_frame<1>(P, slot);
 }
 
-__global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads) k_lm(Pools P) {
+__global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads, 2) k_lm(Pools P) {
     const int slot = P.active[blockIdx.x / kLMCluster];
     const FrameDev &f = P.frames[slot];
     // uniform across the cluster
