@@ -169,3 +169,27 @@ def test_stop_rule_overflow_modes(ctx, oracle, quirk):
     assert st.details["best_sample"] == o["info"].ransac.best_sample
     assert (o["info"].ransac.samples == 1000) == quirk
     assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_nonfinite_points_are_outliers(ctx, oracle):
+    """NaN / inf correspondences are never inliers (comparisons with NaN fail in
+    msac.cuh:46 and entry.cu:22); the FP32 filter stages them as outliers, and
+    samples that contain them give non-finite P3P poses that score n * tau^2."""
+    f = scenes.plain_frame(3)
+    uv, xyz = f.uv.copy(), f.xyz.copy()
+    rng = np.random.default_rng(5)
+    bad = rng.choice(f.n, 120, replace=False)
+    xyz[bad[:40], 0] = np.nan
+    xyz[bad[40:60], 2] = np.inf
+    uv[bad[60:100], 1] = np.nan
+    uv[bad[100:], 0] = -np.inf
+    ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(uv, xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed)
+    o = oracle.estimate(uv, xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000)
+    d, info = st.details, o["info"]
+    assert d["samples"] == info.ransac.samples
+    assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+    assert abs(d["model_score"] - info.ransac.score) <= 1e-12 * info.ransac.score
+    np.testing.assert_array_equal(inl, o["inliers"])
+    assert not inl[bad].any()
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6

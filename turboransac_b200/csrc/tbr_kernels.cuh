@@ -24,6 +24,8 @@
 namespace tbr {
 
 constexpr int kSub = 64;                          // points per FP32 staging block
+// Depth floor of the FP32 filter: the reciprocal of any smaller depth is 2^100.
+constexpr float kDepthFloor = 0x1p-100f;
 constexpr int kBlockFloat2 = kSub * 5;            // float2 entries per block
 constexpr uint32_t kBlockBytes = kBlockFloat2 * 8;  // 2560 B per block
 constexpr int kMaxRoundsPerStep = 128;
@@ -239,11 +241,13 @@ __global__ void k_prep_bounds(Pools P) {
     double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < f.n;
          i += (int64_t)gridDim.x * blockDim.x) {
+        const double v0 = P.X64[3 * (base + i)], v1 = P.X64[3 * (base + i) + 1], v2 = P.X64[3 * (base + i) + 2];
+        if (!(isfinite(v0) && isfinite(v1) && isfinite(v2))) continue;  // staged as an outlier
+        const double v[3] = {v0, v1, v2};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const double v = P.X64[3 * (base + i) + k];
-            lo[k] = fmin(lo[k], v);
-            hi[k] = fmax(hi[k], v);
+            lo[k] = fmin(lo[k], v[k]);
+            hi[k] = fmax(hi[k], v[k]);
         }
     }
 #pragma unroll
@@ -268,9 +272,12 @@ __global__ void k_prep_pack(Pools P) {
     if (a >= P.n_active) return;
     FrameDev &f = P.frames[P.active[a]];
     const int64_t base = f.blk_off * kSub;
-    const double c0 = 0.5 * (ordered_to_dbl(f.bmin[0]) + ordered_to_dbl(f.bmax[0]));
-    const double c1 = 0.5 * (ordered_to_dbl(f.bmin[1]) + ordered_to_dbl(f.bmax[1]));
-    const double c2 = 0.5 * (ordered_to_dbl(f.bmin[2]) + ordered_to_dbl(f.bmax[2]));
+    double cc[3];
+    for (int k = 0; k < 3; ++k) {  // no finite point: centre 0
+        cc[k] = 0.5 * (ordered_to_dbl(f.bmin[k]) + ordered_to_dbl(f.bmax[k]));
+        if (!isfinite(cc[k])) cc[k] = 0.0;
+    }
+    const double c0 = cc[0], c1 = cc[1], c2 = cc[2];
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         f.centre[0] = c0;
         f.centre[1] = c1;
@@ -292,6 +299,13 @@ __global__ void k_prep_pack(Pools P) {
             v[2] = (float)(P.X64[3 * (base + i) + 2] - c2);
             v[3] = (float)(-xn * itau);
             v[4] = (float)(-yn * itau);
+            bool finite = true;
+#pragma unroll
+            for (int k = 0; k < 5; ++k) finite = finite && fabsf(v[k]) <= 0x1p80f;
+            if (!finite) {  // non-finite (never an FP64 inlier) or beyond 2^80: outlier for every pose
+                v[0] = v[1] = v[2] = 0.0f;
+                v[3] = v[4] = 0x1p100f;
+            }
         } else {
             v[0] = v[1] = v[2] = v[3] = v[4] = 0.0f;
         }
@@ -450,16 +464,29 @@ __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
                 // Scoring form: rows 0, 1 scaled by 1/tau, translation moved to the
                 // centred frame (t + R c), all in FP64 before the FP32 rounding.
                 float *Q = P.hP32 + 12 * h;
+                float q32[12];
+                bool finite = true;
 #pragma unroll
                 for (int r = 0; r < 3; ++r) {
                     const double tc = S[4 * r + 3] + S[4 * r] * f.centre[0] + S[4 * r + 1] * f.centre[1] +
                                       S[4 * r + 2] * f.centre[2];
                     const double sc = r < 2 ? itau : 1.0;
-                    Q[4 * r] = (float)(S[4 * r] * sc);
-                    Q[4 * r + 1] = (float)(S[4 * r + 1] * sc);
-                    Q[4 * r + 2] = (float)(S[4 * r + 2] * sc);
-                    Q[4 * r + 3] = (float)(tc * sc);
+                    q32[4 * r] = (float)(S[4 * r] * sc);
+                    q32[4 * r + 1] = (float)(S[4 * r + 1] * sc);
+                    q32[4 * r + 2] = (float)(S[4 * r + 2] * sc);
+                    q32[4 * r + 3] = (float)(tc * sc);
                 }
+                // Rotation rows (scaled by 1/tau) within 2^40 and translations within
+                // 2^80 keep every depth of a staged point (within 2^80) below 2^123:
+                // no overflow, so no inf - inf and no NaN in the filter.
+#pragma unroll
+                for (int e = 0; e < 12; ++e)
+                    finite = finite && fabsf(q32[e]) <= ((e & 3) == 3 ? 0x1p80f : 0x1p40f);
+                // A pose outside that range scores every point as an outlier
+                // (depth -1, lateral offset 1).
+#pragma unroll
+                for (int e = 0; e < 12; ++e)
+                    Q[e] = finite ? q32[e] : (e == 3 || e == 7 ? 1.0f : (e == 11 ? -1.0f : 0.0f));
             }
         }
     }
@@ -534,12 +561,15 @@ __global__ void k_score_plan(Pools P) {
 
 // Per (hypothesis, point) the FP32 filter accumulates min(r^2 / tau^2, 1),
 // counting a point with non-positive depth as an outlier (msac.cuh:46
-// semantics) without a division or a branch: the reciprocal of the depth
-// carries its sign into the squared residual's sign bit, and an unsigned min
-// against the bits of 1.0f clamps NaN, +inf and any negative-signed value to 1.
-// HP hypothesis pairs x PP points as independent packed-FP32 chains, staged so
-// that every depth and its reciprocal issue first and the MUFU latency is
-// covered by the other two rows: z2 -> rcp, then z0, z1, residuals, clamp, sum.
+// semantics) without a division or a branch: a depth below 2^-100 is raised
+// to 2^-100 before the reciprocal, so the residual of a point behind the
+// camera is ~2^100 x its lateral offset and saturates; the last FMA of r^2
+// saturates to [0, 1] itself. Inputs are finite by construction (non-finite
+// points and hypotheses are replaced when staged), so the saturating FMA never
+// sees NaN. HP hypothesis pairs x PP points as independent packed-FP32 chains,
+// staged so that every depth and its reciprocal issue first and the MUFU
+// latency is covered by the other two rows: z2 -> rcp, then z0, z1, residuals,
+// saturating r^2, sum.
 template <int HP, int PP>
 __device__ __forceinline__ void msac_chains(const uint64_t (&c)[HP][12], const uint64_t (&X)[PP],
                                             const uint64_t (&Y)[PP], const uint64_t (&Z)[PP],
@@ -552,8 +582,8 @@ __device__ __forceinline__ void msac_chains(const uint64_t (&c)[HP][12], const u
             const uint64_t z2 = f2fma(c[h][8], X[p], f2fma(c[h][9], Y[p], f2fma(c[h][10], Z[p], c[h][11])));
             float za, zb;
             f2unpack(z2, za, zb);
-            ia[h][p] = rcp_approx(za);
-            ib[h][p] = rcp_approx(zb);
+            ia[h][p] = rcp_approx(fmaxf(za, kDepthFloor));
+            ib[h][p] = rcp_approx(fmaxf(zb, kDepthFloor));
         }
 #pragma unroll
     for (int h = 0; h < HP; ++h)
@@ -564,12 +594,11 @@ __device__ __forceinline__ void msac_chains(const uint64_t (&c)[HP][12], const u
             const uint64_t inv = f2pack(ia[h][p], ib[h][p]);
             const uint64_t r0 = f2fma(z0, inv, NX[p]);
             const uint64_t r1 = f2fma(z1, inv, NY[p]);
-            const uint64_t q = f2fma(r0, r0, f2mul(r1, r1));
-            float qa, qb;
-            f2unpack(q, qa, qb);
-            const uint32_t ca = min(__float_as_uint(qa) | (__float_as_uint(ia[h][p]) & 0x80000000u), 0x3f800000u);
-            const uint32_t cb = min(__float_as_uint(qb) | (__float_as_uint(ib[h][p]) & 0x80000000u), 0x3f800000u);
-            acc[h] = f2add(acc[h], f2pack(__uint_as_float(ca), __uint_as_float(cb)));
+            const uint64_t r1s = f2mul(r1, r1);
+            float r0a, r0b, sa, sb;
+            f2unpack(r0, r0a, r0b);
+            f2unpack(r1s, sa, sb);
+            acc[h] = f2add(acc[h], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
         }
 }
 
