@@ -16,10 +16,25 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 BIN = os.path.join(HERE, "_ref", "tbr_refcuda")
+CURAND_LIB = os.path.join(HERE, "_ref", "libtbr_refcurand.so")
 
 
 def available() -> bool:
-    return os.access(BIN, os.X_OK)
+    return os.access(BIN, os.X_OK) and os.path.exists(CURAND_LIB)
+
+
+def curand_triples(n: int, samples_per_round: int, rounds: int) -> np.ndarray:
+    """The reference's minimal samples (cuRAND XORWOW, its seeds and redraw rule)
+    for `rounds` rounds of `samples_per_round`, in sample order: (rounds*B, 3) int32."""
+    import ctypes as C
+    lib = C.CDLL(CURAND_LIB)
+    lib.ref_curand_triples.argtypes = [C.c_int64, C.c_int64, C.c_int32, C.c_void_p]
+    lib.ref_curand_triples.restype = C.c_int
+    out = np.zeros((rounds * samples_per_round, 3), np.int32)
+    rc = lib.ref_curand_triples(n, samples_per_round, rounds, out.ctypes.data)
+    if rc:
+        raise RuntimeError(f"ref_curand_triples failed ({rc})")
+    return out
 
 
 def _write_frames(path: str, frames) -> None:

@@ -181,6 +181,7 @@ class Engine {
 
     ~Engine() {
         if (stream) cudaStreamSynchronize(stream);
+        for (auto &g : graph_cache) cudaGraphExecDestroy(g.exec);
         if (d_base) cudaFree(d_base);
         if (h_stage) cudaFreeHost(h_stage);
         if (h_counters) cudaFreeHost(h_counters);
@@ -414,6 +415,114 @@ class Engine {
         k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
     }
     void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n); }
+
+    // The step loop as one graph: [reset ->] while (any frame in RANSAC)
+    // { RANSAC step || inliers + LM of the frames that finished in the previous
+    // step (disjoint frames) ; loop test } -> inliers + LM of the last step's.
+    // With d_init, a reset node first restores the frames from d_init.
+    bool build_loop_graph(const Pools &Q, int n, int hr, const FrameDev *d_init, cudaGraph_t *graph_out,
+                          cudaGraphExec_t *exec_out) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphConditionalHandle h;
+        bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                  cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        cudaGraphNode_t reset_node = nullptr, loop_node = nullptr;
+        Pools Qc = Q;
+        const FrameDev *init = d_init;
+        if (ok && d_init) {
+            cudaKernelNodeParams kp = {};
+            void *args[2] = {(void *)&Qc, (void *)&init};
+            kp.func = (void *)k_reset_frames;
+            kp.gridDim = dim3(n);
+            kp.blockDim = dim3(128);
+            kp.kernelParams = args;
+            ok = cudaGraphAddKernelNode(&reset_node, graph, nullptr, 0, &kp) == cudaSuccess;
+        }
+        cudaGraph_t body = nullptr;
+        if (ok) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&loop_node, graph, reset_node ? &reset_node : nullptr, reset_node ? 1 : 0, &cp) ==
+                 cudaSuccess;
+            body = cp.conditional.phGraph_out[0];
+        }
+        if (ok) {
+            ok = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+                 cudaSuccess;
+            if (ok) {
+                cudaEventRecord(ev_fork, stream);
+                cudaStreamWaitEvent(stream2, ev_fork, 0);
+                launch_refine(Q, n, stream2);
+                launch_ransac(Q, n, hr, stream);
+                cudaEventRecord(ev_join, stream2);
+                cudaStreamWaitEvent(stream, ev_join, 0);
+                k_loop_ctl<<<1, 1, 0, stream>>>(Q, h, 100000ull);
+                ok = cudaStreamEndCapture(stream, &body) == cudaSuccess;
+            }
+        }
+        if (ok) {
+            cudaGraph_t tail = nullptr;
+            ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            if (ok) {
+                launch_refine(Q, n, stream);
+                ok = cudaStreamEndCapture(stream, &tail) == cudaSuccess;
+            }
+            cudaGraphNode_t tail_node;
+            if (ok) ok = cudaGraphAddChildGraphNode(&tail_node, graph, &loop_node, 1, tail) == cudaSuccess;
+            if (tail) cudaGraphDestroy(tail);
+        }
+        cudaGraphExec_t exec = nullptr;
+        if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (!ok) {
+            cudaGetLastError();
+            if (graph) cudaGraphDestroy(graph);
+            return false;
+        }
+        *exec_out = exec;
+        if (graph_out) *graph_out = graph;
+        else cudaGraphDestroy(graph);
+        return true;
+    }
+
+    // Instantiated loop graphs of recent (frame count, scoring variant) shapes,
+    // least recently used first.
+    struct CachedGraph {
+        int n, hr, pp;
+        cudaGraphExec_t exec;
+    };
+    std::vector<CachedGraph> graph_cache;
+    static constexpr size_t kGraphCacheSize = 8;
+
+    // Runs the active frames of P (admitted and prepared) to completion as one
+    // graph launch; the counters must be zero.
+    tbr_status run_graph(int na, int hr, int *steps_out) {
+        cudaGraphExec_t exec = nullptr;
+        for (size_t i = 0; i < graph_cache.size(); ++i)
+            if (graph_cache[i].n == na && graph_cache[i].hr == hr && graph_cache[i].pp == pp) {
+                CachedGraph g = graph_cache[i];
+                graph_cache.erase(graph_cache.begin() + i);
+                graph_cache.push_back(g);
+                exec = g.exec;
+                break;
+            }
+        if (!exec) {
+            if (!build_loop_graph(P, na, hr, nullptr, nullptr, &exec)) return fail(TBR_ERR_CUDA, "graph capture failed");
+            if (graph_cache.size() >= kGraphCacheSize) {
+                cudaGraphExecDestroy(graph_cache.front().exec);
+                graph_cache.erase(graph_cache.begin());
+            }
+            graph_cache.push_back({na, hr, pp, exec});
+        }
+        TBR_CUDA(cudaGraphLaunch(exec, stream));
+        TBR_CUDA(cudaMemcpyAsync(h_counters, P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, stream));
+        TBR_CUDA(cudaStreamSynchronize(stream));
+        if (h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+        if (steps_out) *steps_out = (int)h_counters[kCSteps];
+        return TBR_OK;
+    }
 
     // Runs the active frames of `Q` to completion with one host check per step.
     tbr_status run(const Pools &Q, int na, int hr, int max_steps, int *steps_out, Profile *prof = nullptr) {
@@ -729,7 +838,7 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
     TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
     E.launch_prep((int)slots.size(), max_n);
     E.pp = o.pp;
-    st = E.run(slots, o.hr, 100000, steps_out);
+    st = E.run_graph((int)slots.size(), o.hr, steps_out);
     TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
     if (st == TBR_OK) {
         res.resize(fr.size());
@@ -1046,60 +1155,8 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
         b->blk_off.push_back(hf[i].blk_off);
         b->n_blocks.push_back(hf[i].n_blocks);
     }
-    // Graph: reset -> while (any frame in RANSAC) { step; inliers + LM of finished frames }.
-    cudaGraphConditionalHandle h;
-    bool ok = cudaGraphCreate(&b->graph, 0) == cudaSuccess &&
-              cudaGraphConditionalHandleCreate(&h, b->graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
-    cudaGraphNode_t reset_node = nullptr, loop_node = nullptr;
-    if (ok) {
-        cudaKernelNodeParams kp = {};
-        void *args[2] = {(void *)&b->Q, (void *)&b->d_init};
-        kp.func = (void *)k_reset_frames;
-        kp.gridDim = dim3(n_frames);
-        kp.blockDim = dim3(128);
-        kp.kernelParams = args;
-        ok = cudaGraphAddKernelNode(&reset_node, b->graph, nullptr, 0, &kp) == cudaSuccess;
-    }
-    cudaGraph_t body = nullptr;
-    if (ok) {
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        ok = cudaGraphAddNode(&loop_node, b->graph, &reset_node, 1, &cp) == cudaSuccess;
-        body = cp.conditional.phGraph_out[0];
-    }
-    if (ok) {
-        // Body: RANSAC of this step beside the refinement of frames that
-        // finished in the previous step (disjoint frames), then the loop test.
-        ok = cudaStreamBeginCaptureToGraph(E.stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
-             cudaSuccess;
-        if (ok) {
-            E.pp = b->o.pp;
-            cudaEventRecord(E.ev_fork, E.stream);
-            cudaStreamWaitEvent(E.stream2, E.ev_fork, 0);
-            E.launch_refine(b->Q, n_frames, E.stream2);
-            E.launch_ransac(b->Q, n_frames, b->o.hr, E.stream);
-            cudaEventRecord(E.ev_join, E.stream2);
-            cudaStreamWaitEvent(E.stream, E.ev_join, 0);
-            k_loop_ctl<<<1, 1, 0, E.stream>>>(b->Q, h, 100000ull);
-            ok = cudaStreamEndCapture(E.stream, &body) == cudaSuccess;
-        }
-    }
-    if (ok) {
-        // After the loop: refinement of the frames that finished in the last step.
-        cudaGraph_t tail = nullptr;
-        ok = cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
-        if (ok) {
-            E.launch_refine(b->Q, n_frames, E.stream);
-            ok = cudaStreamEndCapture(E.stream, &tail) == cudaSuccess;
-        }
-        cudaGraphNode_t tail_node;
-        if (ok) ok = cudaGraphAddChildGraphNode(&tail_node, b->graph, &loop_node, 1, tail) == cudaSuccess;
-        if (tail) cudaGraphDestroy(tail);
-    }
-    if (ok) ok = cudaGraphInstantiate(&b->exec, b->graph, 0) == cudaSuccess;
+    E.pp = b->o.pp;
+    bool ok = E.build_loop_graph(b->Q, n_frames, b->o.hr, b->d_init, &b->graph, &b->exec);
     if (ok) ok = cudaEventCreate(&b->e0) == cudaSuccess && cudaEventCreate(&b->e1) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
