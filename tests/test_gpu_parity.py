@@ -193,3 +193,17 @@ def test_nonfinite_points_are_outliers(ctx, oracle):
     np.testing.assert_array_equal(inl, o["inliers"])
     assert not inl[bad].any()
     assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_large_frame_cluster_lm_matches_oracle(ctx, oracle):
+    """N = 25000 at 60 % inliers: the LM of this frame runs on a cluster of CTAs
+    (distributed-shared-memory sums); pose within 1e-6 of the FP64 pipeline."""
+    f = scenes.make_frame(25000, 0.60, 1.0, 9191)
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
+    d = st.details
+    assert d["num_inliers"] == o["info"].num_inliers and d["num_inliers"] >= 10000
+    assert d["best_sample"] == o["info"].ransac.best_sample
+    np.testing.assert_array_equal(inl, o["inliers"])
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6

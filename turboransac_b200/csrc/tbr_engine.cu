@@ -602,6 +602,8 @@ struct StagedAdmission {
     std::vector<int> slots;
     std::vector<FrameDev> devs;
     std::vector<Run> runs;
+    std::vector<std::pair<size_t, size_t>> span;  // first and last frame of each run
+    std::vector<CopyJob> jobs;                    // uv, xyz of frame i at 2i, 2i+1
     FrameDev *hd = nullptr;
     int32_t *ha = nullptr;
     int64_t max_n = 0;
@@ -618,9 +620,9 @@ static size_t stage_bytes(const std::vector<FrameHost> &fr) {
 }
 
 // `stage` holds at least stage_bytes(fr) bytes of pinned memory that no copy in
-// flight reads.
+// flight reads. With copy = false the host copies are left in A.jobs.
 static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o, char *stage,
-                               StagedAdmission &A) {
+                               StagedAdmission &A, bool copy = true) {
     if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
     auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     int64_t replay_total = 0;
@@ -655,7 +657,7 @@ static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         A.max_n = std::max(A.max_n, f.n);
     }
     // Runs of adjacent frames.
-    std::vector<std::pair<size_t, size_t>> span;  // first, last frame of each run
+    auto &span = A.span;
     for (size_t i = 0; i < fr.size(); ++i) {
         const int64_t nb = A.devs[i].n_blocks;
         if (!A.runs.empty() && A.runs.back().b1 == offs[i]) {
@@ -667,7 +669,7 @@ static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         }
     }
     char *h = stage;
-    std::vector<CopyJob> jobs;
+    auto &jobs = A.jobs;
     for (size_t r = 0; r < A.runs.size(); ++r) {
         auto &run = A.runs[r];
         const size_t pts = (size_t)(run.b1 - run.b0) * kSub;
@@ -688,19 +690,13 @@ static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         A.hd[i] = A.devs[i];
         A.ha[i] = A.slots[i];
     }
-    parallel_copy(jobs);
+    if (copy) parallel_copy(jobs);
     return TBR_OK;
 }
 
-static tbr_status upload_staged(Engine &E, const StagedAdmission &A) {
+// Frame records and slot list up, scattered by one kernel.
+static tbr_status upload_records(Engine &E, const StagedAdmission &A) {
     const size_t n = A.slots.size();
-    if (n == 0) return TBR_OK;
-    for (auto &r : A.runs) {
-        const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
-        const size_t p0 = (size_t)r.b0 * kSub;
-        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), r.huv, 16 * pts, cudaMemcpyHostToDevice, E.stream));
-        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), r.hxyz, 24 * pts, cudaMemcpyHostToDevice, E.stream));
-    }
     TBR_CUDA(cudaMemcpyAsync(E.d_admit, A.hd, sizeof(FrameDev) * n, cudaMemcpyHostToDevice, E.stream));
     TBR_CUDA(cudaMemcpyAsync(E.d_active, A.ha, 4 * n, cudaMemcpyHostToDevice, E.stream));
     k_admit_frames<<<(int)n, 128, 0, E.stream>>>(E.P.frames, E.d_admit, E.d_active, (int)n);
@@ -709,15 +705,105 @@ static tbr_status upload_staged(Engine &E, const StagedAdmission &A) {
     return TBR_OK;
 }
 
+// Device side of an admission whose host copies are done: one copy per run and array.
+static tbr_status upload_staged(Engine &E, const StagedAdmission &A) {
+    if (A.slots.empty()) return TBR_OK;
+    for (auto &r : A.runs) {
+        const size_t pts = (size_t)(r.b1 - r.b0) * kSub;
+        const size_t p0 = (size_t)r.b0 * kSub;
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * p0), r.huv, 16 * pts, cudaMemcpyHostToDevice, E.stream));
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * p0), r.hxyz, 24 * pts, cudaMemcpyHostToDevice, E.stream));
+    }
+    return upload_records(E, A);
+}
+
+// Host copies and uploads in groups of consecutive frames of a run, so that
+// the link moves one group while the host threads copy the next: copy threads
+// take 1 MiB pieces in group order, and this thread issues a group's upload as
+// soon as its last piece is in.
+static tbr_status copy_and_upload_overlapped(Engine &E, const StagedAdmission &A) {
+    constexpr size_t kGroupBytes = 8u << 20, kPiece = 1u << 20;
+    struct Group {
+        size_t run, i, j;  // frames i .. j-1 of run
+    };
+    std::vector<Group> groups;
+    size_t total = 0;
+    for (size_t r = 0; r < A.runs.size(); ++r)
+        for (size_t i = A.span[r].first; i <= A.span[r].second;) {
+            size_t j = i, bytes = 0;
+            while (j <= A.span[r].second && (j == i || bytes < kGroupBytes)) {
+                bytes += A.jobs[2 * j].bytes + A.jobs[2 * j + 1].bytes;
+                ++j;
+            }
+            groups.push_back({r, i, j});
+            total += bytes;
+            i = j;
+        }
+    auto upload = [&](const Group &g) -> tbr_status {
+        const auto &run = A.runs[g.run];
+        // points [p0, p1) of the run: the group's frames with their padding
+        const size_t p0 = (size_t)(A.devs[g.i].blk_off - run.b0) * kSub;
+        const size_t p1 = (size_t)(A.devs[g.j - 1].blk_off + A.devs[g.j - 1].n_blocks - run.b0) * kSub;
+        const size_t q0 = (size_t)run.b0 * kSub + p0;
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * q0), run.huv + 16 * p0, 16 * (p1 - p0),
+                                 cudaMemcpyHostToDevice, E.stream));
+        TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * q0), run.hxyz + 24 * p0, 24 * (p1 - p0),
+                                 cudaMemcpyHostToDevice, E.stream));
+        return TBR_OK;
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int T = (int)std::min<size_t>(std::min(8u, hw), total / (4 * kPiece));
+    if (T <= 1) {
+        for (auto &g : groups) {
+            for (size_t k = 2 * g.i; k < 2 * g.j; ++k) std::memcpy(A.jobs[k].dst, A.jobs[k].src, A.jobs[k].bytes);
+            tbr_status st = upload(g);
+            if (st) return st;
+        }
+        return upload_records(E, A);
+    }
+    struct Piece {
+        CopyJob job;
+        size_t group;
+    };
+    std::vector<Piece> pieces;
+    std::unique_ptr<std::atomic<int>[]> left(new std::atomic<int>[groups.size()]);
+    for (size_t g = 0; g < groups.size(); ++g) {
+        int cnt = 0;
+        for (size_t k = 2 * groups[g].i; k < 2 * groups[g].j; ++k)
+            for (size_t o = 0; o < A.jobs[k].bytes; o += kPiece, ++cnt)
+                pieces.push_back({{(char *)A.jobs[k].dst + o, (const char *)A.jobs[k].src + o,
+                                   std::min(kPiece, A.jobs[k].bytes - o)},
+                                  g});
+        left[g].store(cnt, std::memory_order_relaxed);
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < pieces.size();) {
+            std::memcpy(pieces[k].job.dst, pieces[k].job.src, pieces[k].job.bytes);
+            left[pieces[k].group].fetch_sub(1, std::memory_order_release);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(work);
+    tbr_status st = TBR_OK;
+    for (size_t g = 0; g < groups.size(); ++g) {
+        while (left[g].load(std::memory_order_acquire) > 0) std::this_thread::yield();
+        if (st == TBR_OK) st = upload(groups[g]);
+    }
+    for (auto &x : th) x.join();
+    if (st) return st;
+    return upload_records(E, A);
+}
+
 // Both halves through the context's own staging buffer.
 static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
                                std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
     tbr_status st = E.ensure_stage(stage_bytes(fr));
     if (st) return st;
     StagedAdmission A;
-    st = stage_frames(E, fr, o, (char *)E.h_stage, A);
+    st = stage_frames(E, fr, o, (char *)E.h_stage, A, false);
     if (st) return st;
-    st = upload_staged(E, A);
+    st = copy_and_upload_overlapped(E, A);
     if (st) return st;
     slots = A.slots;
     max_n = A.max_n;
@@ -1358,6 +1444,9 @@ static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, 
     s->cv_done.notify_all();
 }
 
+// Resident frames from which a serving step overlaps refinement with RANSAC.
+constexpr int kServerOverlapFrames = 64;
+
 // One iteration of the request loop, pipelined with the device:
 //   A. while the previous step runs, take queued requests that fit the free
 //      slots and point blocks and copy them into pinned staging;
@@ -1492,7 +1581,21 @@ static tbr_status server_step(tbr_server *s) {
         for (int i = 0; i < na; ++i) ha[i] = s->resident[i].slot;
         TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * na, cudaMemcpyHostToDevice, E.stream));
         E.P.n_active = na;
-        E.launch_step(E.P, na, s->o.hr);
+        if (na >= kServerOverlapFrames) {
+            // Many resident frames: the refinement of frames that finished RANSAC
+            // in earlier steps runs beside this step's RANSAC (disjoint frames),
+            // as in the batch graph; a frame is refined one step after it finishes.
+            TBR_CUDA(cudaEventRecord(E.ev_fork, E.stream));
+            TBR_CUDA(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
+            E.launch_refine(E.P, na, E.stream2);
+            E.launch_ransac(E.P, na, s->o.hr, E.stream);
+            TBR_CUDA(cudaEventRecord(E.ev_join, E.stream2));
+            TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_join, 0));
+            k_tick<<<1, 1, 0, E.stream>>>(E.P);
+        } else {
+            // Few: RANSAC, then the refinement of what finished, in this step.
+            E.launch_step(E.P, na, s->o.hr);
+        }
         k_gather_status<<<(na + 255) / 256, 256, 0, E.stream>>>(E.P, s->d_status);
         TBR_CUDA(cudaGetLastError());
         TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));

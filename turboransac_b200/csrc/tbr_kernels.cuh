@@ -1419,7 +1419,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
 
 // Frames with fewer inliers than this run their LM on one CTA; larger ones on
 // a cluster of kLMCluster CTAs (a single SM would serialise them).
-constexpr int64_t kLMClusterMin = 3000;
+constexpr int64_t kLMClusterMin = 10000;
 
 __global__ void __launch_bounds__(kLMThreads, 2) k_lm_small(Pools P) {
     const int slot = P.active[blockIdx.x];
