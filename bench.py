@@ -254,6 +254,42 @@ def run_plain_serving(ctx, reqs, count=200):
             "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
 
 
+def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30):
+    """Served throughput at saturation: the serving requests submitted at once
+    (repeats x the pool), completion rate of the continuous-batching server."""
+    import numpy as np
+
+    from turboransac_b200 import Server, scenes
+    srv = Server(ctx, budget_bytes=budget, max_slots=1024)
+    for r in reqs[:32]:
+        srv.submit(r)
+    srv.drain()
+    srv.poll()
+    ids = {}
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        for k, r in enumerate(reqs):
+            ids[srv.submit(r)] = k
+    srv.drain()
+    dt = time.perf_counter() - t0
+    got = []
+    while True:
+        g = srv.poll()
+        if not g:
+            break
+        got += g
+    srv.close()
+    lat = np.array([g["latency_ms"] for g in got])
+    ok = 0
+    for g in got:
+        f = reqs[ids[g["id"]]]
+        ae, te = scenes.pose_error(scenes.quat_to_rotmat(g["q"]), g["t"], f.R_gt, f.t_gt)
+        ok += (g["status"] == 0 and ae < 5.0 and te < 5.0)
+    return {"frames_per_s": len(got) / dt, "requests": len(got), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "success_rate": ok / max(len(got), 1),
+            "load": f"{repeats} x {len(reqs)} serving requests submitted at once"}
+
+
 def run_reference(args, world, rank):
     """--impl reference: the CPU implementation of the path on the host cores."""
     if rank != 0:
@@ -530,6 +566,8 @@ def main():
         serving, reqs = run_serving(ctx, args.serve_seconds)
         serving["plain_call"] = run_plain_serving(ctx, reqs)
         serving["throughput_vs_plain"] = serving["throughput_fps"] / serving["plain_call"]["frames_per_s"]
+        serving["capacity"] = run_serving_capacity(ctx, reqs)
+        serving["capacity_vs_plain"] = serving["capacity"]["frames_per_s"] / serving["plain_call"]["frames_per_s"]
         print(f"[bench] serving: {serving['throughput_fps']:.0f} frames/s p50 {serving['p50_ms']:.2f} ms "
               f"p99 {serving['p99_ms']:.2f} ms success {serving['success_rate']:.4f}", file=sys.stderr, flush=True)
 

@@ -398,7 +398,7 @@ class Engine {
         auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
         beg(8); k_inliers<<<n_active, 1024, 0, st>>>(Q); end(8);
         beg(9);
-        k_lm_small<<<n_active, kLMThreads, 0, st>>>(Q);
+        k_lm_small<<<n_active, kLMSmallThreads, 0, st>>>(Q);
         k_lm<<<n_active * kLMCluster, kLMThreads, 0, st>>>(Q);
         end(9);
     }

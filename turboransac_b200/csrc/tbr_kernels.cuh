@@ -35,7 +35,8 @@ constexpr int kMaxScoreChunks = 64;               // FP32 scoring point chunks p
 constexpr int kMaxActive = 1024;                  // frames advanced by one step
 constexpr uint32_t kMaxPolls = 1u << 26;          // bounded mbarrier waits (~seconds)
 constexpr int kScoreWarps = 4;                    // warps per scoring CTA
-constexpr int kLMThreads = 256;
+constexpr int kLMThreads = 256;       // per CTA of a cluster LM (two CTAs per SM)
+constexpr int kLMSmallThreads = 384;  // one CTA per frame: 12 warps, no register spills
 
 // kLMReady: RANSAC finished in the step stamped in lm_epoch; k_inliers takes it
 // one step later (so that in the captured loop it can run beside the next
@@ -1421,7 +1422,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
 // a cluster of kLMCluster CTAs (a single SM would serialise them).
 constexpr int64_t kLMClusterMin = 10000;
 
-__global__ void __launch_bounds__(kLMThreads, 2) k_lm_small(Pools P) {
+__global__ void __launch_bounds__(kLMSmallThreads, 1) k_lm_small(Pools P) {
     const int slot = P.active[blockIdx.x];
     const FrameDev &f = P.frames[slot];
     if (f.status != kLMPending || f.num_inliers >= kLMClusterMin || f.lm_force_cluster) return;
