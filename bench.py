@@ -491,6 +491,13 @@ def main():
     ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
     ctx = Context(local, 6 << 30)
     batch = Batch(ctx, frames, ro, hyp_per_thread=args.hr)
+    # Scoring shape chosen by the autotuner on this batch (before the timed region).
+    tuned = None
+    if not args.hr:
+        best, tried = batch.autotune(repeats=2)
+        default = next(t for t in tried if t["hyp_per_thread"] == 4 and t["points_per_iter"] == 2
+                       and t["chunk_points"] == 0)
+        tuned = {"best": best, "default_ms": default["ms"], "candidates": len(tried)}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     for _ in range(args.warmup):
@@ -580,7 +587,8 @@ def main():
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "global_batch": world * args.frames,
                        "l2": "flushed before every timed step (256 MiB write)",
-                       "engine_steps_per_batch": steps_per_run, "parallelism": f"replicas x{world}"},
+                       "engine_steps_per_batch": steps_per_run, "parallelism": f"replicas x{world}",
+                       "scoring_shape": tuned},
             "success_rate": succ,
             "pairs_scored_per_batch": pairs,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",

@@ -221,6 +221,24 @@ typedef struct tbr_kernel_profile {
 tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max, int32_t *n_out,
                              uint64_t *pairs_scored);
 
+/* Scoring-shape autotuner (no reference counterpart). Times the batch's graph
+ * `repeats` times under each candidate shape -- hypotheses per warp block
+ * (32 x hyp_per_thread: 64, 128, 256), points per iteration (2, 4) and points
+ * per work-item tile (0 = sized from the step's work, 256, 512, 1024, 2048) --
+ * and keeps the fastest for later tbr_batch_run calls. The shape changes only
+ * the order of FP32 partial sums inside the filter; every candidate within the
+ * filter band is re-scored in FP64, so results do not depend on it. entries
+ * (may be NULL) receive up to max candidates with their mean device ms. */
+typedef struct tbr_tune_entry {
+    int32_t hyp_per_thread;
+    int32_t points_per_iter;
+    int32_t chunk_points;
+    int32_t pad;
+    double ms;
+} tbr_tune_entry;
+tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *entries, int32_t max,
+                              int32_t *n_out, tbr_tune_entry *best);
+
 /* Measured FP32 FMA throughput of the context's device (packed FP32x2 FMA
  * chains on every SM, CUDA-event timed): the denominator of the scoring
  * kernel's roofline. */

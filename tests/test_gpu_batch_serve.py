@@ -112,3 +112,25 @@ def test_server_cancel_and_errors(ctx):
     (r2,) = srv.poll()
     assert r2["id"] == rid2 and r2["status"] == 0
     srv.close()
+
+
+def test_autotune_keeps_results(ctx):
+    """Every scoring shape gives the same results (the FP64 re-rank decides), and
+    the tuned batch keeps returning them."""
+    fr = mixed_frames()
+    b = Batch(ctx, fr, RO)
+    b.run()
+    b.sync()
+    before = b.results()
+    best, tried = b.autotune(repeats=1)
+    assert len(tried) == 20 and all(t["ms"] > 0 for t in tried)
+    assert best["ms"] == min(t["ms"] for t in tried)
+    b.run()
+    b.sync()
+    after = b.results()
+    b.close()
+    for r0, r1 in zip(before, after):
+        assert r1["status"] == 0
+        assert r1["samples"] == r0["samples"] and r1["best_sample"] == r0["best_sample"]
+        assert r1["num_inliers"] == r0["num_inliers"]
+        assert quat_angle(r1["q"], r0["q"]) < 1e-12 and np.abs(r1["t"] - r0["t"]).max() < 1e-12

@@ -85,6 +85,15 @@ class ServerResultC(C.Structure):
                 ("submit_to_done_ms", C.c_double)]
 
 
+class TuneEntryC(C.Structure):
+    _fields_ = [("hyp_per_thread", C.c_int32), ("points_per_iter", C.c_int32), ("chunk_points", C.c_int32),
+                ("pad", C.c_int32), ("ms", C.c_double)]
+
+    def as_dict(self):
+        return {"hyp_per_thread": self.hyp_per_thread, "hyp_per_block": 32 * self.hyp_per_thread,
+                "points_per_iter": self.points_per_iter, "chunk_points": self.chunk_points, "ms": self.ms}
+
+
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
                 ("steps", C.c_int64), ("resident_sum", C.c_int64), ("host_stage_ms", C.c_double),
@@ -101,7 +110,7 @@ EXPORTS = [
     "tbr_abi_version", "tbr_last_error", "tbr_default_ransac_options", "tbr_default_bundle_options",
     "tbr_context_create", "tbr_context_destroy", "tbr_estimate_absolute_pose", "tbr_get_inliers",
     "tbr_bundle_adjust", "tbr_estimate_batch", "tbr_batch_create", "tbr_batch_run", "tbr_batch_sync",
-    "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
+    "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_batch_autotune", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
     "tbr_server_submit_nocopy", "tbr_server_get_stats", "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
     "tbr_debug_score_samples", "tbr_msac_score_noalloc",
 ]
@@ -138,6 +147,8 @@ def lib() -> C.CDLL:
     L.tbr_batch_destroy.argtypes = [vp]
     L.tbr_batch_profile.argtypes = [vp, C.POINTER(KernelProfileC), C.c_int32, C.POINTER(C.c_int32),
                                     C.POINTER(C.c_uint64)]
+    L.tbr_batch_autotune.argtypes = [vp, C.c_int32, C.POINTER(TuneEntryC), C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(TuneEntryC)]
     L.tbr_measure_fp32_peak.argtypes = [vp, C.POINTER(C.c_double)]
     L.tbr_server_create.argtypes = [vp, C.POINTER(ServerConfigC), C.POINTER(vp)]
     L.tbr_server_submit.argtypes = [vp, C.POINTER(FrameDescC), C.POINTER(C.c_uint64)]

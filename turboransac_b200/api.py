@@ -358,6 +358,16 @@ class Batch:
         check(_lib.lib().tbr_batch_profile(self._h, out, 16, C.byref(n), C.byref(pairs)))
         return {out[i].name.decode(): (out[i].total_ms, out[i].launches) for i in range(n.value)}, pairs.value
 
+    def autotune(self, repeats: int = 3):
+        """Time every scoring shape (hypotheses per block x points per iteration x
+        point tile) on this batch and keep the fastest; returns (best, all)."""
+        ent = (_lib.TuneEntryC * 64)()
+        n = C.c_int32()
+        best = _lib.TuneEntryC()
+        with self.ctx._lock:
+            check(_lib.lib().tbr_batch_autotune(self._h, repeats, ent, 64, C.byref(n), C.byref(best)))
+        return best.as_dict(), [ent[i].as_dict() for i in range(n.value)]
+
     def close(self):
         if self._h:
             _lib.lib().tbr_batch_destroy(self._h)

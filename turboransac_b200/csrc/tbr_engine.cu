@@ -1253,6 +1253,87 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
     return TBR_OK;
 }
 
+tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *entries, int32_t max,
+                              int32_t *n_out, tbr_tune_entry *best) {
+    if (!b || repeats < 1 || max < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    Engine &E = b->ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    const int n = (int)b->slots.size();
+    struct Shape {
+        int hr, pp;
+    };
+    const Shape shapes[4] = {{2, 4}, {4, 2}, {4, 4}, {8, 2}};  // the compiled scoring variants
+    const int chunks[5] = {0, 256, 512, 1024, 2048};
+    std::vector<tbr_tune_entry> tried;
+    cudaEvent_t t0, t1;
+    TBR_CUDA(cudaEventCreate(&t0));
+    TBR_CUDA(cudaEventCreate(&t1));
+    auto apply = [&](int hr, int pp, int chunk, cudaGraph_t *g, cudaGraphExec_t *x) -> bool {
+        k_set_shape<<<(n + 127) / 128, 128, 0, E.stream>>>(b->d_init, n, hr, chunk);
+        if (cudaGetLastError() != cudaSuccess) return false;
+        E.pp = pp;
+        return E.build_loop_graph(b->Q, n, hr, b->d_init, g, x);
+    };
+    tbr_status st = TBR_OK;
+    for (const Shape &sh : shapes) {
+        for (int chunk : chunks) {
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t x = nullptr;
+            if (!apply(sh.hr, sh.pp, chunk, &g, &x)) {
+                st = fail(TBR_ERR_CUDA, "autotune graph capture failed");
+                break;
+            }
+            float ms = 0.f;
+            cudaError_t e = cudaGraphLaunch(x, E.stream);  // warm-up
+            if (e == cudaSuccess) e = cudaEventRecord(t0, E.stream);
+            for (int r = 0; r < repeats && e == cudaSuccess; ++r) e = cudaGraphLaunch(x, E.stream);
+            if (e == cudaSuccess) e = cudaEventRecord(t1, E.stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(t1);
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, t0, t1);
+            cudaGraphExecDestroy(x);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                st = fail(TBR_ERR_CUDA, cudaGetErrorString(e));
+                break;
+            }
+            TBR_CUDA(cudaMemcpy(E.h_counters, b->Q.counters, 8 * kCNum, cudaMemcpyDeviceToHost));
+            if (E.h_counters[kCError]) {
+                st = fail(TBR_ERR_INTERNAL, "device error during autotune");
+                break;
+            }
+            tried.push_back({sh.hr, sh.pp, chunk, 0, (double)ms / repeats});
+        }
+        if (st) break;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (st) return st;
+    size_t bi = 0;
+    for (size_t i = 1; i < tried.size(); ++i)
+        if (tried[i].ms < tried[bi].ms) bi = i;
+    const tbr_tune_entry win = tried[bi];
+    // Keep the winner: new initial records and graph for tbr_batch_run.
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    if (!apply(win.hyp_per_thread, win.points_per_iter, win.chunk_points, &g, &x))
+        return fail(TBR_ERR_CUDA, "autotune graph capture failed");
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->graph = g;
+    b->exec = x;
+    b->o.hr = win.hyp_per_thread;
+    b->o.pp = win.points_per_iter;
+    b->o.chunk_points = win.chunk_points;
+    b->launched = false;
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    if (entries)
+        for (int i = 0; i < (int)tried.size() && i < max; ++i) entries[i] = tried[i];
+    if (n_out) *n_out = (int32_t)tried.size();
+    if (best) *best = win;
+    return TBR_OK;
+}
+
 tbr_status tbr_batch_run(tbr_batch *b) {
     if (!b) return fail(TBR_ERR_INVALID_ARG, "NULL batch");
     Engine &E = b->ctx->E;

@@ -1471,6 +1471,14 @@ __global__ void k_reset_frames(Pools P, const FrameDev *init) {
     if (a == 0 && threadIdx.x < kCNum) P.counters[threadIdx.x] = 0;
 }
 
+// Autotuner: the scoring shape of a batch's initial frame records.
+__global__ void k_set_shape(FrameDev *init, int n, int hr, int chunk_points) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+    init[a].hr = hr;
+    init[a].chunk_points = chunk_points;
+}
+
 // Admission: staged[a] -> frames[slots[a]] (one upload for a whole batch).
 __global__ void k_admit_frames(FrameDev *frames, const FrameDev *staged, const int32_t *slots, int n) {
     const int a = blockIdx.x;
