@@ -86,7 +86,9 @@ typedef struct tbr_ext_options {
      * trials multiplier 3, 100000-sample cap, default BundleOptions with a
      * 1/f loss scale (turbo_ransac.cu:145,227,231; entry.cu:122-123).
      * 1: honour success_prob, dyn_num_trials_mult, min_iterations and the
-     * caller's bundle options. */
+     * caller's bundle options; in tbr_bundle_adjust also the loss type
+     * (TRIVIAL, TRUNCATED, HUBER, CAUCHY) and the per-point weights, which
+     * the reference ignores (ba.cu:111-130). */
     int32_t honor_options;
     int32_t skip_refine;          /* 1: return the RANSAC pose, no LM */
     int64_t force_samples;        /* > 0: score exactly this many samples, no early stop */

@@ -44,7 +44,7 @@ class RansacCfg(C.Structure):
                 ("success_prob", C.c_double), ("trials_mult", C.c_double),
                 ("force_samples", C.c_int64), ("seed", C.c_uint64),
                 ("replay", C.c_void_p), ("replay_count", C.c_int64), ("threads", C.c_int),
-                ("quirk", C.c_int)]
+                ("quirk", C.c_int), ("min_samples", C.c_int64)]
 
 
 class RansacOut(C.Structure):
@@ -57,7 +57,7 @@ class LMOpts(C.Structure):
     _fields_ = [("max_iterations", C.c_int64), ("loss_scale", C.c_double),
                 ("gradient_tol", C.c_double), ("step_tol", C.c_double),
                 ("initial_lambda", C.c_double), ("min_lambda", C.c_double),
-                ("max_lambda", C.c_double)]
+                ("max_lambda", C.c_double), ("loss", C.c_int32), ("weights", C.c_void_p)]
 
 
 class LMStats(C.Structure):
@@ -71,9 +71,10 @@ class EstimateInfo(C.Structure):
 
 
 def _cfg(samples_per_round=1000, seed=0, force_samples=0, replay=None, threads=1,
-         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0, quirk=False):
+         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0, quirk=False, min_samples=0):
     cfg = RansacCfg()
     cfg.quirk = int(quirk)
+    cfg.min_samples = min_samples
     cfg.samples_per_round = samples_per_round
     cfg.max_total_samples = max_total_samples
     cfg.success_prob = success_prob
@@ -190,11 +191,13 @@ class Oracle:
         return res
 
     def lm(self, x, X, cam, q, t, max_iterations=100, loss_scale=1.0, gradient_tol=1e-10,
-           step_tol=1e-8, initial_lambda=1e-3, min_lambda=1e-10, max_lambda=1e10):
+           step_tol=1e-8, initial_lambda=1e-3, min_lambda=1e-10, max_lambda=1e10, loss=0, weights=None):
+        """loss: 0 Cauchy (the reference), 1 truncated, 2 Huber, 3 trivial."""
         q = np.array(q, np.float64)
         t = np.array(t, np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
         o = LMOpts(max_iterations, loss_scale, gradient_tol, step_tol, initial_lambda, min_lambda,
-                   max_lambda)
+                   max_lambda, loss, w.ctypes.data if w is not None else None)
         st = LMStats()
         self.lib.orc_lm(np.ascontiguousarray(x), np.ascontiguousarray(X), x.shape[0],
                         np.asarray(cam, np.float64), q, t, C.byref(o), C.byref(st))

@@ -473,6 +473,29 @@ struct LMProblem {
     int64_t n;
     double fx, fy, cx, cy;
     double inv_sq_thr;  // CauchyLoss_cuda, robust_loss.cuh:24-38
+    int loss = 0;                    // 0 Cauchy, 1 truncated, 2 Huber, 3 trivial
+    const double *w8 = nullptr;      // per-point multipliers (NULL: 1.0, jaco.cuh's uniform weight)
+    double thr = 1.0, sq_thr = 1.0;  // loss scale and its square
+
+    double pw(int64_t i) const { return w8 ? w8[i] : 1.0; }
+    // loss(r2): CauchyLoss_cuda / TruncatedLoss_cuda (robust_loss.cuh:10-38); Huber
+    // and trivial as the published PoseLib losses the option enum names.
+    double loss_of(double r2) const {
+        switch (loss) {
+            case 1: return std::fmin(r2, sq_thr);
+            case 2: return r2 <= sq_thr ? r2 : 2.0 * thr * std::sqrt(r2) - sq_thr;
+            case 3: return r2;
+            default: return std::log1p(r2 * inv_sq_thr);
+        }
+    }
+    double weight_of(double r2) const {
+        switch (loss) {
+            case 1: return r2 < sq_thr ? 1.0 : 0.0;
+            case 2: return r2 <= sq_thr ? 1.0 : thr / std::sqrt(r2);
+            case 3: return 1.0;
+            default: return std::fmax(DBL_MIN, inv_sq_thr / (1.0 + r2 * inv_sq_thr));
+        }
+    }
 
     // residual(), jaco.cuh:31-104: Cauchy cost, points behind the camera dropped.
     double residual(const double *q, const double *t) const {
@@ -488,7 +511,7 @@ struct LMProblem {
             p1 = fy * p1 + cy;
             const double r0 = p0 - x[2 * i], r1 = p1 - x[2 * i + 1];
             const double r_squared = r0 * r0 + r1 * r1;
-            cost += valid ? 1.0 * std::log1p(r_squared * inv_sq_thr) : 0.0;
+            cost += valid ? pw(i) * loss_of(r_squared) : 0.0;
         }
         return cost;
     }
@@ -509,7 +532,7 @@ struct LMProblem {
             const double zp0 = fx * z0 + cx, zp1 = fy * z1 + cy;
             double r0 = zp0 - x[2 * i], r1 = zp1 - x[2 * i + 1];
             const double r_squared = r0 * r0 + r1 * r1;
-            const double weight = 1.0 * std::fmax(DBL_MIN, inv_sq_thr / (1.0 + r_squared * inv_sq_thr));
+            const double weight = pw(i) * weight_of(r_squared);
             const double Z_valid = (Z[2] >= 0.0) ? 1.0 : 0.0;
             const double W_valid = (weight != 0.0) ? 1.0 : 0.0;
             const double valid = Z_valid * W_valid;
@@ -828,7 +851,7 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
         if (forced) break;
         int64_t need = needed_samples(out->found ? out->count : 0, n, cfg->success_prob, cfg->trials_mult,
                                       cfg->quirk);
-        if (done > need) stop = true;
+        if (done > need && done >= cfg->min_samples) stop = true;
     }
     out->samples = done;
     out->rounds = rounds;
@@ -839,6 +862,10 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
 void orc_lm(const double *x, const double *X, int64_t n, const double cam[4], double q[4],
             double t[3], const orc_lm_opts *opt, orc_lm_stats *stats) {
     LMProblem pb{x, X, n, cam[0], cam[1], cam[2], cam[3], 1.0 / (opt->loss_scale * opt->loss_scale)};
+    pb.loss = opt->loss;
+    pb.w8 = opt->weights;
+    pb.thr = opt->loss_scale;
+    pb.sq_thr = opt->loss_scale * opt->loss_scale;
     orc_lm_stats st;
     lm_impl(pb, q, t, *opt, st);
     if (stats) *stats = st;

@@ -68,6 +68,7 @@ typedef struct orc_ransac_cfg {
     int64_t replay_count;
     int threads;                /* worker threads over samples (>=1) */
     int quirk;                  /* 1: stop rule with the x86 int-conversion result (INT_MIN) */
+    int64_t min_samples;        /* no stop before this many samples (0: none) */
 } orc_ransac_cfg;
 
 typedef struct orc_ransac_out {
@@ -94,6 +95,11 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
 typedef struct orc_lm_opts {
     int64_t max_iterations;
     double loss_scale, gradient_tol, step_tol, initial_lambda, min_lambda, max_lambda;
+    /* Honoured-options extension (the reference always uses Cauchy and unit
+     * weights): 0 Cauchy, 1 truncated (robust_loss.cuh:10-22), 2 Huber,
+     * 3 trivial; weights: NULL or one multiplier per point on loss and weight. */
+    int32_t loss;
+    const double *weights;
 } orc_lm_opts;
 
 typedef struct orc_lm_stats {

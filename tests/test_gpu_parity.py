@@ -207,3 +207,47 @@ def test_large_frame_cluster_lm_matches_oracle(ctx, oracle):
     assert d["best_sample"] == o["info"].ransac.best_sample
     np.testing.assert_array_equal(inl, o["inliers"])
     assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+def test_honoured_ransac_options_match_oracle(ctx, oracle):
+    """honor_options: min_iterations, success_prob and dyn_num_trials_mult of
+    RansacOptions_cuda (utils.h:16-19, ignored by the reference) take effect and
+    give the oracle's samples, selection and pose."""
+    f = scenes.plain_frame(2)
+    for kw in ({"min_iterations": 5000}, {"success_prob": 0.99, "dyn_num_trials_mult": 1.0},
+               {"min_iterations": 2500, "success_prob": 0.999999}):
+        ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0, **kw)
+        st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                                   honor_options=True)
+        o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000,
+                            min_samples=kw.get("min_iterations", 0), success_prob=kw.get("success_prob", 0.9999),
+                            trials_mult=kw.get("dyn_num_trials_mult", 3.0))
+        d, info = st.details, o["info"]
+        assert d["samples"] == info.ransac.samples, kw
+        if "min_iterations" in kw:
+            assert d["samples"] >= kw["min_iterations"]
+        assert d["best_sample"] == info.ransac.best_sample
+        np.testing.assert_array_equal(inl, o["inliers"])
+        assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("loss_type", [0, 1, 2, 3])
+def test_bundle_adjust_honoured_loss_and_weights(ctx, oracle, loss_type):
+    """honor_options on bundle_adjust_cuda: BundleOptions_cuda::loss_type
+    (TRIVIAL, TRUNCATED, HUBER, CAUCHY; the reference always runs Cauchy) and
+    per-point weights (ignored by the reference) against the FP64 oracle LM."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "lm.npz"))
+    rng = np.random.default_rng(17 + loss_type)
+    for k in range(3):
+        x, X, K = d[f"x{k}"], d[f"X{k}"], d[f"cam{k}"]
+        scale = float(d[f"scale{k}"])
+        w = rng.uniform(0.5, 2.0, x.shape[0])
+        cam = Camera_cuda(1, 640, 480, list(K))
+        pose, st = ctx.bundle_adjust(x, X, cam, CameraPose_cuda(d[f"q0_{k}"], d[f"t0_{k}"]),
+                                     BundleOptions_cuda(loss_scale=scale, loss_type=loss_type), weights=w,
+                                     honor_options=True)
+        oq, ot, ost = oracle.lm(x, X, K, d[f"q0_{k}"], d[f"t0_{k}"], loss_scale=scale,
+                                loss={0: 3, 1: 1, 2: 2, 3: 0}[loss_type], weights=w)
+        assert quat_angle(pose.q, oq) < 1e-6, (loss_type, k)
+        assert np.abs(pose.t - ot).max() < 1e-6, (loss_type, k)

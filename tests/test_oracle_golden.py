@@ -129,3 +129,15 @@ def test_stop_rule_quirk_vs_saturation(oracle):
     s = oracle.ransac(xn, f.xyz, thr * thr, seed=f.seed, samples_per_round=1000, quirk=False, threads=8)
     assert q["samples"] == 1000 and q["count"] < 10   # INT_MIN ends the loop after one round
     assert s["samples"] > 1000 and s["count"] > 300   # saturating rule keeps sampling
+
+
+def test_oracle_min_samples_delays_the_stop(oracle):
+    from helpers import normalized, sq_thr
+    from turboransac_b200 import scenes
+    f = scenes.plain_frame(2)
+    xn = normalized(f)
+    thr = sq_thr(f)
+    a = oracle.ransac(xn, f.xyz, thr, seed=f.seed)
+    b = oracle.ransac(xn, f.xyz, thr, seed=f.seed, min_samples=4000)
+    assert a["samples"] < 4000 <= b["samples"]
+    assert b["score"] <= a["score"]

@@ -103,6 +103,7 @@ struct FrameHost {
 struct RunOptions {
     int64_t B = 1000;
     int64_t max_total = 100000;
+    int64_t min_samples = 0;
     int64_t force_samples = 0;
     double success_prob = 0.9999;
     double trials_mult = 3.0;
@@ -137,6 +138,7 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
     if (honor && ro) {
         o.success_prob = ro->success_prob;
         o.trials_mult = ro->dyn_num_trials_mult;
+        o.min_samples = (int64_t)ro->min_iterations;
     }
     if (honor && bo) {
         o.lm_max_iter = (int64_t)bo->max_iterations;
@@ -219,7 +221,7 @@ class Engine {
         P.max_hyps = std::max<int64_t>(P.max_hyps, 4096);
         P.max_parts = P.max_hyps * 32;
         P.max_hb = P.max_hyps / 32 + kMaxActive;
-        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24) + kBlockBytes;
+        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 8) + kBlockBytes;
         max_blocks = (int64_t)((rest - (size_t)(P.max_hyps * per_hyp) - P.max_hb * 4) / per_block) - 1;
         if (max_blocks < 64) return fail(TBR_ERR_INVALID_ARG, "workspace too small for points");
         // One allocation, carved with 256-byte alignment.
@@ -238,6 +240,7 @@ class Engine {
         add((void **)&P.mask, np);
         add((void **)&P.lx64, 16 * np);
         add((void **)&P.lX64, 24 * np);
+        add((void **)&P.lw64, 8 * np);
         add((void **)&P.pts32, (size_t)kBlockBytes * max_blocks);
         add((void **)&P.sample_prefix, 8 * (kMaxActive + 1));
         add((void **)&P.item_prefix, 8 * (kMaxActive + 1));
@@ -332,6 +335,7 @@ class Engine {
         }
         f.B = o.B;
         f.max_total = o.max_total;
+        f.min_samples = o.min_samples;
         f.force_samples = o.force_samples;
         f.log_missing = std::log(1.0 - o.success_prob);
         f.trials_mult = o.trials_mult;
@@ -1076,13 +1080,26 @@ tbr_status tbr_get_inliers(tbr_context *ctx, const double q[4], const double t[3
 tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X, int64_t n, const double K[4],
                              double q[4], double t[3], const tbr_bundle_options *opt, const double *weights,
                              const tbr_ext_options *ext, tbr_stats *stats) {
-    (void)weights;  // ignored, as in the reference (jaco.cuh:36,123 use a uniform weight)
-    (void)ext;
+    // The reference uses the Cauchy loss and unit weights whatever the options
+    // (ba.cu:111-130, jaco.cuh:36,123); with honor_options the loss type and
+    // the weights are applied.
     if (!ctx || !x || !X || !K || !q || !t || n < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     tbr_bundle_options bo;
     tbr_default_bundle_options(&bo);
     if (opt) bo = *opt;
     if (!(bo.loss_scale > 0)) return fail(TBR_ERR_INVALID_ARG, "loss_scale must be > 0");
+    const bool honor = ext && ext->honor_options;
+    int32_t loss = kLossCauchy;
+    if (honor) {
+        switch (bo.loss_type) {  // BundleOptions_cuda::LossType, utils.h:45-52
+            case 0: loss = kLossTrivial; break;
+            case 1: loss = kLossTruncated; break;
+            case 2: loss = kLossHuber; break;
+            case 3: loss = kLossCauchy; break;
+            default: return fail(TBR_ERR_INVALID_ARG, "loss type not supported (TRUNCATED_LE_ZACH)");
+        }
+    }
+    const bool weighted = honor && weights != nullptr;
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1105,6 +1122,11 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     fd.focal = 1.0;
     for (int k = 0; k < 4; ++k) fd.lm_cam[k] = K[k];
     fd.lm_inv_sq_thr = 1.0 / (bo.loss_scale * bo.loss_scale);  // CauchyLoss_cuda(loss_scale)
+    fd.lm_thr = bo.loss_scale;
+    fd.lm_loss = loss;
+    fd.lm_weighted = weighted ? 1 : 0;
+    if (weighted)
+        TBR_CUDA(cudaMemcpyAsync(E.P.lw64 + fd.blk_off * kSub, weights, 8 * n, cudaMemcpyHostToDevice, E.stream));
     fd.lm_max_iter = (int64_t)bo.max_iterations;
     fd.lm_grad_tol = bo.gradient_tol;
     fd.lm_step_tol = bo.step_tol;

@@ -88,6 +88,7 @@ struct __align__(16) FrameDev {
     unsigned long long bmin[3], bmax[3];
     int64_t B;
     int64_t max_total;
+    int64_t min_samples;  // no stop before this many samples (honoured min_iterations; else 0)
     int64_t force_samples;
     double log_missing, trials_mult;
     int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass (2 * HP)
@@ -95,6 +96,9 @@ struct __align__(16) FrameDev {
     int64_t lm_max_iter;
     double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
     double lm_inv_sq_thr, lm_grad_tol, lm_step_tol, lm_lambda0, lm_min_lambda, lm_max_lambda;
+    double lm_thr;            // loss scale (LM units) of the honoured truncated / Huber losses
+    int32_t lm_loss;          // kLossCauchy (the reference's), kLossTruncated, kLossHuber, kLossTrivial
+    int32_t lm_weighted;      // 1: per-point multipliers in Pools::lw64 (bundle adjust, honoured)
     int32_t chunk_points, max_rounds_step;  // max_rounds_step: 0 = kMaxRoundsPerStep
     // ---- RANSAC progress ----
     int64_t samples_done, rounds_done, hyps_done;
@@ -133,6 +137,7 @@ struct Pools {
     uint8_t *mask;       // final inlier mask (1/pt)
     double *lx64;        // LM: pixels / f (2/pt)
     double *lX64;        // LM: world points (3/pt)
+    double *lw64;        // LM: per-point loss multipliers (bundle adjust with honoured weights)
     float2 *pts32;       // staging blocks: [X|Y|Z|-x/tau|-y/tau] x kSub, each value duplicated
     // step prefixes (n_active + 1)
     int64_t *sample_prefix;
@@ -349,6 +354,7 @@ __global__ void k_plan(Pools P) {
                     r = need / f->B + 1 - f->rounds_done;
                     if (need < 0 || r < 1) r = 1;
                 }
+                r = max(r, (f->min_samples + f->B - 1) / f->B - f->rounds_done);
                 r = min(r, max_rounds - f->rounds_done);
                 r = min(r, (int64_t)(f->max_rounds_step > 0 ? f->max_rounds_step : kMaxRoundsPerStep));
                 // Growth cap: the frame's s-th step runs at most 4 * 2^(s-1) rounds,
@@ -1027,7 +1033,7 @@ __global__ void __launch_bounds__(256) k_finalize(Pools P) {
         if (forced) continue;
         const int64_t after = f.step_first + (r + 1) * f.B;
         const int64_t need = needed_samples(f.found ? f.best_count : 0, f.n, f.log_missing, f.trials_mult, f.quirk);
-        if (after > need || after >= f.max_total) {
+        if ((after > need && after >= f.min_samples) || after >= f.max_total) {
             stop = true;
             r_end = r + 1;
             break;
@@ -1160,7 +1166,8 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, do
 
 constexpr int kLMCluster = 8;  // CTAs cooperating on one frame's LM
 
-constexpr int kLMSums = 28;  // cost + 21 J^T W J + 6 J^T W r
+constexpr int kLMSums = 28;
+enum LMLoss : int32_t { kLossCauchy = 0, kLossTruncated = 1, kLossHuber = 2, kLossTrivial = 3 };  // cost + 21 J^T W J + 6 J^T W r
 
 // One pass over inliers [i0, i1) at pose (q, t): the FP64 Cauchy cost
 // (jaco.cuh:31-104) and, from the same FP64 residuals, the J^T W J lower
@@ -1169,7 +1176,8 @@ constexpr int kLMSums = 28;  // cost + 21 J^T W J + 6 J^T W r
 // reference's parameterisation (rotation post-multiplied, translation t + R dt).
 // out[0] = cost, out[1..27] = accumulators (block totals).
 __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q, const double *t,
-                        const double *cam, double inv_sq_thr, double *scratch, double *out) {
+                        const double *cam, double inv_sq_thr, int loss, double thr, bool weighted,
+                        double *scratch, double *out) {
     double R[9];
     quat_to_rotmat(q, R);
     const float r00 = (float)R[0], r01 = (float)R[1], r02 = (float)R[2], r10 = (float)R[3], r11 = (float)R[4],
@@ -1192,13 +1200,34 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
         const double r0 = (cam[0] * z0d + cam[2]) - P.lx64[2 * o];
         const double r1 = (cam[1] * z1d + cam[3]) - P.lx64[2 * o + 1];
         const double r_squared = r0 * r0 + r1 * r1;
-        cost += valid ? log1p(r_squared * inv_sq_thr) : 0.0;
         // FP32 Jacobian from the FP64 projection and residual.
         const float iz = (float)inv_z, z0 = (float)z0d, z1 = (float)z1d;
         const float rx = (float)r0, ry = (float)r1;
         const float r2 = (float)r_squared;
-        float wgt = isq / (1.0f + r2 * isq);
-        wgt = fmaxf(wgt, FLT_MIN);
+        float wgt;
+        double lc;
+        if (loss == kLossCauchy) {  // CauchyLoss_cuda, robust_loss.cuh:24-38
+            lc = log1p(r_squared * inv_sq_thr);
+            wgt = fmaxf(isq / (1.0f + r2 * isq), FLT_MIN);
+        } else {
+            const double sq = thr * thr;
+            if (loss == kLossTruncated) {  // TruncatedLoss_cuda, robust_loss.cuh:10-22
+                lc = fmin(r_squared, sq);
+                wgt = r_squared < sq ? 1.0f : 0.0f;
+            } else if (loss == kLossHuber) {
+                lc = r_squared <= sq ? r_squared : 2.0 * thr * sqrt(r_squared) - sq;
+                wgt = r_squared <= sq ? 1.0f : (float)(thr / sqrt(r_squared));
+            } else {
+                lc = r_squared;
+                wgt = 1.0f;
+            }
+        }
+        if (weighted) {
+            const double m = P.lw64[o];
+            lc *= m;
+            wgt *= (float)m;
+        }
+        cost += valid ? lc : 0.0;
         const float wv = valid ? wgt : 0.0f;
         const float a0 = fx * iz, a2 = -fx * z0 * iz;
         const float b1 = fy * iz, b2 = -fy * z1 * iz;
@@ -1318,7 +1347,8 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
         for (int k = 0; k < 3; ++k) pt[k] = res.t[k];
     }
     __syncthreads();
-    if (max_it > 0) lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, scratch, part);
+    if (max_it > 0)
+        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch, part);
     else if (threadIdx.x < kLMSums) part[threadIdx.x] = 0.0;
     __syncthreads();
     cluster_totals();
@@ -1375,7 +1405,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
         }
         __syncthreads();
         if (pbrk) break;
-        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, scratch, part);
+        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch, part);
         __syncthreads();
         cluster_totals();
         if (rank == 0 && threadIdx.x == 0) {
