@@ -552,6 +552,21 @@ def main():
     h2d = sum(40 * f.n for f in frames)
     d2h = args.frames * 264
 
+    # Device-resident correspondences (e.g. a GPU matcher's output): the public
+    # device call per step, results to the host.
+    from turboransac_b200 import DeviceFrame, estimate_batch_device
+    dframes = [DeviceFrame(f, device=dev) for f in frames]
+    torch.cuda.synchronize()
+    dev_t = []
+    for i in range(1 + max(1, args.steps // 2)):
+        t0 = time.perf_counter()
+        estimate_batch_device(ctx, dframes, ro)
+        dt = time.perf_counter() - t0
+        if i:
+            dev_t.append(dt)
+    e2e_device_fps = world * args.frames * len(dev_t) / max_over_ranks(pg, sum(dev_t), dev)
+    del dframes
+
     # Plain per-frame calls (the reference's calling pattern) on the same frames.
     plain = None
     if not args.no_plain:
@@ -600,6 +615,9 @@ def main():
             "kernels_ms_per_batch": {k: v[0] for k, v in prof.items()},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e_device_inputs": {"value": e2e_device_fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": d2h,
+                                  "inputs": "correspondences already in device memory (CUDA tensors)"},
             "plain_call": plain,
             "serving": serving,
             "speedup_vs_plain": (value / plain["frames_per_s"]) if plain else None,

@@ -199,6 +199,17 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
                               const tbr_ext_options *ext, tbr_frame_result *results,
                               uint8_t *const *inliers /* n_frames pointers, NULL entries ok */);
 
+/* Correspondences already in device memory (no reference counterpart): as
+ * tbr_estimate_batch, but each frame's points2D / points3D are device pointers
+ * on the context's GPU -- e.g. a GPU feature matcher's output -- and are copied
+ * device-to-device into the workspace, with no host staging. When stream (a
+ * cudaStream_t) is not NULL the copy waits for the work queued on it so far;
+ * with NULL the caller guarantees the data is ready. Results and inlier masks
+ * are written to host memory. */
+tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                     void *stream, tbr_frame_result *results, uint8_t *const *inliers);
+
 /* Device-resident batch: upload once (host->device), run many times with the
  * inputs already in HBM, download results. run() launches the captured graph
  * on the context stream; it is what the throughput measurement times. */

@@ -134,3 +134,37 @@ def test_autotune_keeps_results(ctx):
         assert r1["samples"] == r0["samples"] and r1["best_sample"] == r0["best_sample"]
         assert r1["num_inliers"] == r0["num_inliers"]
         assert quat_angle(r1["q"], r0["q"]) < 1e-12 and np.abs(r1["t"] - r0["t"]).max() < 1e-12
+
+
+def test_device_resident_inputs_match_host_inputs(ctx):
+    """tbr_estimate_batch_device: correspondences handed over as CUDA tensors
+    give the host call's results."""
+    import torch
+
+    from turboransac_b200 import DeviceFrame, estimate_batch_device
+    fr = mixed_frames()
+    host = estimate_batch(ctx, fr, RO)
+    dev_frames = [DeviceFrame(f) for f in fr]
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got = estimate_batch_device(ctx, dev_frames, RO)
+        for a, b in zip(got, host):
+            assert a["status"] == 0
+            assert a["samples"] == b["samples"] and a["best_sample"] == b["best_sample"]
+            assert a["num_inliers"] == b["num_inliers"]
+            assert quat_angle(a["q"], b["q"]) < 1e-12 and np.abs(a["t"] - b["t"]).max() < 1e-12
+    # host pointers are refused, not read as device memory
+    import ctypes as C
+
+    from turboransac_b200 import _lib
+    arr = (_lib.FrameDescC * 1)()
+    f = fr[0]
+    arr[0].points2D = f.uv.ctypes.data
+    arr[0].points3D = f.xyz.ctypes.data
+    arr[0].n = f.n
+    for k in range(4):
+        arr[0].K[k] = float(f.K[k])
+    res = (_lib.FrameResultC * 1)()
+    ro = RO.to_c()
+    st = _lib.lib().tbr_estimate_batch_device(ctx.handle, arr, 1, C.byref(ro), None, None, res, None)
+    assert st != 0

@@ -108,7 +108,7 @@ _lib = None
 # Every entry point declared in include/tbr.h.
 EXPORTS = [
     "tbr_abi_version", "tbr_last_error", "tbr_default_ransac_options", "tbr_default_bundle_options",
-    "tbr_context_create", "tbr_context_destroy", "tbr_estimate_absolute_pose", "tbr_get_inliers",
+    "tbr_context_create", "tbr_context_destroy", "tbr_estimate_absolute_pose", "tbr_get_inliers", "tbr_estimate_batch_device",
     "tbr_bundle_adjust", "tbr_estimate_batch", "tbr_batch_create", "tbr_batch_run", "tbr_batch_sync",
     "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_batch_autotune", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
     "tbr_server_submit_nocopy", "tbr_server_get_stats", "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
@@ -139,6 +139,8 @@ def lib() -> C.CDLL:
                                     C.POINTER(ExtOptionsC), C.POINTER(StatsC)]
     L.tbr_estimate_batch.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32, C.POINTER(RansacOptionsC),
                                      C.POINTER(ExtOptionsC), C.POINTER(FrameResultC), vp]
+    L.tbr_estimate_batch_device.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32, C.POINTER(RansacOptionsC),
+                                            C.POINTER(ExtOptionsC), vp, C.POINTER(FrameResultC), vp]
     L.tbr_batch_create.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32, C.POINTER(RansacOptionsC),
                                    C.POINTER(ExtOptionsC), C.POINTER(vp)]
     L.tbr_batch_run.argtypes = [vp]

@@ -401,6 +401,51 @@ def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None =
     return out
 
 
+def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None):
+    """Frames whose correspondences are already on the context's GPU
+    (tbr_estimate_batch_device). Each frame has `uv` (n, 2) and `xyz` (n, 3)
+    float64 contiguous CUDA tensors (or objects with data_ptr()), `K` and
+    `seed`. `stream`: a torch.cuda.Stream (default: torch's current stream) whose
+    queued work the copy waits for. Results come back to the host."""
+    import torch
+    arr = (_lib.FrameDescC * len(frames))()
+    for i, fr in enumerate(frames):
+        for name, cols in (("uv", 2), ("xyz", 3)):
+            tt = getattr(fr, name)
+            if not (tt.is_cuda and tt.dtype == torch.float64 and tt.is_contiguous() and tt.dim() == 2
+                    and tt.shape[1] == cols):
+                raise ValueError(f"frame {i}: {name} must be a contiguous float64 CUDA tensor (n, {cols})")
+        if fr.uv.shape[0] != fr.xyz.shape[0]:
+            raise ValueError(f"frame {i}: 2D and 3D point counts differ")
+        arr[i].points2D = fr.uv.data_ptr()
+        arr[i].points3D = fr.xyz.data_ptr()
+        arr[i].n = fr.uv.shape[0]
+        for k in range(4):
+            arr[i].K[k] = float(fr.K[k])
+        arr[i].seed = int(fr.seed) & 0xFFFFFFFFFFFFFFFF
+        arr[i].max_reproj_error = 0.0
+    ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+    ext = _lib.ExtOptionsC()
+    res = (_lib.FrameResultC * len(frames))()
+    st = stream if stream is not None else torch.cuda.current_stream()
+    with ctx._lock:
+        check(_lib.lib().tbr_estimate_batch_device(ctx.handle, arr, len(frames), C.byref(ro), C.byref(ext),
+                                                   C.c_void_p(st.cuda_stream), res, None))
+    return _results(res, len(frames))
+
+
+class DeviceFrame:
+    """A frame's correspondences as CUDA tensors (for estimate_batch_device)."""
+
+    def __init__(self, frame, device="cuda"):
+        import torch
+        self.uv = torch.as_tensor(np.ascontiguousarray(frame.uv, np.float64), device=device)
+        self.xyz = torch.as_tensor(np.ascontiguousarray(frame.xyz, np.float64), device=device)
+        self.K = tuple(float(k) for k in frame.K)
+        self.seed = frame.seed
+        self.n = int(self.uv.shape[0])
+
+
 class Server:
     """Continuous-batching request loop (tbr_server_*): submit frames any time;
     a worker advances every resident frame one engine step at a time and admits

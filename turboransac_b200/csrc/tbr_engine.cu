@@ -171,6 +171,8 @@ class Engine {
     int32_t *d_active = nullptr;
     FrameDev *d_admit = nullptr;         // admission staging (device side)
     FrameResult *d_res_stage = nullptr;  // packed results of one download
+    IngestDesc *d_ingest = nullptr;      // device-resident inputs of one admission
+    cudaEvent_t ev_ingest = nullptr;     // the caller's stream, waited on before ingestion
     int32_t *d_res_slots = nullptr;      // slot list of that download
     int32_t *d_replay = nullptr;
     int64_t d_replay_cap = 0;
@@ -192,6 +194,7 @@ class Engine {
         if (ev1) cudaEventDestroy(ev1);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_ingest) cudaEventDestroy(ev_ingest);
         if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -206,6 +209,7 @@ class Engine {
         TBR_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_ingest, cudaEventDisableTiming));
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
         // Split: 30 % hypotheses, the rest points, after the per-frame state.
@@ -233,6 +237,7 @@ class Engine {
         add((void **)&d_active, sizeof(int32_t) * kMaxActive);
         add((void **)&d_admit, sizeof(FrameDev) * kMaxActive);
         add((void **)&d_res_stage, sizeof(FrameResult) * kMaxActive);
+        add((void **)&d_ingest, sizeof(IngestDesc) * kMaxActive);
         add((void **)&d_res_slots, sizeof(int32_t) * kMaxActive);
         add((void **)&P.uv64, 16 * np);
         add((void **)&P.X64, 24 * np);
@@ -626,7 +631,7 @@ static size_t stage_bytes(const std::vector<FrameHost> &fr) {
 // `stage` holds at least stage_bytes(fr) bytes of pinned memory that no copy in
 // flight reads. With copy = false the host copies are left in A.jobs.
 static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o, char *stage,
-                               StagedAdmission &A, bool copy = true) {
+                               StagedAdmission &A, bool copy = true, bool host_points = true) {
     if ((int)fr.size() > (int)E.free_slots.size()) return fail(TBR_ERR_CAPACITY, "too many frames for the context");
     auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     int64_t replay_total = 0;
@@ -659,6 +664,16 @@ static tbr_status stage_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         }
         A.devs.push_back(E.make_frame(f, off, o, d_rep));
         A.max_n = std::max(A.max_n, f.n);
+    }
+    if (!host_points) {  // records only: the points come from device memory
+        auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+        A.hd = (FrameDev *)stage;
+        A.ha = (int32_t *)(stage + r256(sizeof(FrameDev) * fr.size()));
+        for (size_t i = 0; i < fr.size(); ++i) {
+            A.hd[i] = A.devs[i];
+            A.ha[i] = A.slots[i];
+        }
+        return TBR_OK;
     }
     // Runs of adjacent frames.
     auto &span = A.span;
@@ -799,15 +814,31 @@ static tbr_status copy_and_upload_overlapped(Engine &E, const StagedAdmission &A
     return upload_records(E, A);
 }
 
-// Both halves through the context's own staging buffer.
+// Both halves through the context's own staging buffer. With device_points the
+// frames' point arrays are device memory of this GPU: they are copied into the
+// pool by one kernel, with no host staging.
 static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
-                               std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr) {
-    tbr_status st = E.ensure_stage(stage_bytes(fr));
+                               std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr,
+                               bool device_points = false) {
+    auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t rec = r256(sizeof(FrameDev) * fr.size()) + r256(4 * fr.size());
+    tbr_status st = E.ensure_stage(device_points ? rec + r256(sizeof(IngestDesc) * fr.size()) + 256
+                                                 : stage_bytes(fr));
     if (st) return st;
     StagedAdmission A;
-    st = stage_frames(E, fr, o, (char *)E.h_stage, A, false);
+    st = stage_frames(E, fr, o, (char *)E.h_stage, A, false, !device_points);
     if (st) return st;
-    st = copy_and_upload_overlapped(E, A);
+    if (device_points) {
+        IngestDesc *hi = (IngestDesc *)((char *)E.h_stage + rec);
+        for (size_t i = 0; i < fr.size(); ++i) hi[i] = {fr[i].uv, fr[i].xyz, fr[i].n, A.devs[i].blk_off * kSub};
+        TBR_CUDA(cudaMemcpyAsync(E.d_ingest, hi, sizeof(IngestDesc) * fr.size(), cudaMemcpyHostToDevice, E.stream));
+        const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (A.max_n + 1023) / 1024));
+        k_ingest<<<dim3(bx, (unsigned)fr.size()), 256, 0, E.stream>>>(E.d_ingest, E.P);
+        TBR_CUDA(cudaGetLastError());
+        st = upload_records(E, A);
+    } else {
+        st = copy_and_upload_overlapped(E, A);
+    }
     if (st) return st;
     slots = A.slots;
     max_n = A.max_n;
@@ -916,14 +947,14 @@ void tbr_context_destroy(tbr_context *ctx) { delete ctx; }
 
 static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
                                   std::vector<FrameResult> &res, std::vector<uint8_t *> masks,
-                                  float *ms_out, int *steps_out) {
+                                  float *ms_out, int *steps_out, bool device_points = false) {
     Engine &E = ctx->E;
     std::vector<int> slots;
     std::vector<FrameDev> devs;
     int64_t max_n = 0;
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
-    tbr_status st = admit_frames(E, fr, o, slots, max_n, &devs);
+    tbr_status st = admit_frames(E, fr, o, slots, max_n, &devs, device_points);
     if (st) return st;
     TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
     E.launch_prep((int)slots.size(), max_n);
@@ -1020,6 +1051,56 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
     float ms = 0.f;
     int steps = 0;
     tbr_status st = estimate_frames(ctx, fr, o, res, masks, &ms, &steps);
+    if (st) return st;
+    for (int i = 0; i < n_frames; ++i) {
+        for (int k = 0; k < 4; ++k) results[i].q[k] = res[i].q[k];
+        for (int k = 0; k < 3; ++k) results[i].t[k] = res[i].t[k];
+        results[i].status = TBR_OK;
+        fill_stats(res[i], fr[i].n, &results[i].stats, ms);
+    }
+    return TBR_OK;
+}
+
+tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                     void *stream, tbr_frame_result *results, uint8_t *const *inliers) {
+    if (!ctx || !frames || n_frames < 1 || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations must be >= 1");
+    RunOptions o = make_run_options(&ro, nullptr, ext);
+    Engine &E = ctx->E;
+    std::vector<FrameHost> fr;
+    for (int i = 0; i < n_frames; ++i) {
+        const tbr_frame_desc &d = frames[i];
+        if (d.n < 3 || !d.points2D || !d.points3D || !(d.K[0] > 0) || !(d.K[1] > 0))
+            return fail(TBR_ERR_INVALID_ARG, "bad frame");
+        for (const void *p : {(const void *)d.points2D, (const void *)d.points3D}) {
+            cudaPointerAttributes a;
+            if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory");
+            }
+            if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != E.device)
+                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory of the context's GPU");
+        }
+        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
+                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+    }
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    if (stream) {  // the producer's pending writes come first
+        TBR_CUDA(cudaEventRecord(E.ev_ingest, (cudaStream_t)stream));
+        TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_ingest, 0));
+    }
+    std::vector<FrameResult> res;
+    std::vector<uint8_t *> masks(n_frames, nullptr);
+    if (inliers)
+        for (int i = 0; i < n_frames; ++i) masks[i] = inliers[i];
+    float ms = 0.f;
+    int steps = 0;
+    tbr_status st = estimate_frames(ctx, fr, o, res, masks, &ms, &steps, true);
     if (st) return st;
     for (int i = 0; i < n_frames; ++i) {
         for (int k = 0; k < 4; ++k) results[i].q[k] = res[i].q[k];

@@ -1501,6 +1501,24 @@ __global__ void k_reset_frames(Pools P, const FrameDev *init) {
     if (a == 0 && threadIdx.x < kCNum) P.counters[threadIdx.x] = 0;
 }
 
+// Device-resident input: one frame's correspondences, copied into the pool.
+struct IngestDesc {
+    const double *uv, *xyz;
+    int64_t n, dst;  // points; first pool point of the frame
+};
+__global__ void k_ingest(const IngestDesc *d, Pools P) {
+    const IngestDesc g = d[blockIdx.y];
+    double *uv = const_cast<double *>(P.uv64), *X = const_cast<double *>(P.X64);  // the pool's input arrays
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t o = g.dst + i;
+        uv[2 * o] = g.uv[2 * i];
+        uv[2 * o + 1] = g.uv[2 * i + 1];
+        X[3 * o] = g.xyz[3 * i];
+        X[3 * o + 1] = g.xyz[3 * i + 1];
+        X[3 * o + 2] = g.xyz[3 * i + 2];
+    }
+}
+
 // Autotuner: the scoring shape of a batch's initial frame records.
 __global__ void k_set_shape(FrameDev *init, int n, int hr, int chunk_points) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
