@@ -65,7 +65,7 @@ def dist_setup(args):
         backend = "nccl"
         import torch
         torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
