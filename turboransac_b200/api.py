@@ -292,30 +292,44 @@ def bundle_adjust_cuda(x, X, camera: Camera_cuda, pose: CameraPose_cuda, opt: Bu
     return default_context().bundle_adjust(x, X, camera, pose, opt, weights)[0]
 
 
+_DESC_DTYPE = np.dtype(_lib.FrameDescC)
+_RESULT_DTYPE = np.dtype(_lib.FrameResultC)
+
+
+def _f64c(a):
+    return a if (a.dtype == np.float64 and a.flags.c_contiguous) else np.ascontiguousarray(a, np.float64)
+
+
 def _frame_descs(frames, seeds=None, max_reproj_error=0.0):
-    """Build tbr_frame_desc entries (keeps references to the float64 arrays)."""
+    """tbr_frame_desc entries for the frames' float64 arrays: (pointer for the C
+    call, objects to keep alive until it returns)."""
     keep = []
-    arr = (_lib.FrameDescC * len(frames))()
-    for i, fr in enumerate(frames):
-        uv = np.ascontiguousarray(fr.uv, np.float64)
-        X = np.ascontiguousarray(fr.xyz, np.float64)
+    p2, p3 = [], []
+    for fr in frames:
+        uv, X = _f64c(fr.uv), _f64c(fr.xyz)
         keep += [uv, X]
-        arr[i].points2D = uv.ctypes.data
-        arr[i].points3D = X.ctypes.data
-        arr[i].n = uv.shape[0]
-        for k in range(4):
-            arr[i].K[k] = float(fr.K[k])
-        arr[i].seed = (fr.seed if seeds is None else seeds[i]) & 0xFFFFFFFFFFFFFFFF
-        arr[i].max_reproj_error = max_reproj_error or getattr(fr, "threshold_px", 0.0)
-    return arr, keep
+        p2.append(uv.__array_interface__["data"][0])
+        p3.append(X.__array_interface__["data"][0])
+    a = np.zeros(len(frames), _DESC_DTYPE)
+    a["points2D"] = p2
+    a["points3D"] = p3
+    a["n"] = [k.shape[0] for k in keep[0::2]]
+    a["K"] = np.array([[float(k) for k in fr.K] for fr in frames], np.float64)
+    a["seed"] = np.array([(fr.seed if seeds is None else seeds[i]) & 0xFFFFFFFFFFFFFFFF
+                          for i, fr in enumerate(frames)], np.uint64)
+    a["max_reproj_error"] = [max_reproj_error or getattr(fr, "threshold_px", 0.0) for fr in frames]
+    keep.append(a)
+    return a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), keep
 
 
 def _results(res, n):
-    out = []
-    for i in range(n):
-        r = res[i]
-        out.append({"q": np.array(r.q[:]), "t": np.array(r.t[:]), "status": r.status, **r.stats.as_dict()})
-    return out
+    a = np.frombuffer(res, dtype=_RESULT_DTYPE, count=n)
+    q, t, status = a["q"].copy(), a["t"].copy(), a["status"].tolist()
+    stats = a["stats"]
+    names = stats.dtype.names
+    cols = [stats[k].tolist() for k in names]
+    return [{"q": q[i], "t": t[i], "status": status[i], **dict(zip(names, (c[i] for c in cols)))}
+            for i in range(n)]
 
 
 class Batch:
