@@ -85,8 +85,10 @@ typedef struct tbr_ext_options {
     /* 0 (default): the reference's hard-coded choices -- success_prob 0.9999,
      * trials multiplier 3, 100000-sample cap, default BundleOptions with a
      * 1/f loss scale (turbo_ransac.cu:145,227,231; entry.cu:122-123).
-     * 1: honour success_prob, dyn_num_trials_mult, min_iterations and the
-     * caller's bundle options; in tbr_bundle_adjust also the loss type
+     * 1: honour success_prob, dyn_num_trials_mult, min_iterations,
+     * progressive_sampling / max_prosac_iterations (PROSAC over points sorted
+     * by decreasing quality) and the caller's bundle options; in
+     * tbr_bundle_adjust also the loss type
      * (TRIVIAL, TRUNCATED, HUBER, CAUCHY) and the per-point weights, which
      * the reference ignores (ba.cu:111-130). */
     int32_t honor_options;

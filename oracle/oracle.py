@@ -44,7 +44,8 @@ class RansacCfg(C.Structure):
                 ("success_prob", C.c_double), ("trials_mult", C.c_double),
                 ("force_samples", C.c_int64), ("seed", C.c_uint64),
                 ("replay", C.c_void_p), ("replay_count", C.c_int64), ("threads", C.c_int),
-                ("quirk", C.c_int), ("min_samples", C.c_int64)]
+                ("quirk", C.c_int), ("min_samples", C.c_int64), ("prosac", C.c_int32),
+                ("prosac_TN", C.c_double)]
 
 
 class RansacOut(C.Structure):
@@ -71,10 +72,13 @@ class EstimateInfo(C.Structure):
 
 
 def _cfg(samples_per_round=1000, seed=0, force_samples=0, replay=None, threads=1,
-         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0, quirk=False, min_samples=0):
+         max_total_samples=100000, success_prob=0.9999, trials_mult=3.0, quirk=False, min_samples=0,
+         prosac=False, prosac_TN=100000.0):
     cfg = RansacCfg()
     cfg.quirk = int(quirk)
     cfg.min_samples = min_samples
+    cfg.prosac = int(prosac)
+    cfg.prosac_TN = float(prosac_TN)
     cfg.samples_per_round = samples_per_round
     cfg.max_total_samples = max_total_samples
     cfg.success_prob = success_prob
@@ -116,6 +120,8 @@ class Oracle:
         L.orc_estimate_batch.argtypes = [_dp, _dp, _ip64, _dp, _u64p, C.c_int, C.c_double,
                                          C.c_int64, C.c_int, _dp, _dp, _ip64]
         L.orc_estimate_batch.restype = C.c_int
+        L.orc_prosac_table.argtypes = [C.c_int64, C.c_double, _ip64]
+        L.orc_prosac_triple.argtypes = [C.c_uint64, C.c_int64, C.c_int64, _ip64, _ip32]
 
     # -- pieces -------------------------------------------------------------
     def philox(self, ctr, key):
@@ -128,6 +134,18 @@ class Oracle:
     def sample_triples(self, seed: int, first: int, count: int, n: int) -> np.ndarray:
         out = np.empty((count, 3), dtype=np.int32)
         self.lib.orc_sample_triples(seed & 0xFFFFFFFFFFFFFFFF, first, count, n, out)
+        return out
+
+    def prosac_table(self, n: int, TN: float = 100000.0) -> np.ndarray:
+        out = np.zeros(n - 2, np.int64)
+        self.lib.orc_prosac_table(n, TN, out)
+        return out
+
+    def prosac_triples(self, seed: int, first: int, count: int, n: int, TN: float = 100000.0) -> np.ndarray:
+        tp = self.prosac_table(n, TN)
+        out = np.zeros((count, 3), np.int32)
+        for s in range(count):
+            self.lib.orc_prosac_triple(seed & 0xFFFFFFFFFFFFFFFF, first + s, n, tp, out[s])
         return out
 
     def p3p(self, x: np.ndarray, X: np.ndarray) -> np.ndarray:

@@ -751,6 +751,31 @@ void orc_sample_triples(uint64_t seed, int64_t first_sample, int64_t count, int6
         triple_from_sample(seed, (uint64_t)(first_sample + s), (uint32_t)n, idx_out + 3 * s);
 }
 
+void orc_prosac_table(int64_t n, double TN, int64_t *Tp) {
+    auto T = [&](int64_t k) {
+        return ((TN * ((double)k / (double)n)) * ((double)(k - 1) / (double)(n - 1))) *
+               ((double)(k - 2) / (double)(n - 2));
+    };
+    Tp[0] = 1;
+    for (int64_t k = 3; k < n; ++k) Tp[k - 2] = Tp[k - 3] + (int64_t)std::ceil(T(k + 1) - T(k));
+}
+
+void orc_prosac_triple(uint64_t seed, int64_t sample, int64_t n, const int64_t *Tp, int32_t out[3]) {
+    const int64_t t = sample + 1;
+    const int64_t g = std::upper_bound(Tp, Tp + (n - 3), t) - Tp;  // growths so far
+    const int64_t m = 3 + g;
+    if (m >= n && Tp[n - 3] < t) {
+        triple_from_sample(seed, (uint64_t)sample, (uint32_t)n, out);
+        return;
+    }
+    uint32_t c[4] = {(uint32_t)sample, (uint32_t)((uint64_t)sample >> 32), 0u, 0u};
+    philox(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    uint32_t i0 = mulhi_range(c[0], (uint32_t)(m - 1));
+    uint32_t i1 = mulhi_range(c[1], (uint32_t)(m - 2));
+    if (i1 >= i0) ++i1;
+    out[0] = (int32_t)i0; out[1] = (int32_t)i1; out[2] = (int32_t)(m - 1);
+}
+
 int orc_p3p(const double *x, const double *X, double *poses_out) { return p3p_impl(x, X, poses_out); }
 
 void orc_bearing(double x, double y, double out[3]) {
@@ -803,6 +828,7 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
 
     std::vector<SampleResult> res;
     std::vector<int32_t> idx;
+    std::vector<int64_t> prosac_tp;
     int64_t done = 0, nhyp = 0, rounds = 0;
     bool stop = false;
     // Round loop, turbo_ransac.cu:151-259: at least one round, stop once the
@@ -814,6 +840,12 @@ int orc_ransac(const double *xn, const double *X, int64_t n, double sq_thr,
         if (cfg->replay) {
             if (done + cnt > cfg->replay_count) return -2;
             std::memcpy(idx.data(), cfg->replay + 3 * done, sizeof(int32_t) * 3 * cnt);
+        } else if (cfg->prosac) {
+            if (prosac_tp.empty()) {
+                prosac_tp.resize(n - 2);
+                orc_prosac_table(n, cfg->prosac_TN, prosac_tp.data());
+            }
+            for (int64_t s = 0; s < cnt; ++s) orc_prosac_triple(cfg->seed, done + s, n, prosac_tp.data(), &idx[3 * s]);
         } else {
             orc_sample_triples(cfg->seed, done, cnt, n, idx.data());
         }

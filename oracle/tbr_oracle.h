@@ -69,7 +69,20 @@ typedef struct orc_ransac_cfg {
     int threads;                /* worker threads over samples (>=1) */
     int quirk;                  /* 1: stop rule with the x86 int-conversion result (INT_MIN) */
     int64_t min_samples;        /* no stop before this many samples (0: none) */
+    int32_t prosac;             /* 1: PROSAC sampling over points sorted by quality */
+    double prosac_TN;           /* T_N: samples after which PROSAC draws uniformly */
 } orc_ransac_cfg;
+
+/* PROSAC growth table (Chum & Matas, CVPR 2005): Tp[k-3] = T'_k for k = 3..n,
+ * T'_3 = 1, T'_{k+1} = T'_k + ceil(T_{k+1} - T_k), T_k = T_N * C(k,3) / C(n,3)
+ * evaluated as ((T_N * (k/n)) * ((k-1)/(n-1))) * ((k-2)/(n-2)). n-2 entries. */
+void orc_prosac_table(int64_t n, double TN, int64_t *Tp);
+
+/* PROSAC ordered triple of sample `sample` (0-based; iteration t = sample+1):
+ * with g = #{k in 3..n-1 : T'_k <= t} and m = 3 + g, the triple is two
+ * distinct indices of the first m-1 points and point m-1; once m = n and
+ * T'_n < t it is the uniform triple of orc_sample_triples. */
+void orc_prosac_triple(uint64_t seed, int64_t sample, int64_t n, const int64_t *Tp, int32_t out[3]);
 
 typedef struct orc_ransac_out {
     double P[12];          /* best pose, identity if none */

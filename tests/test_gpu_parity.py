@@ -251,3 +251,26 @@ def test_bundle_adjust_honoured_loss_and_weights(ctx, oracle, loss_type):
                                 loss={0: 3, 1: 1, 2: 2, 3: 0}[loss_type], weights=w)
         assert quat_angle(pose.q, oq) < 1e-6, (loss_type, k)
         assert np.abs(pose.t - ot).max() < 1e-6, (loss_type, k)
+
+
+def test_prosac_sampling_matches_oracle(ctx, oracle):
+    """honor_options + progressive_sampling (utils.h:23-25, declared but not
+    implemented by the reference): PROSAC draws over correspondences sorted by
+    quality (here inliers first); samples, selection and pose equal the oracle's."""
+    f = scenes.make_frame(3000, 0.15, 1.0, 5151)
+    order = np.concatenate([np.flatnonzero(f.inlier_gt), np.flatnonzero(~f.inlier_gt)])
+    uv, xyz = f.uv[order].copy(), f.xyz[order].copy()
+    for TN in (100000, 20000):
+        ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0, progressive_sampling=True,
+                                max_prosac_iterations=TN)
+        st, pose, inl = ctx.estimate_absolute_pose(uv, xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                                   honor_options=True)
+        o = oracle.estimate(uv, xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8, prosac=True,
+                            prosac_TN=float(TN))
+        d, info = st.details, o["info"]
+        assert d["samples"] == info.ransac.samples
+        assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+        np.testing.assert_array_equal(inl, o["inliers"])
+        assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+        ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
+        assert ae < 5 and te < 5

@@ -141,3 +141,21 @@ def test_oracle_min_samples_delays_the_stop(oracle):
     b = oracle.ransac(xn, f.xyz, thr, seed=f.seed, min_samples=4000)
     assert a["samples"] < 4000 <= b["samples"]
     assert b["score"] <= a["score"]
+
+
+def test_oracle_prosac_schedule(oracle):
+    """PROSAC growth table and draws (Chum & Matas, CVPR 2005): T' strictly
+    increasing from 1, ending near T_N; every draw before the subset reaches n
+    holds the newest point m-1 and two distinct points below it; afterwards the
+    draws are the uniform ones."""
+    n, TN = 500, 20000.0
+    tp = oracle.prosac_table(n, TN)
+    assert tp[0] == 1 and np.all(np.diff(tp) >= 1)
+    assert TN <= tp[-1] <= TN + n
+    tr = oracle.prosac_triples(11, 0, 3000, n, TN)
+    for s, (a, b, c) in enumerate(tr):
+        t = s + 1
+        m = 3 + int(np.searchsorted(tp[:n - 3], t, side="right"))
+        assert c == m - 1 and a != b and max(a, b) < m - 1
+    late = oracle.prosac_triples(11, int(tp[-1]) + 5, 50, n, TN)
+    np.testing.assert_array_equal(late, oracle.sample_triples(11, int(tp[-1]) + 5, 50, n))

@@ -56,6 +56,35 @@ __host__ __device__ __forceinline__ void draw_triple(uint64_t seed, uint64_t sam
     out[2] = (int32_t)i2;
 }
 
+// PROSAC ordered triple (Chum & Matas, CVPR 2005) of sample `sample` (0-based;
+// iteration t = sample + 1) over points sorted by quality. Tp[k-3] = T'_k for
+// k = 3..n (growth table). With g = #{k in 3..n-1 : T'_k <= t} and m = 3 + g,
+// the triple is two distinct indices of the first m-1 points and point m-1;
+// once m = n and T'_n < t it is the uniform triple of draw_triple.
+__device__ __forceinline__ void prosac_triple(uint64_t seed, uint64_t sample, uint32_t n, const int64_t *Tp,
+                                              int32_t out[3]) {
+    const int64_t t = (int64_t)sample + 1;
+    int64_t lo = 0, hi = (int64_t)n - 3;  // first entry of Tp[0, n-3) above t
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (Tp[mid] <= t) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint32_t m = 3u + (uint32_t)lo;
+    if (m >= n && Tp[n - 3] < t) {
+        draw_triple(seed, sample, n, out);
+        return;
+    }
+    uint32_t c[4] = {(uint32_t)sample, (uint32_t)(sample >> 32), 0u, 0u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    uint32_t i0 = mulhi_range(c[0], m - 1);
+    uint32_t i1 = mulhi_range(c[1], m - 2);
+    if (i1 >= i0) ++i1;
+    out[0] = (int32_t)i0;
+    out[1] = (int32_t)i1;
+    out[2] = (int32_t)(m - 1);
+}
+
 // ------------------------------------------------------------- FP64 math ----
 struct d3 {
     double x, y, z;

@@ -105,6 +105,8 @@ struct RunOptions {
     int64_t max_total = 100000;
     int64_t min_samples = 0;
     int64_t force_samples = 0;
+    int prosac = 0;
+    double prosac_TN = 100000.0;
     double success_prob = 0.9999;
     double trials_mult = 3.0;
     int skip_refine = 0;
@@ -139,6 +141,8 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
         o.success_prob = ro->success_prob;
         o.trials_mult = ro->dyn_num_trials_mult;
         o.min_samples = (int64_t)ro->min_iterations;
+        o.prosac = ro->progressive_sampling ? 1 : 0;
+        if (ro->max_prosac_iterations > 0) o.prosac_TN = (double)ro->max_prosac_iterations;
     }
     if (honor && bo) {
         o.lm_max_iter = (int64_t)bo->max_iterations;
@@ -225,7 +229,7 @@ class Engine {
         P.max_hyps = std::max<int64_t>(P.max_hyps, 4096);
         P.max_parts = P.max_hyps * 32;
         P.max_hb = P.max_hyps / 32 + kMaxActive;
-        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 8) + kBlockBytes;
+        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 8 + 8) + kBlockBytes;
         max_blocks = (int64_t)((rest - (size_t)(P.max_hyps * per_hyp) - P.max_hb * 4) / per_block) - 1;
         if (max_blocks < 64) return fail(TBR_ERR_INVALID_ARG, "workspace too small for points");
         // One allocation, carved with 256-byte alignment.
@@ -246,6 +250,7 @@ class Engine {
         add((void **)&P.lx64, 16 * np);
         add((void **)&P.lX64, 24 * np);
         add((void **)&P.lw64, 8 * np);
+        add((void **)&P.prosac64, 8 * np);
         add((void **)&P.pts32, (size_t)kBlockBytes * max_blocks);
         add((void **)&P.sample_prefix, 8 * (kMaxActive + 1));
         add((void **)&P.item_prefix, 8 * (kMaxActive + 1));
@@ -341,6 +346,8 @@ class Engine {
         f.B = o.B;
         f.max_total = o.max_total;
         f.min_samples = o.min_samples;
+        f.prosac = o.prosac;
+        f.prosac_TN = o.prosac_TN;
         f.force_samples = o.force_samples;
         f.log_missing = std::log(1.0 - o.success_prob);
         f.trials_mult = o.trials_mult;
@@ -422,6 +429,7 @@ class Engine {
         const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024));
         k_prep_bounds<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
         k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
+        k_prosac_table<<<n_active, 1024, 0, stream>>>(Q);
     }
     void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n); }
 

@@ -89,6 +89,9 @@ struct __align__(16) FrameDev {
     int64_t B;
     int64_t max_total;
     int64_t min_samples;  // no stop before this many samples (honoured min_iterations; else 0)
+    double prosac_TN;     // PROSAC: samples after which it draws uniformly
+    int32_t prosac;       // 1: PROSAC sampling (honoured progressive_sampling), table in Pools::prosac64
+    int32_t prosac_pad;
     int64_t force_samples;
     double log_missing, trials_mult;
     int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass (2 * HP)
@@ -138,6 +141,7 @@ struct Pools {
     double *lx64;        // LM: pixels / f (2/pt)
     double *lX64;        // LM: world points (3/pt)
     double *lw64;        // LM: per-point loss multipliers (bundle adjust with honoured weights)
+    int64_t *prosac64;   // PROSAC growth table of a frame, one entry per point (T'_k at k - 3)
     float2 *pts32;       // staging blocks: [X|Y|Z|-x/tau|-y/tau] x kSub, each value duplicated
     // step prefixes (n_active + 1)
     int64_t *sample_prefix;
@@ -322,6 +326,37 @@ __global__ void k_prep_pack(Pools P) {
     }
 }
 
+// PROSAC growth table of each PROSAC frame (one CTA per frame):
+// T'_3 = 1, T'_{k+1} = T'_k + ceil(T_{k+1} - T_k), T_k = T_N C(k,3) / C(n,3)
+// evaluated as ((T_N * (k/n)) * ((k-1)/(n-1))) * ((k-2)/(n-2)) with rounded
+// operations only (no contraction), so the table is the oracle's bit for bit.
+__device__ __forceinline__ double prosac_T(double TN, int64_t k, int64_t n) {
+    const double a = __ddiv_rn((double)k, (double)n), b = __ddiv_rn((double)(k - 1), (double)(n - 1)),
+                 c = __ddiv_rn((double)(k - 2), (double)(n - 2));
+    return __dmul_rn(__dmul_rn(__dmul_rn(TN, a), b), c);
+}
+__global__ void __launch_bounds__(1024) k_prosac_table(Pools P) {
+    __shared__ int64_t sh[33];
+    const int a = blockIdx.x;
+    if (a >= P.n_active) return;
+    const FrameDev &f = P.frames[P.active[a]];
+    if (!f.prosac) return;
+    const int64_t n = f.n, cnt = n - 3;  // increments for k = 3 .. n-1
+    int64_t *Tp = P.prosac64 + f.blk_off * kSub;
+    const int64_t per = (cnt + blockDim.x - 1) / blockDim.x;
+    const int64_t k0 = 3 + (int64_t)threadIdx.x * per, k1 = min(k0 + per, (int64_t)n);
+    int64_t local = 0;
+    for (int64_t k = k0; k < k1; ++k)
+        local += (int64_t)ceil(__dsub_rn(prosac_T(f.prosac_TN, k + 1, n), prosac_T(f.prosac_TN, k, n)));
+    int64_t tot;
+    int64_t run = 1 + block_exclusive_scan(local, sh, tot);
+    if (threadIdx.x == 0) Tp[0] = 1;
+    for (int64_t k = k0; k < k1; ++k) {
+        run += (int64_t)ceil(__dsub_rn(prosac_T(f.prosac_TN, k + 1, n), prosac_T(f.prosac_TN, k, n)));
+        Tp[k - 2] = run;
+    }
+}
+
 // ---------------------------------------------------------------- plan -----
 // Rounds per frame for this step. The first step runs one round; later steps
 // run exactly the rounds the current best's inlier ratio still requires under
@@ -427,6 +462,8 @@ __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
                 idx[0] = f.replay[3 * s];
                 idx[1] = f.replay[3 * s + 1];
                 idx[2] = f.replay[3 * s + 2];
+            } else if (f.prosac) {
+                prosac_triple(f.seed, (uint64_t)s, (uint32_t)f.n, P.prosac64 + f.blk_off * kSub, idx);
             } else {
                 draw_triple(f.seed, (uint64_t)s, (uint32_t)f.n, idx);
             }
