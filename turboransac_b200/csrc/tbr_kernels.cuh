@@ -26,6 +26,7 @@ namespace tbr {
 constexpr int kSub = 64;                          // points per FP32 staging block
 // Depth floor of the FP32 filter: the reciprocal of any smaller depth is 2^100.
 constexpr float kDepthFloor = 0x1p-100f;
+constexpr int kRescoreGroup = 8;  // FP64 re-rank: candidates of a frame scored together per point chunk
 constexpr int kBlockFloat2 = kSub * 5;            // float2 entries per block
 constexpr uint32_t kBlockBytes = kBlockFloat2 * 8;  // 2560 B per block
 constexpr int kMaxRoundsPerStep = 128;
@@ -908,7 +909,7 @@ __global__ void k_rescore_plan(Pools P) {
             const int nrc = (int)(want < kMaxRChunks ? want : kMaxRChunks);
             f.n_rchunks = nrc;
             f.rchunk = (f.n + nrc - 1) / nrc;
-            items = (int64_t)f.cand_count * nrc;
+            items = (int64_t)((f.cand_count + kRescoreGroup - 1) / kRescoreGroup) * nrc;
             for (int c = 0; c < f.cand_count; ++c) P.c_arrive[f.cand_base + c] = 0;
         }
     }
@@ -921,83 +922,104 @@ __global__ void k_rescore_plan(Pools P) {
     }
 }
 
-// Exact FP64 truncated MSAC of one candidate over one point chunk, with the
-// per-point formula of msac.cuh:18-56 (reciprocal of the depth, then
-// products); the last chunk to finish sums the partials in chunk order and adds
+// Exact FP64 truncated MSAC of a group of up to kRescoreGroup candidates of a
+// frame over one point chunk (the chunk's points are read once for the group),
+// with the per-point formula of msac.cuh:18-56 (reciprocal of the depth, then
+// products). Every candidate's sum has the same fixed order whatever the
+// grouping: per thread the strided points, then the warp tree, the warps in
+// order, and the chunks in order by the last chunk to finish, which adds
 // (n - count) * tau^2 (ransac.cuh:322).
 __global__ void __launch_bounds__(256) k_rescore(Pools P) {
-    __shared__ double ss[8];
-    __shared__ int sc[8];
+    constexpr int G = kRescoreGroup;
+    __shared__ double ss[8][G];
+    __shared__ int sc[8][G];
+    __shared__ double sM[G][12];
     __shared__ int64_t s_item;
-    __shared__ unsigned s_prev;
+    __shared__ unsigned s_prev[G];
     const int64_t total = (int64_t)P.counters[kCRescoreTotal];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (;;) {
         if (threadIdx.x == 0) s_item = (int64_t)atomicAdd(&P.counters[kCRescoreNext], 1ull);
         __syncthreads();
         const int64_t item = s_item;
-        __syncthreads();
         if (item >= total) break;
         const int a = find_segment(P.ritem_prefix, P.n_active, item);
         const int slot = P.active[a];
         const FrameDev &f = P.frames[slot];
         const int64_t local = item - P.ritem_prefix[a];
-        const int ci = (int)(local / f.n_rchunks), ch = (int)(local % f.n_rchunks);
-        const int64_t cs = f.cand_base + ci;
-        const int h = P.cHyp[cs];
-        const double *Pp = P.hP64 + 12 * (f.hyp_base + h);
-        double M[12];
-#pragma unroll
-        for (int e = 0; e < 12; ++e) M[e] = Pp[e];
+        const int gi = (int)(local / f.n_rchunks), ch = (int)(local % f.n_rchunks);
+        const int c0 = gi * G, ng = min(G, f.cand_count - c0);
+        if (threadIdx.x < G * 12) {
+            const int g = threadIdx.x / 12, e = threadIdx.x % 12;
+            sM[g][e] = g < ng ? P.hP64[12 * (f.hyp_base + P.cHyp[f.cand_base + c0 + g]) + e] : 0.0;
+        }
+        __syncthreads();
         const int64_t base = f.blk_off * kSub;
         const int64_t p0 = (int64_t)ch * f.rchunk, p1 = (f.n < p0 + f.rchunk ? f.n : p0 + f.rchunk);
-        double s = 0.0;
-        int cnt = 0;
+        double s[G];
+        int cnt[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            s[g] = 0.0;
+            cnt[g] = 0;
+        }
         const double sq = f.sq_thr;
         for (int64_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
             const int64_t p = base + i;
             const double X0 = P.X64[3 * p], X1 = P.X64[3 * p + 1], X2 = P.X64[3 * p + 2];
-            const double z0 = M[0] * X0 + M[1] * X1 + M[2] * X2 + M[3];
-            const double z1 = M[4] * X0 + M[5] * X1 + M[6] * X2 + M[7];
-            const double z2 = M[8] * X0 + M[9] * X1 + M[10] * X2 + M[11];
-            const double inv_z2 = 1.0 / z2;
-            const double r0 = z0 * inv_z2 - P.xn64[2 * p];
-            const double r1 = z1 * inv_z2 - P.xn64[2 * p + 1];
-            const double r_sq = r0 * r0 + r1 * r1;
-            if (r_sq < sq && z2 > 0.0) {
-                s += r_sq;
-                ++cnt;
+            const double x0 = P.xn64[2 * p], x1 = P.xn64[2 * p + 1];
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+                if (g < ng) {
+                    const double *M = sM[g];
+                    const double z0 = M[0] * X0 + M[1] * X1 + M[2] * X2 + M[3];
+                    const double z1 = M[4] * X0 + M[5] * X1 + M[6] * X2 + M[7];
+                    const double z2 = M[8] * X0 + M[9] * X1 + M[10] * X2 + M[11];
+                    const double inv_z2 = 1.0 / z2;
+                    const double r0 = z0 * inv_z2 - x0;
+                    const double r1 = z1 * inv_z2 - x1;
+                    const double r_sq = r0 * r0 + r1 * r1;
+                    if (r_sq < sq && z2 > 0.0) {
+                        s[g] += r_sq;
+                        ++cnt[g];
+                    }
+                }
             }
         }
-        s = warp_sum(s);
-        cnt = warp_sum(cnt);
-        if ((threadIdx.x & 31) == 0) {
-            ss[threadIdx.x >> 5] = s;
-            sc[threadIdx.x >> 5] = cnt;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+            const double sw = warp_sum(s[g]);
+            const int cw = warp_sum(cnt[g]);
+            if (lane == 0) {
+                ss[warp][g] = sw;
+                sc[warp][g] = cw;
+            }
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (threadIdx.x < ng) {
+            const int g = threadIdx.x;
+            const int64_t cs = f.cand_base + c0 + g;
             double S = 0.0;
             int C = 0;
             for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-                S += ss[k];
-                C += sc[k];
+                S += ss[k][g];
+                C += sc[k][g];
             }
             P.cpS[cs * kMaxRChunks + ch] = S;
             P.cpC[cs * kMaxRChunks + ch] = C;
             __threadfence();
-            s_prev = atomicAdd(&P.c_arrive[cs], 1u);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0 && s_prev == (unsigned)(f.n_rchunks - 1)) {
-            __threadfence();
-            double S = 0.0;
-            int64_t C = 0;
-            for (int q = 0; q < f.n_rchunks; ++q) {
-                S += __ldcg(P.cpS + cs * kMaxRChunks + q);
-                C += __ldcg(P.cpC + cs * kMaxRChunks + q);
+            s_prev[g] = atomicAdd(&P.c_arrive[cs], 1u);
+            if (s_prev[g] == (unsigned)(f.n_rchunks - 1)) {
+                __threadfence();
+                double St = 0.0;
+                int64_t Ct = 0;
+                for (int q = 0; q < f.n_rchunks; ++q) {
+                    St += __ldcg(P.cpS + cs * kMaxRChunks + q);
+                    Ct += __ldcg(P.cpC + cs * kMaxRChunks + q);
+                }
+                P.cS64[cs] = St + (double)(f.n - Ct) * sq;
+                P.cCnt[cs] = Ct;
             }
-            P.cS64[cs] = S + (double)(f.n - C) * sq;
-            P.cCnt[cs] = C;
         }
         __syncthreads();
     }
