@@ -163,7 +163,7 @@ def cpu_baseline(frames, seconds_target=15.0):
             "seconds": dt}
 
 
-def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
+def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30, shape=None):
     """Config 4: Poisson stream of independent frames (N log-uniform [300, 50000],
     inlier ratio U[0.05, 0.70], 1 px noise) through the continuous-batching server."""
     import threading
@@ -174,7 +174,7 @@ def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30):
     from turboransac_b200._lib import TbrError
     reqs = [scenes.serving_request(i) for i in range(pool)]
     arrivals = scenes.poisson_arrivals(rate, seconds, seed=11)
-    srv = Server(ctx, budget_bytes=budget, max_slots=1024)
+    srv = Server(ctx, budget_bytes=budget, max_slots=1024, scoring_shape=shape)
     # warm the server (first steps pay one-time costs)
     for r in reqs[:32]:
         srv.submit(r)
@@ -254,13 +254,13 @@ def run_plain_serving(ctx, reqs, count=200):
             "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
 
 
-def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30):
+def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30, shape=None):
     """Served throughput at saturation: the serving requests submitted at once
     (repeats x the pool), completion rate of the continuous-batching server."""
     import numpy as np
 
     from turboransac_b200 import Server, scenes
-    srv = Server(ctx, budget_bytes=budget, max_slots=1024)
+    srv = Server(ctx, budget_bytes=budget, max_slots=1024, scoring_shape=shape)
     for r in reqs[:32]:
         srv.submit(r)
     srv.drain()
@@ -585,10 +585,11 @@ def main():
 
     serving = None
     if args.serve_seconds > 0:
-        serving, reqs = run_serving(ctx, args.serve_seconds)
+        shape = tuned["best"] if tuned else None
+        serving, reqs = run_serving(ctx, args.serve_seconds, shape=shape)
         serving["plain_call"] = run_plain_serving(ctx, reqs)
         serving["throughput_vs_plain"] = serving["throughput_fps"] / serving["plain_call"]["frames_per_s"]
-        serving["capacity"] = run_serving_capacity(ctx, reqs)
+        serving["capacity"] = run_serving_capacity(ctx, reqs, shape=shape)
         serving["capacity_vs_plain"] = serving["capacity"]["frames_per_s"] / serving["plain_call"]["frames_per_s"]
         print(f"[bench] serving: {serving['throughput_fps']:.0f} frames/s p50 {serving['p50_ms']:.2f} ms "
               f"p99 {serving['p99_ms']:.2f} ms success {serving['success_rate']:.4f}", file=sys.stderr, flush=True)
@@ -621,7 +622,9 @@ def main():
             "plain_call": plain,
             "serving": serving,
             "speedup_vs_plain": (value / plain["frames_per_s"]) if plain else None,
-            "gpu_launches": args.steps * (1 + 11 * steps_per_run),
+            # per graph launch: the reset, per engine step 8 RANSAC kernels + 3
+            # refinement kernels + the loop test, and the last step's refinement
+            "gpu_launches": args.steps * (1 + 12 * steps_per_run + 3),
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -471,12 +471,18 @@ class Server:
     copy=True copies them at submit (tbr_server_submit)."""
 
     def __init__(self, ctx: Context, budget_bytes: int = 8 << 30, max_slots: int = 512, max_queue: int = 1 << 16,
-                 ransac_opt: RansacOptions_cuda | None = None, copy: bool = False):
+                 ransac_opt: RansacOptions_cuda | None = None, copy: bool = False, scoring_shape: dict | None = None):
+        """scoring_shape: a Batch.autotune() result (hyp_per_thread, points_per_iter,
+        chunk_points) for the server's scoring pass; default: the built-in shape."""
         cfg = _lib.ServerConfigC()
         cfg.workspace_budget_bytes = budget_bytes
         cfg.max_slots = max_slots
         cfg.max_queue = max_queue
         cfg.ransac = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+        if scoring_shape:
+            cfg.ext.hyp_per_thread = int(scoring_shape.get("hyp_per_thread", 0))
+            cfg.ext.points_per_iter = int(scoring_shape.get("points_per_iter", 0))
+            cfg.ext.chunk_points = int(scoring_shape.get("chunk_points", 0))
         h = C.c_void_p()
         check(_lib.lib().tbr_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self._h = h
