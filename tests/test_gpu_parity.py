@@ -274,3 +274,28 @@ def test_prosac_sampling_matches_oracle(ctx, oracle):
         assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
         ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
         assert ae < 5 and te < 5
+
+
+def test_large_frame_and_workspace_limit(oracle):
+    """N = 100000 (the paper's large-N regime) matches the oracle; a frame that
+    does not fit the context's workspace is refused with OOM, and the context
+    stays usable."""
+    from turboransac_b200 import Context, TbrError
+    big = Context(0, 2 << 30)
+    f = scenes.make_frame(100000, 0.5, 1.0, 777)
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = big.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=16)
+    assert st.details["best_sample"] == o["info"].ransac.best_sample
+    np.testing.assert_array_equal(inl, o["inliers"])
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+    big.close()
+    small = Context(0, 256 << 20)
+    g = scenes.make_frame(2000000, 0.5, 1.0, 778)
+    with pytest.raises(TbrError) as e:
+        small.estimate_absolute_pose(g.uv, g.xyz, cam_of(g), ro, BundleOptions_cuda(), seed=g.seed)
+    assert "OOM" in str(e.value) or "workspace" in str(e.value)
+    h = scenes.plain_frame(0)
+    st, pose, inl = small.estimate_absolute_pose(h.uv, h.xyz, cam_of(h), ro, BundleOptions_cuda(), seed=h.seed)
+    assert st.num_inliers > 0
+    small.close()
