@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
-    ap.add_argument("--case", default="", choices=["", "scoring", "batch64", "precision"],
+    ap.add_argument("--case", default="", choices=["", "plain", "scoring", "batch64", "precision"],
                     help="scoring: one N=20000 frame, exactly 4096 samples; batch64: the batched workload's "
                          "first 64 frames in one graph (small cases for ncu)")
     return ap.parse_args()
@@ -349,6 +349,32 @@ def reference_cuda_build(frames, args):
             "plain_frame": measure([scenes.plain_frame(i) for i in range(64)])}
 
 
+def run_case_plain(args):
+    """Plain single frames (N=2000, 40 % inliers, the reference's call): latency."""
+    import numpy as np
+
+    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda, scenes
+    ctx = Context(0, 1 << 30)
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    frames = [scenes.plain_frame(i) for i in range(64)]
+    lat, gpu, ok = [], [], 0
+    for rep in range(1 + max(1, args.steps // 5)):
+        for f in frames:
+            t0 = time.perf_counter()
+            st, pose, _ = ctx.estimate_absolute_pose(f.uv, f.xyz, Camera_cuda(1, 640, 480, list(f.K)), ro,
+                                                     BundleOptions_cuda(), seed=f.seed)
+            dt = 1000.0 * (time.perf_counter() - t0)
+            if rep:
+                lat.append(dt)
+                gpu.append(st.details["gpu_ms"])
+                ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
+                ok += (ae < 5.0 and te < 5.0)
+    print(json.dumps({"case": "plain", "frames": len(lat), "frames_per_s": len(lat) / (sum(lat) / 1000.0),
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "gpu_p50_ms": float(np.percentile(gpu, 50)), "success_rate": ok / len(lat)}), flush=True)
+    ctx.close()
+
+
 def run_case_scoring(args):
     """Scoring-bound single frame: N=20000, 15 % inliers, exactly 4096 samples."""
     from turboransac_b200 import BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda, scenes
@@ -463,6 +489,9 @@ def main():
     args = parse()
     if args.case == "precision":
         run_case_precision(args)
+        return
+    if args.case == "plain":
+        run_case_plain(args)
         return
     if args.case == "scoring":
         run_case_scoring(args)
