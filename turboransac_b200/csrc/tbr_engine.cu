@@ -1637,7 +1637,7 @@ static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, 
 }
 
 // Resident frames from which a serving step overlaps refinement with RANSAC.
-constexpr int kServerOverlapFrames = 64;
+constexpr int kServerOverlapFrames = 16;
 
 // One iteration of the request loop, pipelined with the device:
 //   A. while the previous step runs, take queued requests that fit the free
@@ -1874,7 +1874,7 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
     s->o = make_run_options(&s->ro, nullptr, &cfg->ext);
     // Serving: bounded rounds per step so that one heavy frame cannot hold a
     // step (and the requests arriving meanwhile) for long.
-    s->o.max_rounds_step = 16;
+    s->o.max_rounds_step = 64;
     s->E.pp = s->o.pp;
     if (cfg->max_queue > 0) s->max_queue = cfg->max_queue;
     if (cudaMalloc(&s->d_status, 4 * kMaxActive) != cudaSuccess ||
@@ -1883,9 +1883,9 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
         delete s;
         return fail(TBR_ERR_OOM, "server allocation failed");
     }
-    // Staging for one step's admissions, sized up front (64 MiB each).
+    // Staging for one step's admissions, sized up front (128 MiB each).
     for (auto &b : s->stage)
-        if (b.ensure(64ull << 20) != TBR_OK) {
+        if (b.ensure(128ull << 20) != TBR_OK) {
             delete s;
             return fail(TBR_ERR_OOM, "server staging allocation failed");
         }
