@@ -343,10 +343,13 @@ def reference_cuda_build(frames, args):
                 "p50_ms": float(np.percentile(r["ms"], 50)), "p99_ms": float(np.percentile(r["ms"], 99)),
                 "success_rate": float(np.mean([a < 5.0 and b < 5.0 for a, b in ok]))}
 
+    sk = refcuda.scoring_kernel(scenes.scoring_frame(0))
+    sk["config"] = "scoring-bound frame (N=20000, 15 % inliers): one round of 4096 samples, kernel only"
     return {"build": "reference src/entry.cu, turbo_ransac.cu, ba.cu, nvcc sm_100a -O3 -rdc=true",
             "timing": "host clock around each call; the reference's stdout sent to /dev/null",
             "batched_workload": measure(frames),
-            "plain_frame": measure([scenes.plain_frame(i) for i in range(64)])}
+            "plain_frame": measure([scenes.plain_frame(i) for i in range(64)]),
+            "scoring_kernel": sk}
 
 
 def run_case_plain(args):

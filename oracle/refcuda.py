@@ -20,7 +20,7 @@ CURAND_LIB = os.path.join(HERE, "_ref", "libtbr_refcurand.so")
 
 
 def available() -> bool:
-    return os.access(BIN, os.X_OK) and os.path.exists(CURAND_LIB)
+    return os.access(BIN, os.X_OK) and os.path.exists(CURAND_LIB) and os.path.exists(KERNEL_LIB)
 
 
 def curand_triples(n: int, samples_per_round: int, rounds: int) -> np.ndarray:
@@ -35,6 +35,42 @@ def curand_triples(n: int, samples_per_round: int, rounds: int) -> np.ndarray:
     if rc:
         raise RuntimeError(f"ref_curand_triples failed ({rc})")
     return out
+
+
+KERNEL_LIB = os.path.join(HERE, "_ref", "libtbr_refkernel.so")
+
+
+def scoring_kernel(frame, samples: int = 4096, reps: int = 5, threshold_px: float = 4.0) -> dict:
+    """The reference's RANSAC kernel on one round of `samples` blocks over the
+    frame (its first-round cuRAND samples), timed on the device; pairs =
+    P3P solutions x points, counted with the reference's own P3P restated by
+    the oracle on the exported samples."""
+    import ctypes as C
+
+    from .oracle import Oracle
+    K = np.asarray(frame.K, np.float64)
+    f = 0.5 * (K[0] + K[1])
+    xn = np.ascontiguousarray(np.stack([(frame.uv[:, 0] - K[2]) / K[0], (frame.uv[:, 1] - K[3]) / K[1]], 1))
+    X = np.ascontiguousarray(frame.xyz, np.float64)
+    lib = C.CDLL(KERNEL_LIB)
+    lib.ref_scoring_kernel.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                       C.POINTER(C.c_float), C.POINTER(C.c_double)]
+    lib.ref_scoring_kernel.restype = C.c_int
+    ms, best = C.c_float(), C.c_double()
+    sq = (threshold_px / f) ** 2
+    rc = lib.ref_scoring_kernel(xn.ctypes.data, X.ctypes.data, frame.n, samples, sq, reps, C.byref(ms),
+                                C.byref(best))
+    if rc:
+        raise RuntimeError(f"ref_scoring_kernel failed ({rc})")
+    o = Oracle()
+    tri = curand_triples(frame.n, samples, 1)
+    hyps = 0
+    for a, b, c in tri:
+        x = np.stack([o.bearing(*xn[i]) for i in (a, b, c)])
+        hyps += o.p3p(x, X[[a, b, c]]).shape[0]
+    pairs = hyps * frame.n
+    return {"samples": samples, "hypotheses": hyps, "pairs": pairs, "kernel_ms": ms.value,
+            "pairs_per_s": pairs / (ms.value / 1000.0), "best_score": best.value}
 
 
 def _write_frames(path: str, frames) -> None:
