@@ -158,9 +158,19 @@ def cpu_baseline(frames, seconds_target=15.0):
     t0 = time.perf_counter()
     o.estimate_batch(sample, threads=cores)
     dt = time.perf_counter() - t0
+    # one core, on a smaller sample (~5 s)
+    m1 = int(max(1, min(len(frames), 5.0 / max(per_frame_wall * cores, 1e-6))))
+    t0 = time.perf_counter()
+    o.estimate_batch(frames[:m1], threads=1)
+    dt1 = time.perf_counter() - t0
+    model = ""
+    try:
+        model = next(l.split(":", 1)[1].strip() for l in open("/proc/cpuinfo") if l.startswith("model name"))
+    except Exception:
+        pass
     return {"value": m / dt, "unit": "frames/s", "cores": cores, "kind": "port",
             "sample": f"first {m} frames of the batched workload, FP64 oracle, {cores} threads over frames",
-            "seconds": dt}
+            "seconds": dt, "one_core": {"value": m1 / dt1, "frames": m1}, "cpu_model": model}
 
 
 def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30, shape=None):
