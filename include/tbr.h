@@ -98,7 +98,7 @@ typedef struct tbr_ext_options {
     uint64_t seed;                /* Philox key of the sampler (0 = ransac.seed) */
     const int32_t *replay_idx;    /* host: replayed triples, replay_count*3 int32 */
     int64_t replay_count;
-    int32_t hyp_per_thread;       /* scoring tile: 0 = auto, else 2, 4 or 8 hypotheses per lane */
+    int32_t hyp_per_thread;       /* scoring tile: 0 = auto, else 2, 4, 6 or 8 hypotheses per lane */
     int32_t chunk_points;         /* scoring tile: 0 = auto, else points per work item */
     /* Stop rule K = ceil(3 log(1-p) / log(1-w^3)) beyond the int range: the
      * reference's double->int assignment (turbo_ransac.cu:231) is undefined
@@ -238,7 +238,7 @@ tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max,
 
 /* Scoring-shape autotuner (no reference counterpart). Times the batch's graph
  * `repeats` times under each candidate shape -- hypotheses per warp block
- * (32 x hyp_per_thread: 64, 128, 256), points per iteration (2, 4) and points
+ * (32 x hyp_per_thread: 64, 128, 192, 256), points per iteration (2, 4) and points
  * per work-item tile (0 = sized from the step's work, 256, 512, 1024, 2048) --
  * and keeps the fastest for later tbr_batch_run calls. The shape changes only
  * the order of FP32 partial sums inside the filter; every candidate within the

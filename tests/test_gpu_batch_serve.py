@@ -123,7 +123,7 @@ def test_autotune_keeps_results(ctx):
     b.sync()
     before = b.results()
     best, tried = b.autotune(repeats=1)
-    assert len(tried) == 20 and all(t["ms"] > 0 for t in tried)
+    assert len(tried) == 30 and all(t["ms"] > 0 for t in tried)
     assert best["ms"] == min(t["ms"] for t in tried)
     b.run()
     b.sync()

@@ -132,7 +132,8 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
         o.quirk = ext->stop_rule_x86_quirk;
         o.force_samples = ext->force_samples;
         if (ext->max_total_samples > 0) o.max_total = ext->max_total_samples;
-        if (ext->hyp_per_thread == 2 || ext->hyp_per_thread == 4 || ext->hyp_per_thread == 8)
+        if (ext->hyp_per_thread == 2 || ext->hyp_per_thread == 4 || ext->hyp_per_thread == 6 ||
+            ext->hyp_per_thread == 8)
             o.hr = ext->hyp_per_thread;
         if (ext->points_per_iter == 2 || ext->points_per_iter == 4) o.pp = ext->points_per_iter;
         o.chunk_points = ext->chunk_points;
@@ -180,7 +181,7 @@ class Engine {
     int32_t *d_res_slots = nullptr;      // slot list of that download
     int32_t *d_replay = nullptr;
     int64_t d_replay_cap = 0;
-    int score_grid[4] = {0, 0, 0, 0};  // (HP, PP) = (1,4), (2,2), (2,4), (4,2)
+    int score_grid[6] = {0, 0, 0, 0, 0, 0};  // (HP, PP) = (1,4), (2,2), (2,4), (4,2), (3,2), (3,4)
     int rescore_grid = 0, p3p_grid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
@@ -285,9 +286,9 @@ class Engine {
         blocks.reset(max_blocks);
         for (int i = max_frames - 1; i >= 0; --i) free_slots.push_back(i);
         int occ = 0;
-        const void *sk[4] = {(const void *)k_score<1, 4>, (const void *)k_score<2, 2>, (const void *)k_score<2, 4>,
-                             (const void *)k_score<4, 2>};
-        for (int v = 0; v < 4; ++v) {
+        const void *sk[6] = {(const void *)k_score<1, 4>, (const void *)k_score<2, 2>, (const void *)k_score<2, 4>,
+                             (const void *)k_score<4, 2>, (const void *)k_score<3, 2>, (const void *)k_score<3, 4>};
+        for (int v = 0; v < 6; ++v) {
             TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sk[v], kScoreWarps * 32, 0));
             score_grid[v] = num_sms * std::max(occ, 1);
         }
@@ -388,6 +389,8 @@ class Engine {
         const int threads = kScoreWarps * 32;
         if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
         else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
+        else if (hr == 6 && pp == 4) k_score<3, 4><<<score_grid[5], threads, 0, st>>>(Q);
+        else if (hr == 6) k_score<3, 2><<<score_grid[4], threads, 0, st>>>(Q);
         else if (pp == 4) k_score<2, 4><<<score_grid[2], threads, 0, st>>>(Q);
         else k_score<2, 2><<<score_grid[1], threads, 0, st>>>(Q);
     }
@@ -1374,7 +1377,7 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
     struct Shape {
         int hr, pp;
     };
-    const Shape shapes[4] = {{2, 4}, {4, 2}, {4, 4}, {8, 2}};  // the compiled scoring variants
+    const Shape shapes[6] = {{2, 4}, {4, 2}, {4, 4}, {6, 2}, {6, 4}, {8, 2}};  // the compiled scoring variants
     const int chunks[5] = {0, 256, 512, 1024, 2048};
     std::vector<tbr_tune_entry> tried;
     cudaEvent_t t0, t1;
