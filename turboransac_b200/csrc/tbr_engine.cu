@@ -281,6 +281,7 @@ class Engine {
         }
         P.active = d_active;
         P.num_sms = num_sms;
+        P.lm_cluster_min = kLMClusterMin;
         TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
         TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
         blocks.reset(max_blocks);
@@ -487,7 +488,9 @@ class Engine {
             cudaGraph_t tail = nullptr;
             ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
             if (ok) {
-                launch_refine(Q, n, stream);
+                Pools Qt = Q;  // nothing runs beside the last step's refinement
+                Qt.lm_cluster_min = kLMClusterMinTail;
+                launch_refine(Qt, n, stream);
                 ok = cudaStreamEndCapture(stream, &tail) == cudaSuccess;
             }
             cudaGraphNode_t tail_node;

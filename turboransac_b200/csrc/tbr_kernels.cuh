@@ -134,6 +134,7 @@ struct Pools {
     const int32_t *active;  // slots advanced by this launch
     int32_t n_active;
     int32_t num_sms;
+    int64_t lm_cluster_min;  // inliers from which a frame's LM runs on a CTA cluster
     // per point (blocks * kSub entries)
     const double *uv64;  // raw pixels (2/pt)
     const double *X64;   // world points (3/pt)
@@ -1507,14 +1508,18 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     if (rank == 0 && threadIdx.x == 0) f.status = kDone;
 }
 
-// Frames with fewer inliers than this run their LM on one CTA; larger ones on
-// a cluster of kLMCluster CTAs (a single SM would serialise them).
+// Frames with fewer inliers than Pools::lm_cluster_min run their LM on one CTA,
+// larger ones on a cluster of kLMCluster CTAs. Beside RANSAC (frames finishing
+// in earlier steps) throughput wins: one CTA up to kLMClusterMin. After the last
+// step nothing else runs and the LM is the whole remaining time: clusters from
+// kLMClusterMinTail.
 constexpr int64_t kLMClusterMin = 10000;
+constexpr int64_t kLMClusterMinTail = 3000;
 
 __global__ void __launch_bounds__(kLMSmallThreads, 1) k_lm_small(Pools P) {
     const int slot = P.active[blockIdx.x];
     const FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending || f.num_inliers >= kLMClusterMin || f.lm_force_cluster) return;
+    if (f.status != kLMPending || f.num_inliers >= P.lm_cluster_min || f.lm_force_cluster) return;
     lm_frame<1>(P, slot);
 }
 
@@ -1522,7 +1527,7 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads,
     const int slot = P.active[blockIdx.x / kLMCluster];
     const FrameDev &f = P.frames[slot];
     // uniform across the cluster
-    if (f.status != kLMPending || (f.num_inliers < kLMClusterMin && !f.lm_force_cluster)) return;
+    if (f.status != kLMPending || (f.num_inliers < P.lm_cluster_min && !f.lm_force_cluster)) return;
     lm_frame<kLMCluster>(P, slot);
 }
 
