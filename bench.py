@@ -633,6 +633,12 @@ def main():
         serving["plain_call"] = run_plain_serving(ctx, reqs)
         serving["throughput_vs_plain"] = serving["throughput_fps"] / serving["plain_call"]["frames_per_s"]
         serving["capacity"] = run_serving_capacity(ctx, reqs, shape=shape)
+        # Latency under heavier offered loads (2 s each).
+        serving["sweep"] = []
+        for rate in (4000.0, 8000.0):
+            r, _ = run_serving(ctx, 2.0, rate=rate, shape=shape)
+            serving["sweep"].append({k: r[k] for k in ("offered_rate_hz", "throughput_fps", "p50_ms", "p99_ms",
+                                                       "p999_ms", "success_rate")})
         serving["capacity_vs_plain"] = serving["capacity"]["frames_per_s"] / serving["plain_call"]["frames_per_s"]
         print(f"[bench] serving: {serving['throughput_fps']:.0f} frames/s p50 {serving['p50_ms']:.2f} ms "
               f"p99 {serving['p99_ms']:.2f} ms success {serving['success_rate']:.4f}", file=sys.stderr, flush=True)
