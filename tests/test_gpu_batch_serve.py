@@ -168,3 +168,14 @@ def test_device_resident_inputs_match_host_inputs(ctx):
     ro = RO.to_c()
     st = _lib.lib().tbr_estimate_batch_device(ctx.handle, arr, 1, C.byref(ro), None, None, res, None)
     assert st != 0
+
+
+def test_estimate_batch_beyond_context_capacity(ctx):
+    """More frames than the context holds at once (1024) run in consecutive
+    groups; every result equals the plain call's."""
+    fr = [scenes.make_frame(300, 0.6, 1.0, 20000 + i) for i in range(1100)]
+    got = estimate_batch(ctx, fr, RO)
+    assert len(got) == 1100 and all(r["status"] == 0 for r in got)
+    for i in (0, 511, 1023, 1024, 1099):
+        d, pose = plain(ctx, fr[i])
+        same(got[i], got[i]["q"], got[i]["t"], d, pose)

@@ -1042,6 +1042,34 @@ tbr_status tbr_estimate_absolute_pose(tbr_context *ctx, const double *points2D, 
     return TBR_OK;
 }
 
+}  // extern "C"
+
+// Frames beyond what the context holds at once run in consecutive groups of
+// at most its frame capacity; each frame's result does not depend on the
+// grouping.
+static tbr_status estimate_frames_chunked(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                          std::vector<FrameResult> &res, const std::vector<uint8_t *> &masks,
+                                          std::vector<float> &ms, bool device_points) {
+    const size_t cap = (size_t)std::max(1, ctx->E.max_frames);
+    res.clear();
+    ms.assign(fr.size(), 0.f);
+    for (size_t i0 = 0; i0 < fr.size(); i0 += cap) {
+        const size_t i1 = std::min(fr.size(), i0 + cap);
+        std::vector<FrameHost> sub(fr.begin() + i0, fr.begin() + i1);
+        std::vector<uint8_t *> sm(masks.begin() + i0, masks.begin() + i1);
+        std::vector<FrameResult> r;
+        float t = 0.f;
+        int steps = 0;
+        tbr_status st = estimate_frames(ctx, sub, o, r, sm, &t, &steps, device_points);
+        if (st) return st;
+        res.insert(res.end(), r.begin(), r.end());
+        for (size_t i = i0; i < i1; ++i) ms[i] = t;
+    }
+    return TBR_OK;
+}
+
+extern "C" {
+
 tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
                               const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
                               tbr_frame_result *results, uint8_t *const *inliers) {
@@ -1062,15 +1090,14 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
     std::vector<uint8_t *> masks(n_frames, nullptr);
     if (inliers)
         for (int i = 0; i < n_frames; ++i) masks[i] = inliers[i];
-    float ms = 0.f;
-    int steps = 0;
-    tbr_status st = estimate_frames(ctx, fr, o, res, masks, &ms, &steps);
+    std::vector<float> ms;
+    tbr_status st = estimate_frames_chunked(ctx, fr, o, res, masks, ms, false);
     if (st) return st;
     for (int i = 0; i < n_frames; ++i) {
         for (int k = 0; k < 4; ++k) results[i].q[k] = res[i].q[k];
         for (int k = 0; k < 3; ++k) results[i].t[k] = res[i].t[k];
         results[i].status = TBR_OK;
-        fill_stats(res[i], fr[i].n, &results[i].stats, ms);
+        fill_stats(res[i], fr[i].n, &results[i].stats, ms[i]);
     }
     return TBR_OK;
 }
@@ -1112,15 +1139,14 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
     std::vector<uint8_t *> masks(n_frames, nullptr);
     if (inliers)
         for (int i = 0; i < n_frames; ++i) masks[i] = inliers[i];
-    float ms = 0.f;
-    int steps = 0;
-    tbr_status st = estimate_frames(ctx, fr, o, res, masks, &ms, &steps, true);
+    std::vector<float> ms;
+    tbr_status st = estimate_frames_chunked(ctx, fr, o, res, masks, ms, true);
     if (st) return st;
     for (int i = 0; i < n_frames; ++i) {
         for (int k = 0; k < 4; ++k) results[i].q[k] = res[i].q[k];
         for (int k = 0; k < 3; ++k) results[i].t[k] = res[i].t[k];
         results[i].status = TBR_OK;
-        fill_stats(res[i], fr[i].n, &results[i].stats, ms);
+        fill_stats(res[i], fr[i].n, &results[i].stats, ms[i]);
     }
     return TBR_OK;
 }
