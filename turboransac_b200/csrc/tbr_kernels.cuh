@@ -1209,12 +1209,25 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
 // out[] (shared). Uses 32*NV doubles of scratch.
 template <int NV>
 __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, double *out) {
+    static_assert(NV <= 32, "one value per lane after the warp reduction");
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // Warp reduce-scatter by recursive halving: at width h a lane trades the
+    // half of its 2h partial sums that its partner (lane ^ h) keeps, so after
+    // 16 + 8 + 4 + 2 + 1 exchanges lane k holds the warp's sum of value k.
+    double a[32];
 #pragma unroll
-    for (int k = 0; k < NV; ++k) {
-        v[k] = warp_sum(v[k]);
-        if (lane == 0) scratch[w * NV + k] = v[k];
+    for (int k = 0; k < 32; ++k) a[k] = k < NV ? v[k] : 0.0;
+#pragma unroll
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool upper = (lane & h) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const double keep = upper ? a[k + h] : a[k];
+            const double give = upper ? a[k] : a[k + h];
+            a[k] = keep + __shfl_xor_sync(0xffffffffu, give, h);
+        }
     }
+    if (lane < NV) scratch[w * NV + lane] = a[0];
     __syncthreads();
     if (threadIdx.x < NV) {
         double s = 0.0;
@@ -1226,8 +1239,8 @@ __device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, do
 
 constexpr int kLMCluster = 8;  // CTAs cooperating on one frame's LM
 
-constexpr int kLMSums = 28;
-enum LMLoss : int32_t { kLossCauchy = 0, kLossTruncated = 1, kLossHuber = 2, kLossTrivial = 3 };  // cost + 21 J^T W J + 6 J^T W r
+constexpr int kLMSums = 28;  // cost + 21 J^T W J + 6 J^T W r
+enum LMLoss : int32_t { kLossCauchy = 0, kLossTruncated = 1, kLossHuber = 2, kLossTrivial = 3 };
 
 // One pass over inliers [i0, i1) at pose (q, t): the FP64 Cauchy cost
 // (jaco.cuh:31-104) and, from the same FP64 residuals, the J^T W J lower
@@ -1411,12 +1424,14 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
         lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch, part);
     else if (threadIdx.x < kLMSums) part[threadIdx.x] = 0.0;
     __syncthreads();
-    cluster_totals();
+    // One CTA: its pass totals are the frame's; a cluster sums its CTAs' in rank 0.
+    const double *T = CL == 1 ? part : tot;
+    if constexpr (CL > 1) cluster_totals();
     if (rank == 0 && threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) q[k] = pq[k];
         for (int k = 0; k < 3; ++k) t[k] = pt[k];
-        cost = tot[0];
-        for (int k = 0; k < 27; ++k) Jc[k] = tot[1 + k];
+        cost = T[0];
+        for (int k = 0; k < 27; ++k) Jc[k] = T[1 + k];
         Jc[27] = 0.0;
         lambda = f.lm_lambda0;
         recompute = 1;
@@ -1456,25 +1471,35 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             quat_rotate(q, x[3], x[4], x[5], dt);
             for (int k = 0; k < 3; ++k) tn[k] = t[k] + dt[k];
         }
-        cluster.sync();
-        if (threadIdx.x == 0) {
-            pbrk = cluster.map_shared_rank(&brk, 0)[0];
-            const double *rq = cluster.map_shared_rank(qn, 0), *rt = cluster.map_shared_rank(tn, 0);
-            for (int k = 0; k < 4; ++k) pq[k] = rq[k];
-            for (int k = 0; k < 3; ++k) pt[k] = rt[k];
+        if constexpr (CL == 1) {
+            // One CTA: the candidate pose and the stop flag are read in place;
+            // the pass's own barriers order this thread's next writes to them.
+            __syncthreads();
+            if (brk) break;
+            lm_pass(P, base, i0, i1, qn, tn, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch,
+                    part);
+        } else {
+            cluster.sync();
+            if (threadIdx.x == 0) {
+                pbrk = cluster.map_shared_rank(&brk, 0)[0];
+                const double *rq = cluster.map_shared_rank(qn, 0), *rt = cluster.map_shared_rank(tn, 0);
+                for (int k = 0; k < 4; ++k) pq[k] = rq[k];
+                for (int k = 0; k < 3; ++k) pt[k] = rt[k];
+            }
+            __syncthreads();
+            if (pbrk) break;
+            lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch,
+                    part);
+            __syncthreads();
+            cluster_totals();
         }
-        __syncthreads();
-        if (pbrk) break;
-        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch, part);
-        __syncthreads();
-        cluster_totals();
         if (rank == 0 && threadIdx.x == 0) {
-            if (tot[0] < cost) {
+            if (T[0] < cost) {
                 for (int k = 0; k < 4; ++k) q[k] = qn[k];
                 for (int k = 0; k < 3; ++k) t[k] = tn[k];
                 lambda = fmax(f.lm_min_lambda, lambda / 10);
-                cost = tot[0];
-                for (int k = 0; k < 27; ++k) Jc[k] = tot[1 + k];
+                cost = T[0];
+                for (int k = 0; k < 27; ++k) Jc[k] = T[1 + k];
                 recompute = 1;
             } else {
                 ++invalid;
