@@ -1261,6 +1261,7 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
     float Sv[27], Cc[27];
 #pragma unroll
     for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
+#pragma unroll 2  // two points per thread in flight: the FP64 division and log1p chains overlap
     for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int64_t o = base + i;
         const double X0d = P.lX64[3 * o], X1d = P.lX64[3 * o + 1], X2d = P.lX64[3 * o + 2];
