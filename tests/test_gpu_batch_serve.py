@@ -179,3 +179,28 @@ def test_estimate_batch_beyond_context_capacity(ctx):
     for i in (0, 511, 1023, 1024, 1099):
         d, pose = plain(ctx, fr[i])
         same(got[i], got[i]["q"], got[i]["t"], d, pose)
+
+
+def test_server_honoured_options_match_plain(ctx):
+    """The server with honor_options (PROSAC over sorted correspondences, a raised
+    minimum sample count) gives the plain call's results under the same options."""
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0, progressive_sampling=True,
+                            max_prosac_iterations=30000, min_iterations=3000)
+    fr = []
+    for i in range(6):
+        f = scenes.make_frame(2500, 0.3, 1.0, 31000 + i)
+        order = np.concatenate([np.flatnonzero(f.inlier_gt), np.flatnonzero(~f.inlier_gt)])
+        f.uv, f.xyz, f.inlier_gt = f.uv[order].copy(), f.xyz[order].copy(), f.inlier_gt[order]
+        fr.append(f)
+    srv = Server(ctx, budget_bytes=1 << 30, max_slots=64, ransac_opt=ro, honor_options=True)
+    ids = [srv.submit(f) for f in fr]
+    srv.drain()
+    got = {r["id"]: r for r in srv.poll()}
+    srv.close()
+    for rid, f in zip(ids, fr):
+        r = got[rid]
+        st, pose, _ = ctx.estimate_absolute_pose(f.uv, f.xyz, Camera_cuda(1, 640, 480, list(f.K)), ro,
+                                                 BundleOptions_cuda(), seed=f.seed, honor_options=True)
+        assert r["status"] == 0 and r["samples"] == st.details["samples"] >= 3000
+        assert r["best_sample"] == st.details["best_sample"]
+        assert quat_angle(r["q"], pose.q) < 1e-9 and np.abs(r["t"] - pose.t).max() < 1e-9

@@ -471,14 +471,18 @@ class Server:
     copy=True copies them at submit (tbr_server_submit)."""
 
     def __init__(self, ctx: Context, budget_bytes: int = 8 << 30, max_slots: int = 512, max_queue: int = 1 << 16,
-                 ransac_opt: RansacOptions_cuda | None = None, copy: bool = False, scoring_shape: dict | None = None):
+                 ransac_opt: RansacOptions_cuda | None = None, copy: bool = False, scoring_shape: dict | None = None,
+                 honor_options: bool = False):
         """scoring_shape: a Batch.autotune() result (hyp_per_thread, points_per_iter,
-        chunk_points) for the server's scoring pass; default: the built-in shape."""
+        chunk_points) for the server's scoring pass; default: the built-in shape.
+        honor_options: apply the RANSAC options the reference ignores (see
+        tbr_ext_options.honor_options)."""
         cfg = _lib.ServerConfigC()
         cfg.workspace_budget_bytes = budget_bytes
         cfg.max_slots = max_slots
         cfg.max_queue = max_queue
         cfg.ransac = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+        cfg.ext.honor_options = int(honor_options)
         if scoring_shape:
             cfg.ext.hyp_per_thread = int(scoring_shape.get("hyp_per_thread", 0))
             cfg.ext.points_per_iter = int(scoring_shape.get("points_per_iter", 0))
