@@ -204,3 +204,29 @@ def test_server_honoured_options_match_plain(ctx):
         assert r["status"] == 0 and r["samples"] == st.details["samples"] >= 3000
         assert r["best_sample"] == st.details["best_sample"]
         assert quat_angle(r["q"], pose.q) < 1e-9 and np.abs(r["t"] - pose.t).max() < 1e-9
+
+
+def test_pinned_host_inputs_match_pageable(ctx):
+    """Frames in page-locked host memory go up without the staging copy (a
+    mix of pinned and pageable frames in one call); results are unchanged."""
+    import dataclasses
+
+    import torch
+    fr = mixed_frames() + [scenes.make_frame(30000, 0.5, 1.0, 9100 + i) for i in range(4)]  # > 512 KiB each
+    ref = estimate_batch(ctx, fr, RO)
+    keep, mixed = [], []
+    for i, f in enumerate(fr):
+        if i % 3 == 2:
+            mixed.append(f)
+            continue
+        tu = torch.empty(f.uv.shape, dtype=torch.float64, pin_memory=True)
+        tx = torch.empty(f.xyz.shape, dtype=torch.float64, pin_memory=True)
+        tu.numpy()[...] = f.uv
+        tx.numpy()[...] = f.xyz
+        keep += [tu, tx]
+        mixed.append(dataclasses.replace(f, uv=tu.numpy(), xyz=tx.numpy()))
+    got = estimate_batch(ctx, mixed, RO)
+    for a, b in zip(got, ref):
+        assert a["status"] == 0 and a["samples"] == b["samples"] and a["best_sample"] == b["best_sample"]
+        np.testing.assert_array_equal(a["q"], b["q"])
+        np.testing.assert_array_equal(a["t"], b["t"])

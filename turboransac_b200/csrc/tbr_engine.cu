@@ -759,12 +759,40 @@ static tbr_status copy_and_upload_overlapped(Engine &E, const StagedAdmission &A
     struct Group {
         size_t run, i, j;  // frames i .. j-1 of run
     };
+    // Large frames whose arrays are already page-locked go up directly, without
+    // a host copy (below ~512 KiB a copy into staging and a shared upload cost
+    // less than an upload call of their own); the others are grouped between them.
+    constexpr size_t kDirectBytes = 512u << 10;
+    auto pinned = [](const void *p) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    std::vector<char> direct(A.devs.size(), 0);
+    for (size_t i = 0; i < A.devs.size(); ++i) {
+        direct[i] = A.jobs[2 * i].bytes + A.jobs[2 * i + 1].bytes >= kDirectBytes && pinned(A.jobs[2 * i].src) &&
+                    pinned(A.jobs[2 * i + 1].src);
+        if (direct[i]) {
+            const size_t q0 = (size_t)A.devs[i].blk_off * kSub;
+            TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * q0), A.jobs[2 * i].src, A.jobs[2 * i].bytes,
+                                     cudaMemcpyHostToDevice, E.stream));
+            TBR_CUDA(cudaMemcpyAsync((void *)(E.P.X64 + 3 * q0), A.jobs[2 * i + 1].src, A.jobs[2 * i + 1].bytes,
+                                     cudaMemcpyHostToDevice, E.stream));
+        }
+    }
     std::vector<Group> groups;
     size_t total = 0;
     for (size_t r = 0; r < A.runs.size(); ++r)
         for (size_t i = A.span[r].first; i <= A.span[r].second;) {
+            if (direct[i]) {
+                ++i;
+                continue;
+            }
             size_t j = i, bytes = 0;
-            while (j <= A.span[r].second && (j == i || bytes < kGroupBytes)) {
+            while (j <= A.span[r].second && !direct[j] && (j == i || bytes < kGroupBytes)) {
                 bytes += A.jobs[2 * j].bytes + A.jobs[2 * j + 1].bytes;
                 ++j;
             }
