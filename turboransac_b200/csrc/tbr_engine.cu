@@ -173,6 +173,7 @@ class Engine {
     void *h_stage = nullptr;
     size_t h_stage_bytes = 0;
     unsigned long long *h_counters = nullptr;
+    FrameResult *h_results = nullptr;  // pinned: one call's packed results
     int32_t *d_active = nullptr;
     FrameDev *d_admit = nullptr;         // admission staging (device side)
     FrameResult *d_res_stage = nullptr;  // packed results of one download
@@ -194,6 +195,7 @@ class Engine {
         if (d_base) cudaFree(d_base);
         if (h_stage) cudaFreeHost(h_stage);
         if (h_counters) cudaFreeHost(h_counters);
+        if (h_results) cudaFreeHost(h_results);
         if (d_replay) cudaFree(d_replay);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -284,6 +286,7 @@ class Engine {
         P.lm_cluster_min = kLMClusterMin;
         TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
         TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
+        TBR_CUDA(cudaMallocHost(&h_results, sizeof(FrameResult) * kMaxActive));
         blocks.reset(max_blocks);
         for (int i = max_frames - 1; i >= 0; --i) free_slots.push_back(i);
         int occ = 0;
@@ -519,9 +522,9 @@ class Engine {
     std::vector<CachedGraph> graph_cache;
     static constexpr size_t kGraphCacheSize = 8;
 
-    // Runs the active frames of P (admitted and prepared) to completion as one
-    // graph launch; the counters must be zero.
-    tbr_status run_graph(int na, int hr, int *steps_out) {
+    // Enqueues the run of the active frames of P (admitted and prepared) to
+    // completion as one graph launch; the counters must be zero.
+    tbr_status launch_graph(int na, int hr) {
         cudaGraphExec_t exec = nullptr;
         for (size_t i = 0; i < graph_cache.size(); ++i)
             if (graph_cache[i].n == na && graph_cache[i].hr == hr && graph_cache[i].pp == pp) {
@@ -540,10 +543,6 @@ class Engine {
             graph_cache.push_back({na, hr, pp, exec});
         }
         TBR_CUDA(cudaGraphLaunch(exec, stream));
-        TBR_CUDA(cudaMemcpyAsync(h_counters, P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, stream));
-        TBR_CUDA(cudaStreamSynchronize(stream));
-        if (h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
-        if (steps_out) *steps_out = (int)h_counters[kCSteps];
         return TBR_OK;
     }
 
@@ -1001,20 +1000,33 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
     TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
     E.launch_prep((int)slots.size(), max_n);
     E.pp = o.pp;
-    st = E.run_graph((int)slots.size(), o.hr, steps_out);
+    st = E.launch_graph((int)slots.size(), o.hr);
     TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
     if (st == TBR_OK) {
-        res.resize(fr.size());
+        // Everything the caller gets back in one round trip: the results in
+        // the order of the active list (= slots), the masks, the counters.
+        const int n = (int)slots.size();
+        k_gather_results<<<(int)std::min<size_t>(1024, (n * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0,
+                           E.stream>>>(E.P.results, E.d_active, n, E.d_res_stage);
+        TBR_CUDA(cudaGetLastError());
+        TBR_CUDA(cudaMemcpyAsync(E.h_results, E.d_res_stage, sizeof(FrameResult) * n, cudaMemcpyDeviceToHost,
+                                 E.stream));
         for (size_t i = 0; i < slots.size(); ++i)
             if (i < masks.size() && masks[i])
                 TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + devs[i].blk_off * kSub, fr[i].n,
                                          cudaMemcpyDeviceToHost, E.stream));
-        st = fetch_results(E, slots, res.data());
-    }
-    if (st == TBR_OK) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, E.ev0, E.ev1);
-        if (ms_out) *ms_out = ms;
+        TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaStreamSynchronize(E.stream));
+        if (E.h_counters[kCError] & kErrTimeout) st = fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+        else if (E.h_counters[kCError] & kErrOverflow)
+            st = fail(TBR_ERR_INTERNAL, "step limit or capacity exceeded");
+        if (st == TBR_OK) {
+            res.assign(E.h_results, E.h_results + n);
+            if (steps_out) *steps_out = (int)E.h_counters[kCSteps];
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, E.ev0, E.ev1);
+            if (ms_out) *ms_out = ms;
+        }
     }
     cudaStreamSynchronize(E.stream);
     for (size_t i = 0; i < slots.size(); ++i) {
