@@ -604,7 +604,7 @@ def main():
         ts = []
         for i in range(1 + max(1, args.steps // 2)):
             t0 = time.perf_counter()
-            estimate_batch(ctx, fr, ro)
+            estimate_batch(ctx, fr, ro, as_array=True)
             dt = time.perf_counter() - t0
             if i:
                 ts.append(dt)
@@ -624,7 +624,7 @@ def main():
     dev_t = []
     for i in range(1 + max(1, args.steps // 2)):
         t0 = time.perf_counter()
-        estimate_batch_device(ctx, dframes, ro)
+        estimate_batch_device(ctx, dframes, ro, as_array=True)
         dt = time.perf_counter() - t0
         if i:
             dev_t.append(dt)
@@ -686,7 +686,9 @@ def main():
             "kernels_ms_per_batch": {k: v[0] for k, v in prof.items()},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_fps, "unit": "frames/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "inputs": "page-locked host memory", "pageable_inputs_value": e2e_pageable_fps},
+                    "inputs": "page-locked host memory", "pageable_inputs_value": e2e_pageable_fps,
+                    "call": "estimate_batch(ctx, frames, ro, as_array=True): Python descriptors, the C call, "
+                            "results as one record array"},
             "e2e_device_inputs": {"value": e2e_device_fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": d2h,
                                   "inputs": "correspondences already in device memory (CUDA tensors)"},

@@ -230,3 +230,44 @@ def test_pinned_host_inputs_match_pageable(ctx):
         assert a["status"] == 0 and a["samples"] == b["samples"] and a["best_sample"] == b["best_sample"]
         np.testing.assert_array_equal(a["q"], b["q"])
         np.testing.assert_array_equal(a["t"], b["t"])
+
+
+def test_staggered_admission_matches_resident_run(ctx):
+    """A host-buffer batch above 16 MiB is admitted in groups that join the
+    running step loop as their uploads land (later groups wait as kPending).
+    Samples, best sample, inliers, masks and poses equal the device-input call,
+    which admits every frame before the loop starts."""
+    import dataclasses
+
+    import torch
+
+    from turboransac_b200 import DeviceFrame, estimate_batch_device
+    rng = np.random.default_rng(77)
+    fr = [scenes.make_frame(12000, float(rng.uniform(0.12, 0.8)), 1.0, 41000 + i) for i in range(40)]
+    assert sum(40 * f.n for f in fr) >= 16 << 20
+    keep, mixed = [], []
+    for i, f in enumerate(fr):  # every third frame page-locked (direct upload inside a later group)
+        if i % 3:
+            mixed.append(f)
+            continue
+        tu = torch.empty(f.uv.shape, dtype=torch.float64, pin_memory=True)
+        tx = torch.empty(f.xyz.shape, dtype=torch.float64, pin_memory=True)
+        tu.numpy()[...] = f.uv
+        tx.numpy()[...] = f.xyz
+        keep += [tu, tx]
+        mixed.append(dataclasses.replace(f, uv=tu.numpy(), xyz=tx.numpy()))
+    dev = estimate_batch_device(ctx, [DeviceFrame(f) for f in fr], RO)
+    tail = list(range(len(fr) - 3, len(fr)))  # frames of the last admission group
+    ref_masks = [ctx.estimate_absolute_pose(fr[i].uv, fr[i].xyz, Camera_cuda(1, 640, 480, list(fr[i].K)), RO,
+                                            BundleOptions_cuda(), seed=fr[i].seed)[2] for i in tail]
+    for _ in range(2):
+        got = estimate_batch(ctx, mixed, RO, masks=True)
+        assert max(r["steps"] for r in got) >= 2
+        for a, b in zip(got, dev):
+            assert a["status"] == 0
+            assert a["samples"] == b["samples"] and a["best_sample"] == b["best_sample"]
+            assert a["num_inliers"] == b["num_inliers"] and a["lm_iterations"] == b["lm_iterations"]
+            np.testing.assert_array_equal(a["q"], b["q"])
+            np.testing.assert_array_equal(a["t"], b["t"])
+        for i, m in zip(tail, ref_masks):
+            np.testing.assert_array_equal(got[i]["inliers"].astype(bool), np.asarray(m).astype(bool))

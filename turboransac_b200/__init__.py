@@ -5,10 +5,10 @@ The compute path is libtbr.so (hand-written sm_100a kernels behind the C ABI in
 include/tbr.h); this package is its Python host mirror.
 """
 from . import build, scenes
-from .api import (Batch, BundleOptions_cuda, Server, Camera_cuda, CameraPose_cuda, Context, DeviceFrame,
+from .api import (RESULT_DTYPE, Batch, BundleOptions_cuda, Server, Camera_cuda, CameraPose_cuda, Context, DeviceFrame,
                   RansacOptions_cuda, RansacStats_cuda, TbrError, bundle_adjust_cuda, default_context,
                   estimate_absolute_pose_cuda, estimate_batch, estimate_batch_device, get_inliers_mx)
 
-__all__ = ["Batch", "Server", "estimate_batch", "estimate_batch_device", "DeviceFrame", "BundleOptions_cuda", "Camera_cuda", "CameraPose_cuda", "Context", "RansacOptions_cuda",
+__all__ = ["RESULT_DTYPE", "Batch", "Server", "estimate_batch", "estimate_batch_device", "DeviceFrame", "BundleOptions_cuda", "Camera_cuda", "CameraPose_cuda", "Context", "RansacOptions_cuda",
            "RansacStats_cuda", "TbrError", "bundle_adjust_cuda", "default_context",
            "estimate_absolute_pose_cuda", "get_inliers_mx"]

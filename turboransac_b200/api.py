@@ -297,39 +297,62 @@ _RESULT_DTYPE = np.dtype(_lib.FrameResultC)
 
 
 def _f64c(a):
+    a = np.asarray(a)
     return a if (a.dtype == np.float64 and a.flags.c_contiguous) else np.ascontiguousarray(a, np.float64)
+
+
+def _ptr(a):
+    """Address of a contiguous array's first element (ctypes' buffer route is
+    the cheapest per array; read-only and empty arrays take numpy's)."""
+    try:
+        return C.addressof(C.c_char.from_buffer(a))
+    except (TypeError, ValueError, BufferError):
+        return a.ctypes.data
+
+
+_U64 = 0xFFFFFFFFFFFFFFFF
 
 
 def _frame_descs(frames, seeds=None, max_reproj_error=0.0):
     """tbr_frame_desc entries for the frames' float64 arrays: (pointer for the C
     call, objects to keep alive until it returns)."""
-    keep = []
-    p2, p3 = [], []
-    for fr in frames:
-        uv, X = _f64c(fr.uv), _f64c(fr.xyz)
-        keep += [uv, X]
-        p2.append(uv.__array_interface__["data"][0])
-        p3.append(X.__array_interface__["data"][0])
-    a = np.zeros(len(frames), _DESC_DTYPE)
-    a["points2D"] = p2
-    a["points3D"] = p3
-    a["n"] = [k.shape[0] for k in keep[0::2]]
-    a["K"] = np.array([[float(k) for k in fr.K] for fr in frames], np.float64)
-    a["seed"] = np.array([(fr.seed if seeds is None else seeds[i]) & 0xFFFFFFFFFFFFFFFF
-                          for i, fr in enumerate(frames)], np.uint64)
-    a["max_reproj_error"] = [max_reproj_error or getattr(fr, "threshold_px", 0.0) for fr in frames]
-    keep.append(a)
-    return a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), keep
+    m = len(frames)
+    uvs = [_f64c(fr.uv) for fr in frames]
+    xyzs = [_f64c(fr.xyz) for fr in frames]
+    for i, (uv, X) in enumerate(zip(uvs, xyzs)):
+        if uv.ndim != 2 or uv.shape[1] != 2 or X.ndim != 2 or X.shape[1] != 3 or uv.shape[0] != X.shape[0]:
+            raise ValueError(f"frame {i}: uv must be (n, 2) and xyz (n, 3) with the same n")
+    a = np.zeros(m, _DESC_DTYPE)
+    a["points2D"] = [_ptr(u) for u in uvs]
+    a["points3D"] = [_ptr(x) for x in xyzs]
+    a["n"] = [u.shape[0] for u in uvs]
+    a["K"] = np.array([fr.K for fr in frames], np.float64).reshape(m, 4)
+    sd = [fr.seed for fr in frames] if seeds is None else list(seeds)
+    try:
+        a["seed"] = np.array(sd, np.uint64)
+    except (OverflowError, ValueError, TypeError):
+        a["seed"] = np.array([int(s) & _U64 for s in sd], np.uint64)
+    a["max_reproj_error"] = (max_reproj_error if max_reproj_error
+                             else [getattr(fr, "threshold_px", 0.0) for fr in frames])
+    return a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), (uvs, xyzs, a)
 
 
-def _results(res, n):
+_STAT_NAMES = _RESULT_DTYPE["stats"].names
+
+
+RESULT_DTYPE = _RESULT_DTYPE
+"""numpy dtype of one packed frame result (tbr_frame_result): fields q, t,
+status and the stats record."""
+
+
+def _results(res, n, as_array=False):
     a = np.frombuffer(res, dtype=_RESULT_DTYPE, count=n)
+    if as_array:
+        return a
     q, t, status = a["q"].copy(), a["t"].copy(), a["status"].tolist()
-    stats = a["stats"]
-    names = stats.dtype.names
-    cols = [stats[k].tolist() for k in names]
-    return [{"q": q[i], "t": t[i], "status": status[i], **dict(zip(names, (c[i] for c in cols)))}
-            for i in range(n)]
+    keys = ("q", "t", "status") + _STAT_NAMES
+    rows = a["stats"].tolist()
+    return [dict(zip(keys, (q[i], t[i], status[i]) + rows[i])) for i in range(n)]
 
 
 class Batch:
@@ -394,8 +417,12 @@ class Batch:
             pass
 
 
-def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, masks: bool = False):
-    """Host buffers in, results out, all frames in one call (tbr_estimate_batch)."""
+def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, masks: bool = False,
+                   as_array: bool = False):
+    """Host buffers in, results out, all frames in one call (tbr_estimate_batch).
+    Returns one dict per frame, or with as_array=True the packed results as a
+    numpy record array of RESULT_DTYPE (no per-frame Python objects; with masks
+    the inlier masks are then returned beside it: (array, [masks]))."""
     arr, keep = _frame_descs(frames)
     ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
     ext = _lib.ExtOptionsC()
@@ -408,44 +435,56 @@ def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None =
     with ctx._lock:
         check(_lib.lib().tbr_estimate_batch(ctx.handle, arr, len(frames), C.byref(ro), C.byref(ext), res,
                                             C.cast(mptrs, C.c_void_p) if masks else None))
-    out = _results(res, len(frames))
+    out = _results(res, len(frames), as_array)
+    if as_array:
+        return (out, mbufs) if masks else out
     if masks:
         for o, m in zip(out, mbufs):
             o["inliers"] = m
     return out
 
 
-def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None):
+def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None,
+                          as_array: bool = False):
     """Frames whose correspondences are already on the context's GPU
     (tbr_estimate_batch_device). Each frame has `uv` (n, 2) and `xyz` (n, 3)
     float64 contiguous CUDA tensors (or objects with data_ptr()), `K` and
     `seed`. `stream`: a torch.cuda.Stream (default: torch's current stream) whose
-    queued work the copy waits for. Results come back to the host."""
+    queued work the copy waits for. Results come back to the host, as dicts or
+    (as_array=True) as one record array of RESULT_DTYPE."""
     import torch
-    arr = (_lib.FrameDescC * len(frames))()
-    for i, fr in enumerate(frames):
-        for name, cols in (("uv", 2), ("xyz", 3)):
-            tt = getattr(fr, name)
-            if not (tt.is_cuda and tt.dtype == torch.float64 and tt.is_contiguous() and tt.dim() == 2
-                    and tt.shape[1] == cols):
-                raise ValueError(f"frame {i}: {name} must be a contiguous float64 CUDA tensor (n, {cols})")
-        if fr.uv.shape[0] != fr.xyz.shape[0]:
+    f64 = torch.float64
+    m = len(frames)
+    uvs = [fr.uv for fr in frames]
+    xyzs = [fr.xyz for fr in frames]
+    for i, (u, x) in enumerate(zip(uvs, xyzs)):
+        if not (u.is_cuda and x.is_cuda and u.dtype == f64 and x.dtype == f64 and u.dim() == 2 and x.dim() == 2
+                and u.is_contiguous() and x.is_contiguous()):
+            raise ValueError(f"frame {i}: uv and xyz must be contiguous float64 CUDA tensors (n, 2), (n, 3)")
+        su, sx = u.shape, x.shape
+        if su[1] != 2 or sx[1] != 3:
+            raise ValueError(f"frame {i}: uv must be (n, 2) and xyz (n, 3)")
+        if su[0] != sx[0]:
             raise ValueError(f"frame {i}: 2D and 3D point counts differ")
-        arr[i].points2D = fr.uv.data_ptr()
-        arr[i].points3D = fr.xyz.data_ptr()
-        arr[i].n = fr.uv.shape[0]
-        for k in range(4):
-            arr[i].K[k] = float(fr.K[k])
-        arr[i].seed = int(fr.seed) & 0xFFFFFFFFFFFFFFFF
-        arr[i].max_reproj_error = 0.0
+    a = np.zeros(m, _DESC_DTYPE)
+    a["points2D"] = [u.data_ptr() for u in uvs]
+    a["points3D"] = [x.data_ptr() for x in xyzs]
+    a["n"] = [u.shape[0] for u in uvs]
+    a["K"] = np.array([fr.K for fr in frames], np.float64).reshape(m, 4)
+    sd = [fr.seed for fr in frames]
+    try:
+        a["seed"] = np.array(sd, np.uint64)
+    except (OverflowError, ValueError, TypeError):
+        a["seed"] = np.array([int(s) & _U64 for s in sd], np.uint64)
     ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
     ext = _lib.ExtOptionsC()
-    res = (_lib.FrameResultC * len(frames))()
+    res = (_lib.FrameResultC * m)()
     st = stream if stream is not None else torch.cuda.current_stream()
     with ctx._lock:
-        check(_lib.lib().tbr_estimate_batch_device(ctx.handle, arr, len(frames), C.byref(ro), C.byref(ext),
-                                                   C.c_void_p(st.cuda_stream), res, None))
-    return _results(res, len(frames))
+        check(_lib.lib().tbr_estimate_batch_device(ctx.handle, a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), m,
+                                                   C.byref(ro), C.byref(ext), C.c_void_p(st.cuda_stream), res,
+                                                   None))
+    return _results(res, m, as_array)
 
 
 class DeviceFrame:

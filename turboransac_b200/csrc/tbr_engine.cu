@@ -177,7 +177,7 @@ class Engine {
     int32_t *d_active = nullptr;
     FrameDev *d_admit = nullptr;         // admission staging (device side)
     FrameResult *d_res_stage = nullptr;  // packed results of one download
-    IngestDesc *d_ingest = nullptr;      // device-resident inputs of one admission
+    char *d_ingest = nullptr;            // ingestion tables of one admission (k_ingest)
     cudaEvent_t ev_ingest = nullptr;     // the caller's stream, waited on before ingestion
     int32_t *d_res_slots = nullptr;      // slot list of that download
     int32_t *d_replay = nullptr;
@@ -187,6 +187,7 @@ class Engine {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void *d_stage_alias = nullptr;              // device address of the pinned staging buffer
     std::mutex mu;  // one call at a time per context
 
     ~Engine() {
@@ -244,7 +245,7 @@ class Engine {
         add((void **)&d_active, sizeof(int32_t) * kMaxActive);
         add((void **)&d_admit, sizeof(FrameDev) * kMaxActive);
         add((void **)&d_res_stage, sizeof(FrameResult) * kMaxActive);
-        add((void **)&d_ingest, sizeof(IngestDesc) * kMaxActive);
+        add((void **)&d_ingest, kIngestTableBytes);
         add((void **)&d_res_slots, sizeof(int32_t) * kMaxActive);
         add((void **)&P.uv64, 16 * np);
         add((void **)&P.X64, 24 * np);
@@ -313,6 +314,11 @@ class Engine {
         size_t nb = std::max(bytes, h_stage_bytes * 2);
         TBR_CUDA(cudaMallocHost(&h_stage, nb));
         h_stage_bytes = nb;
+        d_stage_alias = nullptr;
+        if (cudaHostGetDevicePointer(&d_stage_alias, h_stage, 0) != cudaSuccess) {
+            cudaGetLastError();
+            d_stage_alias = nullptr;
+        }
         return TBR_OK;
     }
 
@@ -432,20 +438,34 @@ class Engine {
         launch_refine(Q, n_active, stream, prof);
     }
 
-    void launch_prep(const Pools &Q, int n_active, int64_t max_n) {
+    void launch_prep(const Pools &Q, int n_active, int64_t max_n, cudaStream_t st) {
         const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024));
-        k_prep_bounds<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
-        k_prep_pack<<<dim3(bx, n_active), 256, 0, stream>>>(Q);
-        k_prosac_table<<<n_active, 1024, 0, stream>>>(Q);
+        k_prep_bounds<<<dim3(bx, n_active), 256, 0, st>>>(Q);
+        k_prep_pack<<<dim3(bx, n_active), 256, 0, st>>>(Q);
+        k_prosac_table<<<n_active, 1024, 0, st>>>(Q);
     }
-    void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n); }
+    void launch_prep(const Pools &Q, int n_active, int64_t max_n) { launch_prep(Q, n_active, max_n, stream); }
+    void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n, stream); }
+
+    static constexpr size_t kIngestTableBytes = 64 * 32 + sizeof(IngestTile) * kIngestTileCap;
+    static constexpr int kIngestGridHost = 32;  // CTAs of a zero-copy ingestion (the link saturates at 16)
+
+    // Split admission of a graph: the active frames from n_first on arrive
+    // during the first step (kPending; their ingestion table at d_ingest).
+    struct Stagger {
+        int n_first = 0;
+        int64_t max_n_rest = 0;
+    };
+    static int prep_bx(int64_t max_n) { return (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024)); }
 
     // The step loop as one graph: [reset ->] while (any frame in RANSAC)
     // { RANSAC step || inliers + LM of the frames that finished in the previous
     // step (disjoint frames) ; loop test } -> inliers + LM of the last step's.
-    // With d_init, a reset node first restores the frames from d_init.
+    // With d_init, a reset node first restores the frames from d_init. With sg,
+    // the first step runs before the loop, beside the ingestion and preparation
+    // of the frames that arrive late, which start RANSAC in the second step.
     bool build_loop_graph(const Pools &Q, int n, int hr, const FrameDev *d_init, cudaGraph_t *graph_out,
-                          cudaGraphExec_t *exec_out) {
+                          cudaGraphExec_t *exec_out, const Stagger *sg = nullptr) {
         cudaGraph_t graph = nullptr;
         cudaGraphConditionalHandle h;
         bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess &&
@@ -461,6 +481,27 @@ class Engine {
             kp.blockDim = dim3(128);
             kp.kernelParams = args;
             ok = cudaGraphAddKernelNode(&reset_node, graph, nullptr, 0, &kp) == cudaSuccess;
+        }
+        if (ok && sg && !d_init) {
+            cudaGraph_t pro = nullptr;
+            ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            if (ok) {
+                Pools Qr = Q;
+                Qr.active = Q.active + sg->n_first;
+                Qr.n_active = n - sg->n_first;
+                cudaEventRecord(ev_fork, stream);
+                cudaStreamWaitEvent(stream2, ev_fork, 0);
+                k_ingest<<<kIngestGridHost, 256, 0, stream2>>>((const int64_t *)d_ingest);
+                launch_prep(Qr, Qr.n_active, sg->max_n_rest, stream2);
+                launch_ransac(Q, n, hr, stream);
+                cudaEventRecord(ev_join, stream2);
+                cudaStreamWaitEvent(stream, ev_join, 0);
+                k_activate<<<1, kMaxActive, 0, stream>>>(Qr);
+                k_tick<<<1, 1, 0, stream>>>(Q);
+                ok = cudaStreamEndCapture(stream, &pro) == cudaSuccess;
+            }
+            if (ok) ok = cudaGraphAddChildGraphNode(&reset_node, graph, nullptr, 0, pro) == cudaSuccess;
+            if (pro) cudaGraphDestroy(pro);
         }
         cudaGraph_t body = nullptr;
         if (ok) {
@@ -516,7 +557,7 @@ class Engine {
     // Instantiated loop graphs of recent (frame count, scoring variant) shapes,
     // least recently used first.
     struct CachedGraph {
-        int n, hr, pp;
+        int n, hr, pp, n_first, bx;  // n_first, bx: split admission (0, 0 without)
         cudaGraphExec_t exec;
     };
     std::vector<CachedGraph> graph_cache;
@@ -524,10 +565,12 @@ class Engine {
 
     // Enqueues the run of the active frames of P (admitted and prepared) to
     // completion as one graph launch; the counters must be zero.
-    tbr_status launch_graph(int na, int hr) {
+    tbr_status launch_graph(int na, int hr, const Stagger *sg = nullptr) {
         cudaGraphExec_t exec = nullptr;
+        const int nf = sg ? sg->n_first : 0, bx = sg ? prep_bx(sg->max_n_rest) : 0;
         for (size_t i = 0; i < graph_cache.size(); ++i)
-            if (graph_cache[i].n == na && graph_cache[i].hr == hr && graph_cache[i].pp == pp) {
+            if (graph_cache[i].n == na && graph_cache[i].hr == hr && graph_cache[i].pp == pp &&
+                graph_cache[i].n_first == nf && graph_cache[i].bx == bx) {
                 CachedGraph g = graph_cache[i];
                 graph_cache.erase(graph_cache.begin() + i);
                 graph_cache.push_back(g);
@@ -535,12 +578,18 @@ class Engine {
                 break;
             }
         if (!exec) {
-            if (!build_loop_graph(P, na, hr, nullptr, nullptr, &exec)) return fail(TBR_ERR_CUDA, "graph capture failed");
+            Stagger s2;
+            if (sg) {  // the graph's preparation grid is sized for bx, whatever the frames
+                s2.n_first = nf;
+                s2.max_n_rest = (int64_t)bx * 1024;
+            }
+            if (!build_loop_graph(P, na, hr, nullptr, nullptr, &exec, sg ? &s2 : nullptr))
+                return fail(TBR_ERR_CUDA, "graph capture failed");
             if (graph_cache.size() >= kGraphCacheSize) {
                 cudaGraphExecDestroy(graph_cache.front().exec);
                 graph_cache.erase(graph_cache.begin());
             }
-            graph_cache.push_back({na, hr, pp, exec});
+            graph_cache.push_back({na, hr, pp, nf, bx, exec});
         }
         TBR_CUDA(cudaGraphLaunch(exec, stream));
         return TBR_OK;
@@ -753,27 +802,31 @@ static tbr_status upload_staged(Engine &E, const StagedAdmission &A) {
 // the link moves one group while the host threads copy the next: copy threads
 // take 1 MiB pieces in group order, and this thread issues a group's upload as
 // soon as its last piece is in.
+// Large frames whose arrays are already page-locked go up directly, without a
+// host copy (below ~512 KiB a copy into staging and a shared upload cost less
+// than an upload call of their own).
+constexpr size_t kDirectUploadBytes = 512u << 10;
+static bool page_locked(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+static bool direct_upload(const StagedAdmission &A, size_t i) {
+    return A.jobs[2 * i].bytes + A.jobs[2 * i + 1].bytes >= kDirectUploadBytes && page_locked(A.jobs[2 * i].src) &&
+           page_locked(A.jobs[2 * i + 1].src);
+}
+
 static tbr_status copy_and_upload_overlapped(Engine &E, const StagedAdmission &A) {
     constexpr size_t kGroupBytes = 8u << 20, kPiece = 1u << 20;
     struct Group {
         size_t run, i, j;  // frames i .. j-1 of run
     };
-    // Large frames whose arrays are already page-locked go up directly, without
-    // a host copy (below ~512 KiB a copy into staging and a shared upload cost
-    // less than an upload call of their own); the others are grouped between them.
-    constexpr size_t kDirectBytes = 512u << 10;
-    auto pinned = [](const void *p) {
-        cudaPointerAttributes at;
-        if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-            cudaGetLastError();
-            return false;
-        }
-        return at.type == cudaMemoryTypeHost;
-    };
     std::vector<char> direct(A.devs.size(), 0);
     for (size_t i = 0; i < A.devs.size(); ++i) {
-        direct[i] = A.jobs[2 * i].bytes + A.jobs[2 * i + 1].bytes >= kDirectBytes && pinned(A.jobs[2 * i].src) &&
-                    pinned(A.jobs[2 * i + 1].src);
+        direct[i] = direct_upload(A, i);
         if (direct[i]) {
             const size_t q0 = (size_t)A.devs[i].blk_off * kSub;
             TBR_CUDA(cudaMemcpyAsync((void *)(E.P.uv64 + 2 * q0), A.jobs[2 * i].src, A.jobs[2 * i].bytes,
@@ -855,36 +908,250 @@ static tbr_status copy_and_upload_overlapped(Engine &E, const StagedAdmission &A
     return upload_records(E, A);
 }
 
+// ------------------------------------------------------ ingestion tables --
+// Tiles of one (source, pool destination) row, at most `tile` bytes each.
+static void add_row_tiles(std::vector<IngestTile> &v, const void *src, const void *dst, size_t bytes, size_t tile) {
+    for (size_t o = 0; o < bytes; o += tile)
+        v.push_back({(const char *)src + o, (char *)dst + o, (int64_t)std::min(tile, bytes - o)});
+}
+// Frame k's two rows: uv into the pool's uv64, xyz into X64.
+static void add_frame_tiles(std::vector<IngestTile> &v, const Engine &E, const FrameDev &d, int64_t n,
+                            const void *src_uv, const void *src_xyz, size_t tile) {
+    const size_t q0 = (size_t)d.blk_off * kSub;
+    add_row_tiles(v, src_uv, E.P.uv64 + 2 * q0, 16 * (size_t)n, tile);
+    add_row_tiles(v, src_xyz, E.P.X64 + 3 * q0, 24 * (size_t)n, tile);
+}
+// Tile size that keeps every table of one call within d_ingest.
+static size_t ingest_tile_bytes(const std::vector<FrameHost> &fr) {
+    size_t tile = kIngestTileBytes;
+    for (;;) {
+        size_t cnt = 0;
+        for (auto &f : fr) cnt += (16 * (size_t)f.n + tile - 1) / tile + (24 * (size_t)f.n + tile - 1) / tile;
+        if (cnt <= (size_t)kIngestTileCap) return tile;
+        tile *= 2;
+    }
+}
+// Writes a table (count header + tiles) at byte `off` of the pinned mirror
+// `h` and enqueues its upload to the same offset of d_ingest; returns the
+// device address of the table and advances `off`.
+static const int64_t *put_table(Engine &E, char *h, size_t &off, const std::vector<IngestTile> &t) {
+    if (off + 16 + sizeof(IngestTile) * t.size() > Engine::kIngestTableBytes) return nullptr;
+    int64_t *hdr = (int64_t *)(h + off);
+    hdr[0] = (int64_t)t.size();
+    hdr[1] = 0;
+    if (!t.empty()) std::memcpy(hdr + 2, t.data(), sizeof(IngestTile) * t.size());
+    const size_t bytes = 16 + sizeof(IngestTile) * t.size();
+    const int64_t *d = (const int64_t *)(E.d_ingest + off);
+    if (cudaMemcpyAsync((void *)d, hdr, bytes, cudaMemcpyHostToDevice, E.stream) != cudaSuccess) return nullptr;
+    off += (bytes + 15) & ~size_t(15);
+    return d;
+}
+// Device address of page-locked host memory (nullptr for pageable memory).
+static const void *mapped_address(const void *p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
+}
+
+// Host-buffer admission by zero-copy ingestion: every frame's arrays are read
+// by k_ingest over the link, from the caller's memory when it is page-locked,
+// else from a staging copy made by the host threads. Frames are ingested in
+// groups of about kIngestGroupBytes of staged data, so the link moves one
+// group while the host threads copy the next; page-locked frames cost no host
+// work at all, and no per-frame copy call is issued.
+//
+// With `launch`, the call also starts the run and overlaps it with the
+// ingestion: the frames are split, in order, and only the first part (about
+// kStaggerFirstShare of the bytes) is ingested and prepared before the loop
+// graph starts; the rest is admitted kPending and ingested and prepared by the
+// graph itself beside the first engine step, and starts RANSAC in the second
+// (a frame's samples and results do not depend on the step it starts in;
+// nothing waits on another stream). E.ev0 then marks the start of the first
+// part's preparation.
+//
+// `slots`, `max_n` and `devs` are set as soon as the frames hold slots (the
+// caller releases them whatever happens next).
+constexpr size_t kZeroCopyMinBytes = 4u << 20;
+constexpr size_t kIngestGroupBytes = 8u << 20;
+constexpr size_t kStaggerMinBytes = 16u << 20;
+constexpr double kStaggerFirstShare = 0.35;
+
+static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                    std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> &devs,
+                                    bool launch) {
+    constexpr size_t kPiece = 1u << 20;
+    const size_t n = fr.size();
+    const size_t tab_off = stage_bytes(fr);
+    tbr_status st = E.ensure_stage(tab_off + Engine::kIngestTableBytes);
+    if (st) return st;
+    StagedAdmission A;
+    st = stage_frames(E, fr, o, (char *)E.h_stage, A, false, true);
+    if (st) return st;
+    slots = A.slots;
+    max_n = A.max_n;
+    devs = A.devs;
+    if (!E.d_stage_alias) return fail(TBR_ERR_CUDA, "staging buffer has no device address");
+    // Sources as the device sees them.
+    std::vector<const void *> su(n), sx(n);
+    std::vector<char> staged(n, 0);
+    std::vector<size_t> fb(n);
+    size_t total = 0;
+    for (size_t k = 0; k < n; ++k) {
+        total += (fb[k] = A.jobs[2 * k].bytes + A.jobs[2 * k + 1].bytes);
+        su[k] = mapped_address(fr[k].uv);
+        sx[k] = su[k] ? mapped_address(fr[k].xyz) : nullptr;
+        if (!su[k] || !sx[k]) {
+            staged[k] = 1;
+            su[k] = (const char *)E.d_stage_alias + ((const char *)A.jobs[2 * k].dst - (const char *)E.h_stage);
+            sx[k] = (const char *)E.d_stage_alias + ((const char *)A.jobs[2 * k + 1].dst - (const char *)E.h_stage);
+        }
+    }
+    size_t n_first = n;
+    Engine::Stagger sg;
+    if (launch) {
+        size_t acc = 0;
+        const size_t first = (size_t)(kStaggerFirstShare * (double)total);
+        n_first = 0;
+        while (n_first < n && (n_first == 0 || acc < first)) acc += fb[n_first++];
+        if (n_first == n) n_first = n - 1;  // at least one late frame
+        sg.n_first = (int)n_first;
+        for (size_t k = n_first; k < n; ++k) {
+            A.hd[k].status = kPending;
+            sg.max_n_rest = std::max(sg.max_n_rest, fr[k].n);
+        }
+    }
+    // Ingestion groups of the first part: [gb[g], gb[g + 1]); at most about
+    // 60 tables, so that their headers fit d_ingest.
+    size_t staged_total = 0;
+    for (size_t k = 0; k < n_first; ++k) staged_total += staged[k] ? fb[k] : 0;
+    const size_t group_bytes = std::max(kIngestGroupBytes, staged_total / 60 + 1);
+    std::vector<size_t> gb{0};
+    for (size_t k = 0, acc = 0; k < n_first; ++k) {
+        acc += staged[k] ? fb[k] : 0;
+        if (acc >= group_bytes || k + 1 == n_first) {
+            gb.push_back(k + 1);
+            acc = 0;
+        }
+    }
+    const size_t G = gb.size() - 1;  // the late frames are group G
+    struct Piece {
+        CopyJob job;
+        size_t group;
+    };
+    std::vector<Piece> pieces;
+    std::unique_ptr<std::atomic<int>[]> left(new std::atomic<int>[G + 1]);
+    for (size_t g = 0; g <= G; ++g) {
+        const size_t k0 = g < G ? gb[g] : n_first, k1 = g < G ? gb[g + 1] : n;
+        int cnt = 0;
+        for (size_t k = k0; k < k1; ++k)
+            if (staged[k])
+                for (size_t jb = 2 * k; jb < 2 * k + 2; ++jb)
+                    for (size_t off = 0; off < A.jobs[jb].bytes; off += kPiece, ++cnt)
+                        pieces.push_back({{(char *)A.jobs[jb].dst + off, (const char *)A.jobs[jb].src + off,
+                                           std::min(kPiece, A.jobs[jb].bytes - off)},
+                                          g});
+        left[g].store(cnt, std::memory_order_relaxed);
+    }
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < pieces.size();) {
+            std::memcpy(pieces[k].job.dst, pieces[k].job.src, pieces[k].job.bytes);
+            left[pieces[k].group].fetch_sub(1, std::memory_order_release);
+        }
+    };
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> th;
+    const size_t staged_bytes = pieces.size() * kPiece;
+    if (staged_bytes >= 4 * kPiece)
+        for (unsigned t = 0; t < std::min(8u, hw); ++t) th.emplace_back(work);
+    else
+        work();  // little to copy: this thread does it
+    auto wait_group = [&](size_t g) {
+        while (left[g].load(std::memory_order_acquire) > 0) std::this_thread::yield();
+    };
+    const size_t tile = ingest_tile_bytes(fr);
+    auto enqueue = [&]() -> tbr_status {
+        tbr_status s2 = upload_records(E, A);
+        if (s2) return s2;
+        char *h = (char *)E.h_stage + tab_off;
+        // The late frames' table sits at offset 0, where the graph reads it;
+        // the first part's tables follow it.
+        std::vector<IngestTile> late;
+        if (launch)
+            for (size_t k = n_first; k < n; ++k) add_frame_tiles(late, E, A.devs[k], fr[k].n, su[k], sx[k], tile);
+        size_t off = launch ? ((16 + sizeof(IngestTile) * late.size() + 15) & ~size_t(15)) : 0;
+        std::vector<IngestTile> t;
+        for (size_t g = 0; g < G; ++g) {
+            t.clear();
+            for (size_t k = gb[g]; k < gb[g + 1]; ++k) add_frame_tiles(t, E, A.devs[k], fr[k].n, su[k], sx[k], tile);
+            wait_group(g);
+            const int64_t *d = put_table(E, h, off, t);
+            if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+            k_ingest<<<Engine::kIngestGridHost, 256, 0, E.stream>>>(d);
+            TBR_CUDA(cudaGetLastError());
+        }
+        if (!launch) return TBR_OK;
+        size_t off0 = 0;
+        wait_group(G);  // the graph reads the late frames' staging copies
+        if (!put_table(E, h, off0, late)) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+        TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
+        Pools Qf = E.P;
+        Qf.n_active = (int32_t)n_first;
+        int64_t max_first = 0;
+        for (size_t k = 0; k < n_first; ++k) max_first = std::max(max_first, fr[k].n);
+        E.launch_prep(Qf, (int)n_first, max_first, E.stream);
+        E.pp = o.pp;
+        return E.launch_graph((int)n, o.hr, &sg);
+    };
+    st = enqueue();
+    for (auto &x : th) x.join();
+    return st;
+}
+
 // Both halves through the context's own staging buffer. With device_points the
 // frames' point arrays are device memory of this GPU: they are copied into the
-// pool by one kernel, with no host staging.
+// pool by one kernel, with no host staging. Multi-frame host batches of some
+// size are ingested zero-copy (admit_host_frames); a small admission uploads
+// its staging runs with copy calls.
 static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
                                std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> *host_devs = nullptr,
                                bool device_points = false) {
+    size_t in_bytes = 0;
+    for (auto &f : fr) in_bytes += 40 * (size_t)f.n;
+    if (!device_points && fr.size() >= 2 && in_bytes >= kZeroCopyMinBytes) {
+        std::vector<FrameDev> d;
+        tbr_status st = admit_host_frames(E, fr, o, slots, max_n, d, false);
+        if (host_devs) *host_devs = d;
+        return st;
+    }
     auto r256 = [](size_t b) { return (b + 255) & ~size_t(255); };
     const size_t rec = r256(sizeof(FrameDev) * fr.size()) + r256(4 * fr.size());
-    tbr_status st = E.ensure_stage(device_points ? rec + r256(sizeof(IngestDesc) * fr.size()) + 256
-                                                 : stage_bytes(fr));
+    tbr_status st = E.ensure_stage(device_points ? rec + Engine::kIngestTableBytes : stage_bytes(fr));
     if (st) return st;
     StagedAdmission A;
     st = stage_frames(E, fr, o, (char *)E.h_stage, A, false, !device_points);
     if (st) return st;
+    // The caller releases these, whatever happens next.
+    slots = A.slots;
+    max_n = A.max_n;
+    if (host_devs) *host_devs = A.devs;
     if (device_points) {
-        IngestDesc *hi = (IngestDesc *)((char *)E.h_stage + rec);
-        for (size_t i = 0; i < fr.size(); ++i) hi[i] = {fr[i].uv, fr[i].xyz, fr[i].n, A.devs[i].blk_off * kSub};
-        TBR_CUDA(cudaMemcpyAsync(E.d_ingest, hi, sizeof(IngestDesc) * fr.size(), cudaMemcpyHostToDevice, E.stream));
-        const int bx = (int)std::min<int64_t>(64, std::max<int64_t>(1, (A.max_n + 1023) / 1024));
-        k_ingest<<<dim3(bx, (unsigned)fr.size()), 256, 0, E.stream>>>(E.d_ingest, E.P);
+        std::vector<IngestTile> t;
+        for (size_t i = 0; i < fr.size(); ++i)
+            add_frame_tiles(t, E, A.devs[i], fr[i].n, fr[i].uv, fr[i].xyz, ingest_tile_bytes(fr));
+        size_t off = 0;
+        const int64_t *d = put_table(E, (char *)E.h_stage + rec, off, t);
+        if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+        k_ingest<<<E.num_sms * 2, 256, 0, E.stream>>>(d);
         TBR_CUDA(cudaGetLastError());
         st = upload_records(E, A);
     } else {
         st = copy_and_upload_overlapped(E, A);
     }
-    if (st) return st;
-    slots = A.slots;
-    max_n = A.max_n;
-    if (host_devs) *host_devs = A.devs;
-    return TBR_OK;
+    return st;
 }
 
 // Results of `slots` into `out` (host), through one packed download.
@@ -995,13 +1262,21 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
     int64_t max_n = 0;
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
-    tbr_status st = admit_frames(E, fr, o, slots, max_n, &devs, device_points);
-    if (st) return st;
-    TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
-    E.launch_prep((int)slots.size(), max_n);
-    E.pp = o.pp;
-    st = E.launch_graph((int)slots.size(), o.hr);
-    TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    size_t in_bytes = 0;
+    for (auto &f : fr) in_bytes += 40 * (size_t)f.n;
+    tbr_status st;
+    if (!device_points && fr.size() >= 2 && in_bytes >= kStaggerMinBytes) {
+        st = admit_host_frames(E, fr, o, slots, max_n, devs, true);
+    } else {
+        st = admit_frames(E, fr, o, slots, max_n, &devs, device_points);
+        if (st == TBR_OK) {
+            TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
+            E.launch_prep((int)slots.size(), max_n);
+            E.pp = o.pp;
+            st = E.launch_graph((int)slots.size(), o.hr);
+        }
+    }
+    if (st == TBR_OK) TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
     if (st == TBR_OK) {
         // Everything the caller gets back in one round trip: the results in
         // the order of the active list (= slots), the masks, the counters.

@@ -42,7 +42,18 @@ constexpr int kLMSmallThreads = 384;  // one CTA per frame: 12 warps, no registe
 // kLMReady: RANSAC finished in the step stamped in lm_epoch; k_inliers takes it
 // one step later (so that in the captured loop it can run beside the next
 // step's RANSAC kernels without racing them) and moves it to kLMPending.
-enum FrameStatus : int32_t { kFree = 0, kRansac = 1, kLMPending = 2, kDone = 3, kFailed = 4, kLMReady = 5 };
+// kPending: admitted, its correspondences still on the way; every step kernel
+// skips it until k_activate moves it to kRansac (a frame's samples and results
+// do not depend on the step it starts in).
+enum FrameStatus : int32_t {
+    kFree = 0,
+    kRansac = 1,
+    kLMPending = 2,
+    kDone = 3,
+    kFailed = 4,
+    kLMReady = 5,
+    kPending = 6
+};
 
 enum Counter : int {
     kCScoreNext = 0,
@@ -1581,6 +1592,15 @@ __global__ void k_loop_ctl(Pools P, cudaGraphConditionalHandle h, unsigned long 
     cudaGraphSetConditional(h, v);
 }
 
+// Frames of Q waiting for their data start RANSAC (their points are in the
+// pool and prepared).
+__global__ void k_activate(Pools Q) {
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < Q.n_active; a += gridDim.x * blockDim.x) {
+        FrameDev &f = Q.frames[Q.active[a]];
+        if (f.status == kPending) f.status = kRansac;
+    }
+}
+
 // Restores the frames of a batch to their post-admission state.
 __global__ void k_reset_frames(Pools P, const FrameDev *init) {
     const int a = blockIdx.x;
@@ -1591,25 +1611,53 @@ __global__ void k_reset_frames(Pools P, const FrameDev *init) {
     if (a == 0 && threadIdx.x < kCNum) P.counters[threadIdx.x] = 0;
 }
 
-// Device-resident input: one frame's correspondences, copied into the pool.
-struct IngestDesc {
-    const double *uv, *xyz;
-    int64_t n, dst;  // points; first pool point of the frame
+// Correspondence ingestion: a table of byte ranges (tiles) copied into the
+// pool, from device memory or from page-locked host memory read over the link
+// (zero-copy). The table is an int64 tile count, a pad word, then the tiles.
+struct IngestTile {
+    const char *src;
+    char *dst;
+    int64_t bytes;  // a multiple of 8
 };
-__global__ void k_ingest(const IngestDesc *d, Pools P) {
-    const IngestDesc g = d[blockIdx.y];
-    double *uv = const_cast<double *>(P.uv64), *X = const_cast<double *>(P.X64);  // the pool's input arrays
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t o = g.dst + i;
-        uv[2 * o] = g.uv[2 * i];
-        uv[2 * o + 1] = g.uv[2 * i + 1];
-        X[3 * o] = g.xyz[3 * i];
-        X[3 * o + 1] = g.xyz[3 * i + 1];
-        X[3 * o + 2] = g.xyz[3 * i + 2];
+constexpr int kIngestTileCap = 8192;           // tiles of one call, all tables together
+constexpr size_t kIngestTileBytes = 256u << 10;
+
+// Copies `bytes` (a multiple of 8) from src to dst with the threads of one
+// CTA: 16-byte words four at a time when both ends allow it.
+__device__ __forceinline__ void copy_block(const char *__restrict__ src, char *__restrict__ dst, int64_t bytes) {
+    const int t = threadIdx.x, T = blockDim.x;
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+        const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+        uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+        const int64_t n4 = bytes / 16;
+        int64_t i = t;
+        for (; i + 3 * T < n4; i += 4 * T) {
+            const uint4 a = s4[i], b = s4[i + T], c = s4[i + 2 * T], d = s4[i + 3 * T];
+            d4[i] = a;
+            d4[i + T] = b;
+            d4[i + 2 * T] = c;
+            d4[i + 3 * T] = d;
+        }
+        for (; i < n4; i += T) d4[i] = s4[i];
+        if (t == 0 && (bytes & 15))
+            reinterpret_cast<unsigned long long *>(dst)[bytes / 8 - 1] =
+                reinterpret_cast<const unsigned long long *>(src)[bytes / 8 - 1];
+    } else {
+        const unsigned long long *s8 = reinterpret_cast<const unsigned long long *>(src);
+        unsigned long long *d8 = reinterpret_cast<unsigned long long *>(dst);
+        for (int64_t i = t; i < bytes / 8; i += T) d8[i] = s8[i];
     }
 }
 
-// Autotuner: the scoring shape of a batch's initial frame records.
+__global__ void __launch_bounds__(256) k_ingest(const int64_t *table) {
+    const int64_t n = table[0];
+    const IngestTile *tiles = reinterpret_cast<const IngestTile *>(table + 2);
+    for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+        const IngestTile t = tiles[k];
+        copy_block(t.src, t.dst, t.bytes);
+    }
+}
+
 __global__ void k_set_shape(FrameDev *init, int n, int hr, int chunk_points) {
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= n) return;
