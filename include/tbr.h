@@ -321,7 +321,7 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D,
                                    double max_reproj_error, const int32_t *triples,
                                    int64_t n_samples, int64_t *ids, double *poses,
                                    float *scores32, int64_t *counts, int64_t cap,
-                                   int64_t *n_hyp);
+                                   int64_t *n_hyp, const tbr_ext_options *ext);
 
 /* --------------------------------------------------------- no allocation --
  * No counterpart in the reference. FP64 truncated-MSAC scores and inlier counts

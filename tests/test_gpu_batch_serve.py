@@ -271,3 +271,28 @@ def test_staggered_admission_matches_resident_run(ctx):
             np.testing.assert_array_equal(a["t"], b["t"])
         for i, m in zip(tail, ref_masks):
             np.testing.assert_array_equal(got[i]["inliers"].astype(bool), np.asarray(m).astype(bool))
+
+
+def test_tensor_scoring_batch_matches_fp32_shape(ctx):
+    """A batch scored on the tensor cores (hyp_per_thread=2, points_per_iter=128,
+    several point-chunk sizes) gives the FP32 shape's results: the FP64 re-rank
+    decides, the filter only has to keep the best within its band."""
+    fr = mixed_frames() + [scenes.make_frame(30000, 0.15, 1.0, 9300), scenes.make_frame(700, 0.5, 2.0, 9301)]
+    b = Batch(ctx, fr, RO)
+    b.run()
+    b.sync()
+    ref = b.results()
+    b.close()
+    for chunk in (0, 256, 2048):
+        b = Batch(ctx, fr, RO, hyp_per_thread=2, points_per_iter=128, chunk_points=chunk)
+        for _ in range(2):
+            b.run()
+            b.sync()
+            got = b.results()
+            for r0, r1 in zip(ref, got):
+                assert r1["status"] == 0
+                assert r1["samples"] == r0["samples"] and r1["best_sample"] == r0["best_sample"]
+                assert r1["num_inliers"] == r0["num_inliers"]
+                np.testing.assert_array_equal(r1["q"], r0["q"])
+                np.testing.assert_array_equal(r1["t"], r0["t"])
+        b.close()

@@ -21,11 +21,17 @@ def cam_of(f):
     return Camera_cuda(1, 640, 480, list(f.K))
 
 
-def test_debug_scores_counts_vs_oracle(ctx, oracle):
+# Scoring shape on the tensor cores (tcgen05, TF32 split operands).
+TENSOR = {"hyp_per_thread": 2, "points_per_iter": 128}
+
+
+@pytest.mark.parametrize("shape", [None, TENSOR, dict(TENSOR, chunk_points=256)],
+                         ids=["fp32", "tensor", "tensor-chunk256"])
+def test_debug_scores_counts_vs_oracle(ctx, oracle, shape):
     f = scenes.plain_frame(1)
     S = 512
     tr = oracle.sample_triples(f.seed, 0, S, f.n)
-    ids, poses, s32, cnt = ctx.debug_score_samples(f.uv, f.xyz, f.K, 4.0, tr, counts=True)
+    ids, poses, s32, cnt = ctx.debug_score_samples(f.uv, f.xyz, f.K, 4.0, tr, counts=True, shape=shape)
     xn = normalized(f)
     sq = sq_thr(f)
     o = oracle.ransac(xn, f.xyz, sq, dump=4 * S, replay=tr, force_samples=S, samples_per_round=S)
@@ -77,6 +83,31 @@ def test_scoring_bound_config_matches_oracle(ctx, oracle):
     assert d["ransac_inliers"] == info.ransac.count
     assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
     np.testing.assert_array_equal(inl, o["inliers"])
+
+
+def test_tensor_scoring_matches_oracle(ctx, oracle):
+    """The tensor-core scoring shape decides like the FP64 pipeline: the
+    scoring-bound frame (4096 samples, 15 % inliers, N = 20000) and a frame
+    that needs many rounds give the oracle's samples, selection and pose."""
+    f = scenes.scoring_frame(0)
+    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                               force_samples=4096, **TENSOR)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=4096, force_samples=4096, threads=8)
+    d, info = st.details, o["info"]
+    assert d["hypotheses"] == info.ransac.hypotheses
+    assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+    assert d["ransac_inliers"] == info.ransac.count
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+    np.testing.assert_array_equal(inl, o["inliers"])
+    f = scenes.make_frame(3000, 0.10, 1.0, 4242)
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
+                                               **TENSOR)
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
+    d, info = st.details, o["info"]
+    assert d["samples"] == info.ransac.samples and d["best_sample"] == info.ransac.best_sample
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
 
 
 def test_multi_round_termination_matches_oracle(ctx, oracle):

@@ -161,7 +161,7 @@ def lib() -> C.CDLL:
     L.tbr_server_drain.argtypes = [vp]
     L.tbr_server_destroy.argtypes = [vp]
     L.tbr_debug_score_samples.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_double, vp, C.c_int64, vp,
-                                          vp, vp, vp, C.c_int64, C.POINTER(C.c_int64)]
+                                          vp, vp, vp, C.c_int64, C.POINTER(C.c_int64), vp]
     L.tbr_msac_score_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int32, C.c_double, vp, vp, vp]
     for name in EXPORTS:
         fn = getattr(L, name)

@@ -171,7 +171,7 @@ class Context:
                                replay=None, force_samples: int = 0, skip_refine: bool = False,
                                honor_options: bool = False, hyp_per_thread: int = 0,
                                chunk_points: int = 0, max_total_samples: int = 0,
-                               stop_rule_x86_quirk: bool = False):
+                               stop_rule_x86_quirk: bool = False, points_per_iter: int = 0):
         """Returns (RansacStats_cuda, CameraPose_cuda, inliers uint8[N])."""
         x = _f64(points2D, 2)
         X = _f64(points3D, 3)
@@ -186,6 +186,7 @@ class Context:
         ext.max_total_samples = max_total_samples
         ext.seed = (seed or 0) & 0xFFFFFFFFFFFFFFFF
         ext.hyp_per_thread = hyp_per_thread
+        ext.points_per_iter = points_per_iter
         ext.chunk_points = chunk_points
         ext.stop_rule_x86_quirk = int(stop_rule_x86_quirk)
         rep = None
@@ -242,8 +243,16 @@ class Context:
                                                C.byref(st)))
         return CameraPose_cuda(q, t), st.as_dict()
 
-    def debug_score_samples(self, points2D, points3D, K, max_reproj_error, triples, counts=False):
-        """Per-hypothesis (ids, FP64 poses (H,3,4), FP32 scores in tau^2 units, counts or None)."""
+    def debug_score_samples(self, points2D, points3D, K, max_reproj_error, triples, counts=False, shape=None):
+        """Per-hypothesis (ids, FP64 poses (H,3,4), FP32 scores in tau^2 units, counts or None).
+        shape: a scoring shape (dict with hyp_per_thread, points_per_iter,
+        chunk_points) for the FP32 pass; default: the built-in one."""
+        ext = None
+        if shape:
+            ext = _lib.ExtOptionsC()
+            ext.hyp_per_thread = int(shape.get("hyp_per_thread", 0))
+            ext.points_per_iter = int(shape.get("points_per_iter", 0))
+            ext.chunk_points = int(shape.get("chunk_points", 0))
         x = _f64(points2D, 2)
         X = _f64(points3D, 3)
         tr = np.ascontiguousarray(np.asarray(triples, np.int32).reshape(-1, 3))
@@ -258,7 +267,7 @@ class Context:
             check(_lib.lib().tbr_debug_score_samples(
                 self._h, x.ctypes.data, X.ctypes.data, x.shape[0], Kc.ctypes.data, max_reproj_error,
                 tr.ctypes.data, tr.shape[0], ids.ctypes.data, poses.ctypes.data, s32.ctypes.data,
-                cnt.ctypes.data if counts else None, cap, C.byref(nh)))
+                cnt.ctypes.data if counts else None, cap, C.byref(nh), C.byref(ext) if ext else None))
         m = nh.value
         return ids[:m], poses[:m].reshape(m, 3, 4), s32[:m], (cnt[:m] if counts else None)
 

@@ -136,6 +136,10 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
             ext->hyp_per_thread == 8)
             o.hr = ext->hyp_per_thread;
         if (ext->points_per_iter == 2 || ext->points_per_iter == 4) o.pp = ext->points_per_iter;
+        if (ext->points_per_iter == kTcPP) {  // tensor-core scoring: 64 hypotheses per block
+            o.pp = kTcPP;
+            o.hr = 2;
+        }
         o.chunk_points = ext->chunk_points;
     }
     if (honor && ro) {
@@ -297,6 +301,7 @@ class Engine {
             TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sk[v], kScoreWarps * 32, 0));
             score_grid[v] = num_sms * std::max(occ, 1);
         }
+        TBR_CUDA(cudaFuncSetAttribute(k_score_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
         TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rescore, 256, 0));
         rescore_grid = num_sms * std::max(occ, 1);
         p3p_grid = num_sms * 8;
@@ -397,7 +402,8 @@ class Engine {
     // Scoring kernel variant: HR hypotheses per lane = 2*HP, PP points per iteration.
     void launch_score(const Pools &Q, int hr, int pp, cudaStream_t st) {
         const int threads = kScoreWarps * 32;
-        if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
+        if (hr == 2 && pp == kTcPP) k_score_tc<<<2 * num_sms, kTcThreads, kTcSmem, st>>>(Q);
+        else if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
         else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
         else if (hr == 6 && pp == 4) k_score<3, 4><<<score_grid[5], threads, 0, st>>>(Q);
         else if (hr == 6) k_score<3, 2><<<score_grid[4], threads, 0, st>>>(Q);
@@ -2346,12 +2352,21 @@ void tbr_server_destroy(tbr_server *s) {
 tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, const double *points3D,
                                    int64_t n, const double K[4], double max_reproj_error,
                                    const int32_t *triples, int64_t n_samples, int64_t *ids, double *poses,
-                                   float *scores32, int64_t *counts, int64_t cap, int64_t *n_hyp) {
+                                   float *scores32, int64_t *counts, int64_t cap, int64_t *n_hyp,
+                                   const tbr_ext_options *ext) {
     if (!ctx || !points2D || !points3D || !K || !triples || n < 3 || n_samples < 1)
         return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     RunOptions o;
+    if (ext) {  // scoring shape only
+        tbr_ext_options sh;
+        std::memset(&sh, 0, sizeof(sh));
+        sh.hyp_per_thread = ext->hyp_per_thread;
+        sh.points_per_iter = ext->points_per_iter;
+        sh.chunk_points = ext->chunk_points;
+        o = make_run_options(nullptr, nullptr, &sh);
+    }
     o.B = n_samples;
     o.force_samples = n_samples;
     o.skip_refine = 1;

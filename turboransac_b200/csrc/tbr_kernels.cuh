@@ -831,6 +831,370 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
     }
 }
 
+// ------------------------------------------------ tensor-core scoring --
+// The same filter with the projection on the 5th-generation tensor cores:
+// for a tile of 128 points and a block of 64 hypotheses, one tcgen05.mma
+// (kind::tf32, M = 128 points, N = 192 = z2 | z0 | z1 rows of the 64
+// hypotheses, K = 16) writes every z of the tile into tensor memory, and the
+// epilogue (one thread per point) does the reciprocal, the residuals, the
+// saturating r^2 and the sum per hypothesis. TF32 keeps 11 significant bits,
+// so each operand is split into a hi part (rounded to nearest TF32) and the
+// rounded remainder, and K carries all four cross terms
+//   A row (point)      = [Xh Yh Zh 1 | Xl Yl Zl 0 | Xh Yh Zh 1 | Xl Yl Zl 0]
+//   B row (hyp. row c) = [ch0..ch3   | ch0..ch2 0 | cl0..cl3   | cl0..cl2 0]
+// whose products are exact in FP32 and sum to c . [X 1] with an error of the
+// order of FP32 rounding (the remainders' own rounding is 2^-23 relative).
+// Selected by the scoring shape hyp_per_thread = 2, points_per_iter = 128.
+constexpr int kTcHyp = 64;        // hypotheses per item (HB at HR = 2)
+constexpr int kTcHalf = 32;       // hypotheses per MMA: two halves, each its own accumulator
+constexpr int kTcN = 3 * kTcHalf;  // MMA N: z2 | z0 | z1 rows of a half
+constexpr int kTcPts = 128;       // MMA M: points per tile
+constexpr int kTcThreads = 128;   // one thread per point row of the accumulators
+constexpr int kTcCols = 256;      // tensor-memory columns per CTA: half h at column 128 h
+constexpr int kTcPP = 128;        // points_per_iter value of the shape
+// At most two CTAs per SM (so that 2 x 256 columns never exceed the 512 of
+// an SM and tcgen05.alloc never waits): each asks for more than a third of
+// the SM's shared memory.
+constexpr int kTcSmem = 80 * 1024;
+constexpr uint32_t kTcIdesc = (1u << 4)                        // D: F32
+                              | (2u << 7) | (2u << 10)         // A, B: TF32, both K-major
+                              | ((uint32_t)(kTcN >> 3) << 17)  // N
+                              | ((uint32_t)(kTcPts >> 4) << 24);  // M
+// Shared-memory carve-up (bytes): two A tiles, B (the two halves' 96 rows
+// each), two point-staging buffers (two blocks each), the per-tile point
+// offsets (-x/tau, -y/tau), the cross-warp sums, then barriers and control.
+constexpr int kTcOffA = 0, kTcOffB = 16384, kTcOffPts = 28672, kTcOffNxy = 38912, kTcOffRed = 40960,
+              kTcOffCtl = 41984;
+
+// Byte offset of element (row r, k) of a K-major operand with 16 K values per
+// row, no swizzle: 8-row x 16-byte core matrices, the four K chunks of a row
+// group adjacent (leading byte offset 128), row groups 512 bytes apart.
+__device__ __forceinline__ int tc_off(int r, int k) {
+    return (((r >> 3) * 4 + (k >> 2)) * 128) + (r & 7) * 16 + (k & 3) * 4;
+}
+__device__ __forceinline__ uint64_t tc_desc(const void *smem) {
+    return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ float tf32_rn(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    const uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(kTcIdesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// B operand of hypothesis block hb: 192 rows, half h (hypotheses 32 h ..
+// 32 h + 31) in rows 96 h + [z2 x 32 | z0 x 32 | z1 x 32]. Thread t writes
+// the three rows of hypothesis hb * 64 + t (t < 64; zero past the count).
+__device__ __forceinline__ void tc_build_b(float *sB, const Pools &P, const FrameDev &f, int hb) {
+    const int t = threadIdx.x;
+    if (t >= kTcHyp) return;
+    const int i = hb * kTcHyp + t;
+    const float *src = P.hP32 + 12 * (f.hyp_base + i);
+    float c[12];
+#pragma unroll
+    for (int e = 0; e < 12; ++e) c[e] = i < f.hyp_count ? __ldg(src + e) : 0.0f;
+    char *rb = reinterpret_cast<char *>(sB);
+#pragma unroll
+    for (int comp = 0; comp < 3; ++comp) {
+        const int n = (t / kTcHalf) * kTcN + comp * kTcHalf + (t & (kTcHalf - 1));
+        const int cb = comp == 0 ? 8 : (comp == 1 ? 0 : 4);  // z2 | z0 | z1
+        float hi[4], lo[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            hi[k] = tf32_rn(c[cb + k]);
+            lo[k] = tf32_rn(c[cb + k] - hi[k]);
+        }
+        *reinterpret_cast<float4 *>(rb + tc_off(n, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<float4 *>(rb + tc_off(n, 4)) = make_float4(hi[0], hi[1], hi[2], 0.0f);
+        *reinterpret_cast<float4 *>(rb + tc_off(n, 8)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        *reinterpret_cast<float4 *>(rb + tc_off(n, 12)) = make_float4(lo[0], lo[1], lo[2], 0.0f);
+    }
+}
+
+// A tile of `cnt` valid points from a staging buffer (two blocks): thread t
+// writes row t and keeps the point's residual offsets for the epilogue.
+__device__ __forceinline__ void tc_build_a(float *sA, float2 *nxy, const float2 *stg, int cnt) {
+    const int t = threadIdx.x;
+    const bool v = t < cnt;
+    const float2 *tb = stg + (t >> 6) * kBlockFloat2;
+    const int j = t & (kSub - 1);
+    const float X = v ? tb[j].x : 0.0f, Y = v ? tb[kSub + j].x : 0.0f, Z = v ? tb[2 * kSub + j].x : 0.0f;
+    const float xh = tf32_rn(X), yh = tf32_rn(Y), zh = tf32_rn(Z);
+    const float xl = tf32_rn(X - xh), yl = tf32_rn(Y - yh), zl = tf32_rn(Z - zh);
+    const float one = v ? 1.0f : 0.0f;
+    char *ra = reinterpret_cast<char *>(sA);
+    *reinterpret_cast<float4 *>(ra + tc_off(t, 0)) = make_float4(xh, yh, zh, one);
+    *reinterpret_cast<float4 *>(ra + tc_off(t, 4)) = make_float4(xl, yl, zl, 0.0f);
+    *reinterpret_cast<float4 *>(ra + tc_off(t, 8)) = make_float4(xh, yh, zh, one);
+    *reinterpret_cast<float4 *>(ra + tc_off(t, 12)) = make_float4(xl, yl, zl, 0.0f);
+    nxy[t] = v ? make_float2(tb[3 * kSub + j].x, tb[4 * kSub + j].x) : make_float2(0.0f, 0.0f);
+}
+
+// Epilogue of one accumulator half: the thread's point against 32
+// hypotheses (two groups of 16), sums into acc[16 h .. 16 h + 15].
+__device__ __forceinline__ void tc_epilogue_half(uint32_t taddr, float2 o, bool v, uint64_t *acc) {
+    const uint64_t nx2 = f2pack(o.x, o.x), ny2 = f2pack(o.y, o.y);
+#pragma unroll
+    for (int gq = 0; gq < 2; ++gq) {
+        float z2[16], z0[16], z1[16];
+        tc_ld16(taddr + (uint32_t)(16 * gq), z2);
+        tc_ld16(taddr + (uint32_t)(kTcHalf + 16 * gq), z0);
+        tc_ld16(taddr + (uint32_t)(2 * kTcHalf + 16 * gq), z1);
+        tc_wait_ld();
+        if (v) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float ia = rcp_approx(fmaxf(z2[2 * q], kDepthFloor));
+                const float ib = rcp_approx(fmaxf(z2[2 * q + 1], kDepthFloor));
+                const uint64_t inv = f2pack(ia, ib);
+                const uint64_t r0 = f2fma(f2pack(z0[2 * q], z0[2 * q + 1]), inv, nx2);
+                const uint64_t r1 = f2fma(f2pack(z1[2 * q], z1[2 * q + 1]), inv, ny2);
+                const uint64_t r1s = f2mul(r1, r1);
+                float r0a, r0b, sa, sb;
+                f2unpack(r0, r0a, r0b);
+                f2unpack(r1s, sa, sb);
+                acc[8 * gq + q] = f2add(acc[8 * gq + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
+            }
+        }
+    }
+}
+
+// Sum of the lane's 64 accumulators over the warp's 32 lanes by recursive
+// halving: afterwards lane L holds the sums of hypotheses 2L and 2L + 1.
+__device__ __forceinline__ uint64_t tc_warp_reduce(uint64_t (&acc)[32]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16, m = 16; o > 0; o >>= 1, m >>= 1) {
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int j = 0; j < m; ++j) {
+            const uint64_t keep = up ? acc[m + j] : acc[j];
+            const uint64_t send = up ? acc[j] : acc[m + j];
+            acc[j] = f2add(keep, __shfl_xor_sync(0xffffffffu, send, o));
+        }
+    }
+    return acc[0];
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(Pools P) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    float *sA = reinterpret_cast<float *>(tc_smem + kTcOffA);             // [2][128 x 16]
+    float *sB = reinterpret_cast<float *>(tc_smem + kTcOffB);
+    float2 *sPts = reinterpret_cast<float2 *>(tc_smem + kTcOffPts);       // [2][2 blocks]
+    float2 *sNxy = reinterpret_cast<float2 *>(tc_smem + kTcOffNxy);       // [2][128]
+    float *red = reinterpret_cast<float *>(tc_smem + kTcOffRed);          // [4][64]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem + kTcOffCtl);  // staging 0, 1; MMA half 0, 1
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(tc_smem + kTcOffCtl + 32);
+    int *ctl = reinterpret_cast<int *>(tc_smem + kTcOffCtl + 48);
+    long long *run = reinterpret_cast<long long *>(tc_smem + kTcOffCtl + 64);
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (tid == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mbar_init(&bars[k], 1);
+        fence_mbar_init();
+    }
+    if (w == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
+                     "r"((uint32_t)kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);  // this warp's 32 lanes
+    uint32_t phs = 0u, phm = 0u;  // phase parities: bit s of staging buffer s / of MMA half s
+    const int64_t total = (int64_t)P.counters[kCScoreTotal];
+    const int64_t ctas = gridDim.x;
+    int cur_a = -1, cur_hb = -1;
+    int64_t run_next = 0, run_end = 0;
+    bool ok = true;
+    for (;;) {
+        if (run_next >= run_end) {
+            if (tid == 0) {
+                const int64_t done = (int64_t)*(volatile unsigned long long *)&P.counters[kCScoreNext];
+                const int64_t len = max((int64_t)1, min((int64_t)8, (total - done) / (4 * ctas)));
+                run[0] = (long long)atomicAdd(&P.counters[kCScoreNext], (unsigned long long)len);
+                run[1] = len;
+            }
+            __syncthreads();
+            const int64_t start = run[0], len = run[1];
+            __syncthreads();
+            if (start >= total) break;
+            run_next = start;
+            run_end = min(total, start + len);
+        }
+        const int64_t item = run_next++;
+        const int a = find_segment(P.item_prefix, P.n_active, item);
+        FrameDev &f = P.frames[P.active[a]];
+        const int64_t local = item - P.item_prefix[a];
+        const int nch = f.n_chunks;
+        const int hb = (int)(local / nch), ch = (int)(local % nch);
+        const int nh = f.hyp_count;
+        if (a != cur_a || hb != cur_hb) {  // every MMA of the previous item has completed
+            tc_build_b(sB, P, f, hb);
+            cur_a = a;
+            cur_hb = hb;
+        }
+        const int b0 = ch * f.chunk_blocks;
+        const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
+        const int ntiles = (b1 - b0 + 1) / 2;
+        const float2 *g = P.pts32 + (f.blk_off + b0) * kBlockFloat2;
+        auto tile_blocks = [&](int i) { return min(2, b1 - b0 - 2 * i); };
+        auto tile_cnt = [&](int i) {
+            return (int)min((int64_t)tile_blocks(i) * kSub, f.n - (int64_t)(b0 + 2 * i) * kSub);
+        };
+        auto fetch = [&](int i) {  // thread 0: points of tile i into staging buffer i & 1
+            fence_proxy_async();
+            bulk_load(sPts + (i & 1) * 2 * kBlockFloat2, g + (int64_t)(2 * i) * kBlockFloat2,
+                      (uint32_t)(tile_blocks(i) * kBlockBytes), &bars[i & 1]);
+        };
+        auto mma_half = [&](int i, int h) {  // thread 0: half h of tile i into accumulator half h
+            tc_fence_after();
+            const char *A = reinterpret_cast<const char *>(sA + (i & 1) * (kTcPts * 16));
+            const char *B = reinterpret_cast<const char *>(sB) + h * (kTcN / 8) * 512;
+            const uint32_t d = tmem + (uint32_t)(128 * h);
+            tc_mma(d, tc_desc(A), tc_desc(B), 0u);
+            tc_mma(d, tc_desc(A + 256), tc_desc(B + 256), 1u);
+            tc_commit(&bars[2 + h]);
+        };
+        // Thread 0 waits on barrier k (bounded); every thread learns the outcome.
+        auto wait_all = [&](int k, uint32_t parity) -> bool {
+            if (tid == 0) ctl[0] = mbar_wait(&bars[k], parity, kMaxPolls) ? 1 : 0;
+            __syncthreads();
+            const bool r = ctl[0] != 0;
+            __syncthreads();
+            return r;
+        };
+        // Tile i's A from its staging buffer (waits for the points).
+        auto build = [&](int i) -> bool {
+            const int s = i & 1;
+            if (!wait_all(s, (phs >> s) & 1u)) return false;
+            phs ^= 1u << s;
+            tc_build_a(sA + s * (kTcPts * 16), sNxy + s * kTcPts, sPts + s * 2 * kBlockFloat2, tile_cnt(i));
+            fence_proxy_async();  // the operands, written by threads, are read by the tensor core
+            return true;
+        };
+        if (tid == 0) {
+            fetch(0);
+            if (ntiles > 1) fetch(1);
+        }
+        uint64_t acc[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] = 0ull;
+        ok = build(0);
+        if (ok) {
+            __syncthreads();
+            if (tid == 0) {
+                mma_half(0, 0);
+                mma_half(0, 1);
+                if (ntiles > 2) fetch(2);
+            }
+        }
+        for (int i = 0; ok && i < ntiles; ++i) {
+            const int s = i & 1;
+            const bool more = i + 1 < ntiles;
+            // The next tile's A while this tile's MMAs run.
+            if (more && !build(i + 1)) {
+                ok = false;
+                break;
+            }
+            const int pt = tid;
+            const float2 o = sNxy[s * kTcPts + pt];
+            const bool v = pt < tile_cnt(i);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (!wait_all(2 + h, (phm >> h) & 1u)) {
+                    ok = false;
+                    break;
+                }
+                phm ^= 1u << h;
+                tc_fence_after();
+                tc_epilogue_half(trow + (uint32_t)(128 * h), o, v, acc + 16 * h);
+                tc_fence_before();
+                __syncthreads();  // accumulator half h is free
+                if (tid == 0 && more) {
+                    mma_half(i + 1, h);
+                    if (h == 0 && i + 3 < ntiles) fetch(i + 3);
+                }
+            }
+        }
+        if (!ok) break;
+        // Chunk partials: warp sums, then the four warps in fixed order.
+        {
+            const uint64_t pr = tc_warp_reduce(acc);
+            float lo, hi;
+            f2unpack(pr, lo, hi);
+            red[w * kTcHyp + 2 * lane] = lo;
+            red[w * kTcHyp + 2 * lane + 1] = hi;
+        }
+        __syncthreads();
+        float *part = P.part + f.part_base;
+        if (tid < kTcHyp) {
+            const int i = hb * kTcHyp + tid;
+            const float s4 = ((red[tid] + red[kTcHyp + tid]) + red[2 * kTcHyp + tid]) + red[3 * kTcHyp + tid];
+            if (i < nh) part[(int64_t)i * nch + ch] = s4;
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) ctl[2] = (int)atomicAdd(&P.hb_arrive[f.hb_base + hb], 1u);
+        __syncthreads();
+        if (ctl[2] == nch - 1 && tid < kTcHyp) {
+            __threadfence();
+            const int i = hb * kTcHyp + tid;
+            if (i < nh) {
+                float s = 0.0f;
+                for (int q = 0; q < nch; ++q) s += __ldcg(part + (int64_t)i * nch + q);
+                P.hS32[f.hyp_base + i] = s;
+                const int64_t sample = P.hId[f.hyp_base + i] >> 2;
+                const int64_t r = (sample - f.step_first) / f.step_div;
+                const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | (unsigned)i;
+                atomicMin(&f.round_min[r], key);
+            }
+        }
+        __syncthreads();  // red and ctl are reused by the next item
+    }
+    if (!ok) {
+        // Give up: record it and let the copies and MMAs in flight land
+        // (bounded) before the tensor memory is released.
+        if (tid == 0) {
+            flag_error(P, kErrTimeout);
+#pragma unroll 1
+            for (int k = 0; k < 2; ++k) {
+                mbar_wait(&bars[k], (phs >> k) & 1u, kMaxPolls);
+                mbar_wait(&bars[2 + k], (phm >> k) & 1u, kMaxPolls);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcCols));
+}
+
 // ---------------------------------------------------------- candidates -----
 // Candidates for the exact FP64 re-rank: every hypothesis whose FP32 score is
 // within a band of the running minimum (over this step's rounds so far and the
