@@ -105,7 +105,9 @@ typedef struct tbr_ext_options {
      * there and x86 yields INT_MIN, ending the loop after one round.
      * 0 (default): saturate -- keep sampling up to the cap; 1: reproduce x86. */
     int32_t stop_rule_x86_quirk;
-    int32_t points_per_iter;      /* scoring tile: 0 = auto, else 2 or 4 points per inner step */
+    int32_t points_per_iter;      /* scoring tile: 0 = auto, else 2 or 4 points per inner step;
+                                     128 = tensor-core scoring (tcgen05 MMA over 128-point tiles,
+                                     64 hypotheses per block; implies hyp_per_thread = 2) */
 } tbr_ext_options;
 
 /* Results of one estimate. The reference returns RansacStats_cuda unfilled except
