@@ -107,7 +107,7 @@ typedef struct tbr_ext_options {
     int32_t stop_rule_x86_quirk;
     int32_t points_per_iter;      /* scoring tile: 0 = auto, else 2 or 4 points per inner step;
                                      128 = tensor-core scoring (tcgen05 MMA over 128-point tiles,
-                                     64 hypotheses per block; implies hyp_per_thread = 2) */
+                                     32 hypotheses per block; overrides hyp_per_thread) */
 } tbr_ext_options;
 
 /* Results of one estimate. The reference returns RansacStats_cuda unfilled except
@@ -239,9 +239,11 @@ tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max,
                              uint64_t *pairs_scored);
 
 /* Scoring-shape autotuner (no reference counterpart). Times the batch's graph
- * `repeats` times under each candidate shape -- hypotheses per warp block
+ * `repeats` times under each candidate shape -- FP32: hypotheses per warp block
  * (32 x hyp_per_thread: 64, 128, 192, 256), points per iteration (2, 4) and points
- * per work-item tile (0 = sized from the step's work, 256, 512, 1024, 2048) --
+ * per work-item tile (0 = sized from the step's work, 256, 512, 1024, 2048);
+ * tensor cores: points_per_iter = 128 (32 hypotheses per block, reported as
+ * hyp_per_thread = 1) with tiles 0 and 8192; 32 candidates in all --
  * and keeps the fastest for later tbr_batch_run calls. The shape changes only
  * the order of FP32 partial sums inside the filter; every candidate within the
  * filter band is re-scored in FP64, so results do not depend on it. entries

@@ -123,7 +123,8 @@ def test_autotune_keeps_results(ctx):
     b.sync()
     before = b.results()
     best, tried = b.autotune(repeats=1)
-    assert len(tried) == 30 and all(t["ms"] > 0 for t in tried)
+    assert len(tried) == 32 and all(t["ms"] > 0 for t in tried)
+    assert sum(t["points_per_iter"] == 128 for t in tried) == 2  # the tensor-core shape is a candidate
     assert best["ms"] == min(t["ms"] for t in tried)
     b.run()
     b.sync()
@@ -274,16 +275,16 @@ def test_staggered_admission_matches_resident_run(ctx):
 
 
 def test_tensor_scoring_batch_matches_fp32_shape(ctx):
-    """A batch scored on the tensor cores (hyp_per_thread=2, points_per_iter=128,
-    several point-chunk sizes) gives the FP32 shape's results: the FP64 re-rank
-    decides, the filter only has to keep the best within its band."""
+    """A batch scored on the tensor cores (points_per_iter=128, several point-chunk
+    sizes) gives the FP32 shape's results: the FP64 re-rank decides, the filter
+    only has to keep the best within its band."""
     fr = mixed_frames() + [scenes.make_frame(30000, 0.15, 1.0, 9300), scenes.make_frame(700, 0.5, 2.0, 9301)]
     b = Batch(ctx, fr, RO)
     b.run()
     b.sync()
     ref = b.results()
     b.close()
-    for chunk in (0, 256, 2048):
+    for chunk in (0, 256, 2048, 8192):
         b = Batch(ctx, fr, RO, hyp_per_thread=2, points_per_iter=128, chunk_points=chunk)
         for _ in range(2):
             b.run()

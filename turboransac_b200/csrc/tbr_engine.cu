@@ -136,9 +136,9 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
             ext->hyp_per_thread == 8)
             o.hr = ext->hyp_per_thread;
         if (ext->points_per_iter == 2 || ext->points_per_iter == 4) o.pp = ext->points_per_iter;
-        if (ext->points_per_iter == kTcPP) {  // tensor-core scoring: 64 hypotheses per block
+        if (ext->points_per_iter == kTcPP) {  // tensor-core scoring: 32 hypotheses per block
             o.pp = kTcPP;
-            o.hr = 2;
+            o.hr = 1;
         }
         o.chunk_points = ext->chunk_points;
     }
@@ -402,7 +402,7 @@ class Engine {
     // Scoring kernel variant: HR hypotheses per lane = 2*HP, PP points per iteration.
     void launch_score(const Pools &Q, int hr, int pp, cudaStream_t st) {
         const int threads = kScoreWarps * 32;
-        if (hr == 2 && pp == kTcPP) k_score_tc<<<2 * num_sms, kTcThreads, kTcSmem, st>>>(Q);
+        if (pp == kTcPP) k_score_tc<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);
         else if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
         else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
         else if (hr == 6 && pp == 4) k_score<3, 4><<<score_grid[5], threads, 0, st>>>(Q);
@@ -1727,8 +1727,18 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
     struct Shape {
         int hr, pp;
     };
-    const Shape shapes[6] = {{2, 4}, {4, 2}, {4, 4}, {6, 2}, {6, 4}, {8, 2}};  // the compiled scoring variants
+    // The compiled FP32 scoring variants x point-chunk sizes, then the
+    // tensor-core shape (32 hypotheses per block) with planned and long chunks.
+    const Shape shapes[6] = {{2, 4}, {4, 2}, {4, 4}, {6, 2}, {6, 4}, {8, 2}};
     const int chunks[5] = {0, 256, 512, 1024, 2048};
+    struct Cand {
+        int hr, pp, chunk;
+    };
+    std::vector<Cand> cands;
+    for (const Shape &sh : shapes)
+        for (int chunk : chunks) cands.push_back({sh.hr, sh.pp, chunk});
+    cands.push_back({1, kTcPP, 0});
+    cands.push_back({1, kTcPP, 8192});
     std::vector<tbr_tune_entry> tried;
     cudaEvent_t t0, t1;
     TBR_CUDA(cudaEventCreate(&t0));
@@ -1740,11 +1750,11 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
         return E.build_loop_graph(b->Q, n, hr, b->d_init, g, x);
     };
     tbr_status st = TBR_OK;
-    for (const Shape &sh : shapes) {
-        for (int chunk : chunks) {
+    for (const Cand &cd : cands) {
+        {
             cudaGraph_t g = nullptr;
             cudaGraphExec_t x = nullptr;
-            if (!apply(sh.hr, sh.pp, chunk, &g, &x)) {
+            if (!apply(cd.hr, cd.pp, cd.chunk, &g, &x)) {
                 st = fail(TBR_ERR_CUDA, "autotune graph capture failed");
                 break;
             }
@@ -1766,7 +1776,7 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
                 st = fail(TBR_ERR_INTERNAL, "device error during autotune");
                 break;
             }
-            tried.push_back({sh.hr, sh.pp, chunk, 0, (double)ms / repeats});
+            tried.push_back({cd.hr, cd.pp, cd.chunk, 0, (double)ms / repeats});
         }
         if (st) break;
     }

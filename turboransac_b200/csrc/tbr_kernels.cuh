@@ -845,26 +845,23 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
 // whose products are exact in FP32 and sum to c . [X 1] with an error of the
 // order of FP32 rounding (the remainders' own rounding is 2^-23 relative).
 // Selected by the scoring shape hyp_per_thread = 2, points_per_iter = 128.
-constexpr int kTcHyp = 64;        // hypotheses per item (HB at HR = 2)
-constexpr int kTcHalf = 32;       // hypotheses per MMA: two halves, each its own accumulator
-constexpr int kTcN = 3 * kTcHalf;  // MMA N: z2 | z0 | z1 rows of a half
+constexpr int kTcHyp = 32;        // hypotheses per item (HB at HR = 1)
+constexpr int kTcN = 3 * kTcHyp;   // MMA N: z2 | z0 | z1 rows of the block
 constexpr int kTcPts = 128;       // MMA M: points per tile
-constexpr int kTcThreads = 128;   // one thread per point row of the accumulators
-constexpr int kTcCols = 256;      // tensor-memory columns per CTA: half h at column 128 h
+constexpr int kTcThreads = 128;   // one thread per point row of the accumulator
+constexpr int kTcCols = 128;      // tensor-memory columns per CTA (four CTAs per SM at most)
 constexpr int kTcPP = 128;        // points_per_iter value of the shape
-// At most two CTAs per SM (so that 2 x 256 columns never exceed the 512 of
-// an SM and tcgen05.alloc never waits): each asks for more than a third of
-// the SM's shared memory.
-constexpr int kTcSmem = 80 * 1024;
+// At most four CTAs per SM (so that 4 x 128 columns never exceed the 512 of an
+// SM and tcgen05.alloc never waits): each asks for more than a fifth of the
+// SM's shared memory. Four CTAs give the epilogue 16 warps per SM.
+constexpr int kTcSmem = 48 * 1024;
 constexpr uint32_t kTcIdesc = (1u << 4)                        // D: F32
                               | (2u << 7) | (2u << 10)         // A, B: TF32, both K-major
                               | ((uint32_t)(kTcN >> 3) << 17)  // N
                               | ((uint32_t)(kTcPts >> 4) << 24);  // M
-// Shared-memory carve-up (bytes): two A tiles, B (the two halves' 96 rows
-// each), two point-staging buffers (two blocks each), the per-tile point
-// offsets (-x/tau, -y/tau), the cross-warp sums, then barriers and control.
-constexpr int kTcOffA = 0, kTcOffB = 16384, kTcOffPts = 28672, kTcOffNxy = 38912, kTcOffRed = 40960,
-              kTcOffCtl = 41984;
+// Shared-memory carve-up (bytes): A, B, two point-staging buffers (two
+// blocks each), the cross-warp sums, then barriers and control words.
+constexpr int kTcOffA = 0, kTcOffB = 8192, kTcOffPts = 14336, kTcOffRed = 24576, kTcOffCtl = 25088;
 
 // Byte offset of element (row r, k) of a K-major operand with 16 K values per
 // row, no swizzle: 8-row x 16-byte core matrices, the four K chunks of a row
@@ -906,9 +903,8 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 }
 __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// B operand of hypothesis block hb: 192 rows, half h (hypotheses 32 h ..
-// 32 h + 31) in rows 96 h + [z2 x 32 | z0 x 32 | z1 x 32]. Thread t writes
-// the three rows of hypothesis hb * 64 + t (t < 64; zero past the count).
+// B operand of hypothesis block hb: thread t < 32 writes the z2, z0 and z1 rows
+// (t, 32 + t, 64 + t) of hypothesis hb * 32 + t (zero rows past the count).
 __device__ __forceinline__ void tc_build_b(float *sB, const Pools &P, const FrameDev &f, int hb) {
     const int t = threadIdx.x;
     if (t >= kTcHyp) return;
@@ -920,7 +916,7 @@ __device__ __forceinline__ void tc_build_b(float *sB, const Pools &P, const Fram
     char *rb = reinterpret_cast<char *>(sB);
 #pragma unroll
     for (int comp = 0; comp < 3; ++comp) {
-        const int n = (t / kTcHalf) * kTcN + comp * kTcHalf + (t & (kTcHalf - 1));
+        const int n = comp * kTcHyp + t;
         const int cb = comp == 0 ? 8 : (comp == 1 ? 0 : 4);  // z2 | z0 | z1
         float hi[4], lo[4];
 #pragma unroll
@@ -935,86 +931,21 @@ __device__ __forceinline__ void tc_build_b(float *sB, const Pools &P, const Fram
     }
 }
 
-// A tile of `cnt` valid points from a staging buffer (two blocks): thread t
-// writes row t and keeps the point's residual offsets for the epilogue.
-__device__ __forceinline__ void tc_build_a(float *sA, float2 *nxy, const float2 *stg, int cnt) {
-    const int t = threadIdx.x;
-    const bool v = t < cnt;
-    const float2 *tb = stg + (t >> 6) * kBlockFloat2;
-    const int j = t & (kSub - 1);
-    const float X = v ? tb[j].x : 0.0f, Y = v ? tb[kSub + j].x : 0.0f, Z = v ? tb[2 * kSub + j].x : 0.0f;
-    const float xh = tf32_rn(X), yh = tf32_rn(Y), zh = tf32_rn(Z);
-    const float xl = tf32_rn(X - xh), yl = tf32_rn(Y - yh), zl = tf32_rn(Z - zh);
-    const float one = v ? 1.0f : 0.0f;
-    char *ra = reinterpret_cast<char *>(sA);
-    *reinterpret_cast<float4 *>(ra + tc_off(t, 0)) = make_float4(xh, yh, zh, one);
-    *reinterpret_cast<float4 *>(ra + tc_off(t, 4)) = make_float4(xl, yl, zl, 0.0f);
-    *reinterpret_cast<float4 *>(ra + tc_off(t, 8)) = make_float4(xh, yh, zh, one);
-    *reinterpret_cast<float4 *>(ra + tc_off(t, 12)) = make_float4(xl, yl, zl, 0.0f);
-    nxy[t] = v ? make_float2(tb[3 * kSub + j].x, tb[4 * kSub + j].x) : make_float2(0.0f, 0.0f);
-}
-
-// Epilogue of one accumulator half: the thread's point against 32
-// hypotheses (two groups of 16), sums into acc[16 h .. 16 h + 15].
-__device__ __forceinline__ void tc_epilogue_half(uint32_t taddr, float2 o, bool v, uint64_t *acc) {
-    const uint64_t nx2 = f2pack(o.x, o.x), ny2 = f2pack(o.y, o.y);
-#pragma unroll
-    for (int gq = 0; gq < 2; ++gq) {
-        float z2[16], z0[16], z1[16];
-        tc_ld16(taddr + (uint32_t)(16 * gq), z2);
-        tc_ld16(taddr + (uint32_t)(kTcHalf + 16 * gq), z0);
-        tc_ld16(taddr + (uint32_t)(2 * kTcHalf + 16 * gq), z1);
-        tc_wait_ld();
-        if (v) {
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float ia = rcp_approx(fmaxf(z2[2 * q], kDepthFloor));
-                const float ib = rcp_approx(fmaxf(z2[2 * q + 1], kDepthFloor));
-                const uint64_t inv = f2pack(ia, ib);
-                const uint64_t r0 = f2fma(f2pack(z0[2 * q], z0[2 * q + 1]), inv, nx2);
-                const uint64_t r1 = f2fma(f2pack(z1[2 * q], z1[2 * q + 1]), inv, ny2);
-                const uint64_t r1s = f2mul(r1, r1);
-                float r0a, r0b, sa, sb;
-                f2unpack(r0, r0a, r0b);
-                f2unpack(r1s, sa, sb);
-                acc[8 * gq + q] = f2add(acc[8 * gq + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
-            }
-        }
-    }
-}
-
-// Sum of the lane's 64 accumulators over the warp's 32 lanes by recursive
-// halving: afterwards lane L holds the sums of hypotheses 2L and 2L + 1.
-__device__ __forceinline__ uint64_t tc_warp_reduce(uint64_t (&acc)[32]) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int o = 16, m = 16; o > 0; o >>= 1, m >>= 1) {
-        const bool up = (lane & o) != 0;
-#pragma unroll
-        for (int j = 0; j < m; ++j) {
-            const uint64_t keep = up ? acc[m + j] : acc[j];
-            const uint64_t send = up ? acc[j] : acc[m + j];
-            acc[j] = f2add(keep, __shfl_xor_sync(0xffffffffu, send, o));
-        }
-    }
-    return acc[0];
-}
-
-__global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(Pools P) {
+__global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    float *sA = reinterpret_cast<float *>(tc_smem + kTcOffA);             // [2][128 x 16]
+    float *sA = reinterpret_cast<float *>(tc_smem + kTcOffA);
     float *sB = reinterpret_cast<float *>(tc_smem + kTcOffB);
-    float2 *sPts = reinterpret_cast<float2 *>(tc_smem + kTcOffPts);       // [2][2 blocks]
-    float2 *sNxy = reinterpret_cast<float2 *>(tc_smem + kTcOffNxy);       // [2][128]
-    float *red = reinterpret_cast<float *>(tc_smem + kTcOffRed);          // [4][64]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem + kTcOffCtl);  // staging 0, 1; MMA half 0, 1
+    float2 *sPts = reinterpret_cast<float2 *>(tc_smem + kTcOffPts);  // 2 buffers x 2 staging blocks
+    float *red = reinterpret_cast<float *>(tc_smem + kTcOffRed);      // [4][32]
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem + kTcOffCtl);  // points 0, 1; MMA
     uint32_t *tslot = reinterpret_cast<uint32_t *>(tc_smem + kTcOffCtl + 32);
     int *ctl = reinterpret_cast<int *>(tc_smem + kTcOffCtl + 48);
     long long *run = reinterpret_cast<long long *>(tc_smem + kTcOffCtl + 64);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid == 0) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) mbar_init(&bars[k], 1);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
     if (w == 0) {
@@ -1027,7 +958,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(Pools P) {
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);  // this warp's 32 lanes
-    uint32_t phs = 0u, phm = 0u;  // phase parities: bit s of staging buffer s / of MMA half s
+    uint32_t ph0 = 0, ph1 = 0, phm = 0;
     const int64_t total = (int64_t)P.counters[kCScoreTotal];
     const int64_t ctas = gridDim.x;
     int cur_a = -1, cur_hb = -1;
@@ -1065,92 +996,115 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(Pools P) {
         const int ntiles = (b1 - b0 + 1) / 2;
         const float2 *g = P.pts32 + (f.blk_off + b0) * kBlockFloat2;
         auto tile_blocks = [&](int i) { return min(2, b1 - b0 - 2 * i); };
-        auto tile_cnt = [&](int i) {
-            return (int)min((int64_t)tile_blocks(i) * kSub, f.n - (int64_t)(b0 + 2 * i) * kSub);
-        };
-        auto fetch = [&](int i) {  // thread 0: points of tile i into staging buffer i & 1
-            fence_proxy_async();
-            bulk_load(sPts + (i & 1) * 2 * kBlockFloat2, g + (int64_t)(2 * i) * kBlockFloat2,
-                      (uint32_t)(tile_blocks(i) * kBlockBytes), &bars[i & 1]);
-        };
-        auto mma_half = [&](int i, int h) {  // thread 0: half h of tile i into accumulator half h
-            tc_fence_after();
-            const char *A = reinterpret_cast<const char *>(sA + (i & 1) * (kTcPts * 16));
-            const char *B = reinterpret_cast<const char *>(sB) + h * (kTcN / 8) * 512;
-            const uint32_t d = tmem + (uint32_t)(128 * h);
-            tc_mma(d, tc_desc(A), tc_desc(B), 0u);
-            tc_mma(d, tc_desc(A + 256), tc_desc(B + 256), 1u);
-            tc_commit(&bars[2 + h]);
-        };
-        // Thread 0 waits on barrier k (bounded); every thread learns the outcome.
-        auto wait_all = [&](int k, uint32_t parity) -> bool {
-            if (tid == 0) ctl[0] = mbar_wait(&bars[k], parity, kMaxPolls) ? 1 : 0;
-            __syncthreads();
-            const bool r = ctl[0] != 0;
-            __syncthreads();
-            return r;
-        };
-        // Tile i's A from its staging buffer (waits for the points).
-        auto build = [&](int i) -> bool {
-            const int s = i & 1;
-            if (!wait_all(s, (phs >> s) & 1u)) return false;
-            phs ^= 1u << s;
-            tc_build_a(sA + s * (kTcPts * 16), sNxy + s * kTcPts, sPts + s * 2 * kBlockFloat2, tile_cnt(i));
-            fence_proxy_async();  // the operands, written by threads, are read by the tensor core
-            return true;
-        };
         if (tid == 0) {
-            fetch(0);
-            if (ntiles > 1) fetch(1);
+            fence_proxy_async();
+            bulk_load(sPts, g, (uint32_t)(tile_blocks(0) * kBlockBytes), &bars[0]);
+            if (ntiles > 1)
+                bulk_load(sPts + 2 * kBlockFloat2, g + 2 * kBlockFloat2, (uint32_t)(tile_blocks(1) * kBlockBytes),
+                          &bars[1]);
         }
-        uint64_t acc[32];
+        uint64_t acc[16];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) acc[j] = 0ull;
-        ok = build(0);
-        if (ok) {
-            __syncthreads();
-            if (tid == 0) {
-                mma_half(0, 0);
-                mma_half(0, 1);
-                if (ntiles > 2) fetch(2);
-            }
-        }
-        for (int i = 0; ok && i < ntiles; ++i) {
+        for (int j = 0; j < 16; ++j) acc[j] = 0ull;
+        // Each tile's points are waited for by thread 0 before the barrier that
+        // ends the previous tile (the first tile's here).
+        if (tid == 0) ctl[0] = mbar_wait(&bars[0], ph0, kMaxPolls) ? 1 : 0;
+        __syncthreads();
+        for (int i = 0; i < ntiles; ++i) {
             const int s = i & 1;
-            const bool more = i + 1 < ntiles;
-            // The next tile's A while this tile's MMAs run.
-            if (more && !build(i + 1)) {
+            if (!ctl[0]) {
                 ok = false;
                 break;
             }
-            const int pt = tid;
-            const float2 o = sNxy[s * kTcPts + pt];
-            const bool v = pt < tile_cnt(i);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (!wait_all(2 + h, (phm >> h) & 1u)) {
-                    ok = false;
-                    break;
-                }
-                phm ^= 1u << h;
+            if (s) ph1 ^= 1u; else ph0 ^= 1u;
+            // A row of this thread's point.
+            const int64_t p0 = (int64_t)(b0 + 2 * i) * kSub;
+            const int cnt = (int)min((int64_t)tile_blocks(i) * kSub, f.n - p0);
+            const bool v = tid < cnt;
+            const float2 *tb = sPts + s * 2 * kBlockFloat2 + (tid >> 6) * kBlockFloat2;
+            const int j = tid & (kSub - 1);
+            const float X = v ? tb[j].x : 0.0f, Y = v ? tb[kSub + j].x : 0.0f, Z = v ? tb[2 * kSub + j].x : 0.0f;
+            const float NX = v ? tb[3 * kSub + j].x : 0.0f, NY = v ? tb[4 * kSub + j].x : 0.0f;
+            {
+                const float xh = tf32_rn(X), yh = tf32_rn(Y), zh = tf32_rn(Z);
+                const float xl = tf32_rn(X - xh), yl = tf32_rn(Y - yh), zl = tf32_rn(Z - zh);
+                const float one = v ? 1.0f : 0.0f;
+                char *ra = reinterpret_cast<char *>(sA);
+                *reinterpret_cast<float4 *>(ra + tc_off(tid, 0)) = make_float4(xh, yh, zh, one);
+                *reinterpret_cast<float4 *>(ra + tc_off(tid, 4)) = make_float4(xl, yl, zl, 0.0f);
+                *reinterpret_cast<float4 *>(ra + tc_off(tid, 8)) = make_float4(xh, yh, zh, one);
+                *reinterpret_cast<float4 *>(ra + tc_off(tid, 12)) = make_float4(xl, yl, zl, 0.0f);
+            }
+            fence_proxy_async();  // the operands, written by threads, are read by the tensor core
+            __syncthreads();
+            if (tid == 0) {
                 tc_fence_after();
-                tc_epilogue_half(trow + (uint32_t)(128 * h), o, v, acc + 16 * h);
-                tc_fence_before();
-                __syncthreads();  // accumulator half h is free
-                if (tid == 0 && more) {
-                    mma_half(i + 1, h);
-                    if (h == 0 && i + 3 < ntiles) fetch(i + 3);
+                tc_mma(tmem, tc_desc(sA), tc_desc(sB), 0u);
+                tc_mma(tmem, tc_desc(reinterpret_cast<char *>(sA) + 256), tc_desc(reinterpret_cast<char *>(sB) + 256),
+                       1u);
+                tc_commit(&bars[2]);
+                if (i + 2 < ntiles) {  // the staging buffer is free again
+                    fence_proxy_async();
+                    bulk_load(sPts + s * 2 * kBlockFloat2, g + (int64_t)(2 * (i + 2)) * kBlockFloat2,
+                              (uint32_t)(tile_blocks(i + 2) * kBlockBytes), &bars[s]);
+                }
+                ctl[1] = mbar_wait(&bars[2], phm, kMaxPolls) ? 1 : 0;
+            }
+            __syncthreads();
+            if (!ctl[1]) {
+                ok = false;
+                break;
+            }
+            phm ^= 1u;
+            tc_fence_after();
+            const uint64_t nx2 = f2pack(NX, NX), ny2 = f2pack(NY, NY);
+#pragma unroll
+            for (int gq = 0; gq < 2; ++gq) {
+                float z2[16], z0[16], z1[16];
+                tc_ld16(trow + (uint32_t)(16 * gq), z2);
+                tc_ld16(trow + (uint32_t)(kTcHyp + 16 * gq), z0);
+                tc_ld16(trow + (uint32_t)(2 * kTcHyp + 16 * gq), z1);
+                tc_wait_ld();
+                if (v) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float ia = rcp_approx(fmaxf(z2[2 * q], kDepthFloor));
+                        const float ib = rcp_approx(fmaxf(z2[2 * q + 1], kDepthFloor));
+                        const uint64_t inv = f2pack(ia, ib);
+                        const uint64_t r0 = f2fma(f2pack(z0[2 * q], z0[2 * q + 1]), inv, nx2);
+                        const uint64_t r1 = f2fma(f2pack(z1[2 * q], z1[2 * q + 1]), inv, ny2);
+                        const uint64_t r1s = f2mul(r1, r1);
+                        float r0a, r0b, sa, sb;
+                        f2unpack(r0, r0a, r0b);
+                        f2unpack(r1s, sa, sb);
+                        acc[8 * gq + q] = f2add(acc[8 * gq + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
+                    }
                 }
             }
+            tc_fence_before();
+            if (tid == 0 && i + 1 < ntiles) ctl[0] = mbar_wait(&bars[s ^ 1], s ? ph0 : ph1, kMaxPolls) ? 1 : 0;
+            __syncthreads();  // the accumulator and the A tile are free for the next tile
         }
         if (!ok) break;
-        // Chunk partials: warp sums, then the four warps in fixed order.
-        {
-            const uint64_t pr = tc_warp_reduce(acc);
+        // Chunk partials: the warp's 32 hypotheses over its 32 points (lanes
+        // 2p, 2p + 1 end with hypotheses 2p, 2p + 1), then the four warps in
+        // fixed order.
+#pragma unroll
+        for (int o = 16, m = 8; o >= 2; o >>= 1, m >>= 1) {
+            const bool up = (lane & o) != 0;
+#pragma unroll
+            for (int jj = 0; jj < m; ++jj) {
+                const uint64_t keep = up ? acc[m + jj] : acc[jj];
+                const uint64_t send = up ? acc[jj] : acc[m + jj];
+                acc[jj] = f2add(keep, __shfl_xor_sync(0xffffffffu, send, o));
+            }
+        }
+        acc[0] = f2add(acc[0], __shfl_xor_sync(0xffffffffu, acc[0], 1));
+        if ((lane & 1) == 0) {
             float lo, hi;
-            f2unpack(pr, lo, hi);
-            red[w * kTcHyp + 2 * lane] = lo;
-            red[w * kTcHyp + 2 * lane + 1] = hi;
+            f2unpack(acc[0], lo, hi);
+            red[w * kTcHyp + lane] = lo;
+            red[w * kTcHyp + lane + 1] = hi;
         }
         __syncthreads();
         float *part = P.part + f.part_base;
@@ -1179,15 +1133,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_score_tc(Pools P) {
         __syncthreads();  // red and ctl are reused by the next item
     }
     if (!ok) {
-        // Give up: record it and let the copies and MMAs in flight land
+        // Give up: record it and let the copies and the MMA in flight land
         // (bounded) before the tensor memory is released.
         if (tid == 0) {
             flag_error(P, kErrTimeout);
-#pragma unroll 1
-            for (int k = 0; k < 2; ++k) {
-                mbar_wait(&bars[k], (phs >> k) & 1u, kMaxPolls);
-                mbar_wait(&bars[2 + k], (phm >> k) & 1u, kMaxPolls);
-            }
+            mbar_wait(&bars[0], ph0, kMaxPolls);
+            mbar_wait(&bars[1], ph1, kMaxPolls);
+            mbar_wait(&bars[2], phm, kMaxPolls);
         }
     }
     tc_fence_before();
