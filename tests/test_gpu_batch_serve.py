@@ -297,3 +297,21 @@ def test_tensor_scoring_batch_matches_fp32_shape(ctx):
                 np.testing.assert_array_equal(r1["q"], r0["q"])
                 np.testing.assert_array_equal(r1["t"], r0["t"])
         b.close()
+
+
+def test_server_tensor_scoring_shape_matches_plain(ctx):
+    """The server running the tensor-core scoring shape (an autotuner result it
+    can be handed) returns the plain call's results."""
+    fr = mixed_frames()
+    ref = [plain(ctx, f) for f in fr]
+    srv = Server(ctx, budget_bytes=2 << 30, max_slots=64,
+                 scoring_shape={"hyp_per_thread": 1, "points_per_iter": 128, "chunk_points": 8192})
+    ids = {srv.submit(f): i for i, f in enumerate(fr)}
+    srv.drain()
+    got = srv.poll()
+    srv.close()
+    assert len(got) == len(fr)
+    for r in got:
+        d, pose = ref[ids[r["id"]]]
+        assert r["status"] == 0
+        same(r, r["q"], r["t"], d, pose)
