@@ -310,32 +310,42 @@ def _f64c(a):
     return a if (a.dtype == np.float64 and a.flags.c_contiguous) else np.ascontiguousarray(a, np.float64)
 
 
-def _ptr(a):
-    """Address of a contiguous array's first element (ctypes' buffer route is
-    the cheapest per array; read-only and empty arrays take numpy's)."""
-    try:
-        return C.addressof(C.c_char.from_buffer(a))
-    except (TypeError, ValueError, BufferError):
-        return a.ctypes.data
-
-
 _U64 = 0xFFFFFFFFFFFFFFFF
+
+
+_F64 = np.dtype(np.float64)
 
 
 def _frame_descs(frames, seeds=None, max_reproj_error=0.0):
     """tbr_frame_desc entries for the frames' float64 arrays: (pointer for the C
-    call, objects to keep alive until it returns)."""
+    call, objects to keep alive until it returns). One pass over the frames
+    (this runs once per batch call, so its per-frame cost counts)."""
     m = len(frames)
-    uvs = [_f64c(fr.uv) for fr in frames]
-    xyzs = [_f64c(fr.xyz) for fr in frames]
-    for i, (uv, X) in enumerate(zip(uvs, xyzs)):
-        if uv.ndim != 2 or uv.shape[1] != 2 or X.ndim != 2 or X.shape[1] != 3 or uv.shape[0] != X.shape[0]:
+    keep = []
+    p2, p3, ns, Ks = [0] * m, [0] * m, [0] * m, [None] * m
+    from_buffer, addressof = C.c_char.from_buffer, C.addressof
+    for i, fr in enumerate(frames):
+        u, x = fr.uv, fr.xyz
+        if type(u) is not np.ndarray or u.dtype != _F64 or not u.flags.c_contiguous:
+            u = np.ascontiguousarray(u, np.float64)
+        if type(x) is not np.ndarray or x.dtype != _F64 or not x.flags.c_contiguous:
+            x = np.ascontiguousarray(x, np.float64)
+        su, sx = u.shape, x.shape
+        if len(su) != 2 or su[1] != 2 or len(sx) != 2 or sx[1] != 3 or su[0] != sx[0]:
             raise ValueError(f"frame {i}: uv must be (n, 2) and xyz (n, 3) with the same n")
+        try:  # ctypes' buffer route is the cheapest address per array
+            p2[i], p3[i] = addressof(from_buffer(u)), addressof(from_buffer(x))
+        except (TypeError, ValueError, BufferError):  # read-only or empty arrays
+            p2[i], p3[i] = u.ctypes.data, x.ctypes.data
+        keep.append(u)
+        keep.append(x)
+        ns[i] = su[0]
+        Ks[i] = fr.K
     a = np.zeros(m, _DESC_DTYPE)
-    a["points2D"] = [_ptr(u) for u in uvs]
-    a["points3D"] = [_ptr(x) for x in xyzs]
-    a["n"] = [u.shape[0] for u in uvs]
-    a["K"] = np.array([fr.K for fr in frames], np.float64).reshape(m, 4)
+    a["points2D"] = p2
+    a["points3D"] = p3
+    a["n"] = ns
+    a["K"] = np.array(Ks, np.float64).reshape(m, 4)
     sd = [fr.seed for fr in frames] if seeds is None else list(seeds)
     try:
         a["seed"] = np.array(sd, np.uint64)
@@ -343,7 +353,8 @@ def _frame_descs(frames, seeds=None, max_reproj_error=0.0):
         a["seed"] = np.array([int(s) & _U64 for s in sd], np.uint64)
     a["max_reproj_error"] = (max_reproj_error if max_reproj_error
                              else [getattr(fr, "threshold_px", 0.0) for fr in frames])
-    return a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), (uvs, xyzs, a)
+    keep.append(a)
+    return a.ctypes.data_as(C.POINTER(_lib.FrameDescC)), keep
 
 
 _STAT_NAMES = _RESULT_DTYPE["stats"].names
