@@ -454,7 +454,8 @@ class Engine {
     void launch_prep(int n_active, int64_t max_n) { launch_prep(P, n_active, max_n, stream); }
 
     static constexpr size_t kIngestTableBytes = 64 * 32 + sizeof(IngestTile) * kIngestTileCap;
-    static constexpr int kIngestGridHost = 32;  // CTAs of a zero-copy ingestion (the link saturates at 16)
+    static constexpr int kIngestGridHost = 16;  // CTAs of a zero-copy ingestion: the link saturates at 16, and
+                                                // late frames are read beside the first engine step
 
     // Split admission of a graph: the active frames from n_first on arrive
     // during the first step (kPending; their ingestion table at d_ingest).
