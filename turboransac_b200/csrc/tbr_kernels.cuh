@@ -940,9 +940,11 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(tc_smem + kTcOffCtl);  // points 0, 1; MMA
     uint32_t *tslot = reinterpret_cast<uint32_t *>(tc_smem + kTcOffCtl + 32);
     int *ctl = reinterpret_cast<int *>(tc_smem + kTcOffCtl + 48);
+    volatile int *err = reinterpret_cast<volatile int *>(tc_smem + kTcOffCtl + 60);  // a wait gave up
     long long *run = reinterpret_cast<long long *>(tc_smem + kTcOffCtl + 64);
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     if (tid == 0) {
+        *err = 0;
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         mbar_init(&bars[2], 1);
@@ -1006,16 +1008,13 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
         uint64_t acc[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[j] = 0ull;
-        // Each tile's points are waited for by thread 0 before the barrier that
-        // ends the previous tile (the first tile's here).
-        if (tid == 0) ctl[0] = mbar_wait(&bars[0], ph0, kMaxPolls) ? 1 : 0;
-        __syncthreads();
+        // Every thread waits on the copy and MMA barriers itself (two CTA
+        // barriers per tile). A wait that gives up records the error and the
+        // thread carries on through the same barriers, so the CTA leaves the
+        // tile loop together once the error is visible to all.
         for (int i = 0; i < ntiles; ++i) {
             const int s = i & 1;
-            if (!ctl[0]) {
-                ok = false;
-                break;
-            }
+            if (!*err && !mbar_wait(&bars[s], s ? ph1 : ph0, kMaxPolls)) *err = 1;
             if (s) ph1 ^= 1u; else ph0 ^= 1u;
             // A row of this thread's point.
             const int64_t p0 = (int64_t)(b0 + 2 * i) * kSub;
@@ -1036,25 +1035,20 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
                 *reinterpret_cast<float4 *>(ra + tc_off(tid, 12)) = make_float4(xl, yl, zl, 0.0f);
             }
             fence_proxy_async();  // the operands, written by threads, are read by the tensor core
-            __syncthreads();
+            __syncthreads();      // the A tile is complete; staging buffer s is free
             if (tid == 0) {
                 tc_fence_after();
                 tc_mma(tmem, tc_desc(sA), tc_desc(sB), 0u);
                 tc_mma(tmem, tc_desc(reinterpret_cast<char *>(sA) + 256), tc_desc(reinterpret_cast<char *>(sB) + 256),
                        1u);
                 tc_commit(&bars[2]);
-                if (i + 2 < ntiles) {  // the staging buffer is free again
+                if (i + 2 < ntiles) {
                     fence_proxy_async();
                     bulk_load(sPts + s * 2 * kBlockFloat2, g + (int64_t)(2 * (i + 2)) * kBlockFloat2,
                               (uint32_t)(tile_blocks(i + 2) * kBlockBytes), &bars[s]);
                 }
-                ctl[1] = mbar_wait(&bars[2], phm, kMaxPolls) ? 1 : 0;
             }
-            __syncthreads();
-            if (!ctl[1]) {
-                ok = false;
-                break;
-            }
+            if (!*err && !mbar_wait(&bars[2], phm, kMaxPolls)) *err = 1;
             phm ^= 1u;
             tc_fence_after();
             const uint64_t nx2 = f2pack(NX, NX), ny2 = f2pack(NY, NY);
@@ -1082,9 +1076,9 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
                 }
             }
             tc_fence_before();
-            if (tid == 0 && i + 1 < ntiles) ctl[0] = mbar_wait(&bars[s ^ 1], s ? ph0 : ph1, kMaxPolls) ? 1 : 0;
             __syncthreads();  // the accumulator and the A tile are free for the next tile
         }
+        if (*err) ok = false;  // written before the last barrier, so every thread reads the same
         if (!ok) break;
         // Chunk partials: the warp's 32 hypotheses over its 32 points (lanes
         // 2p, 2p + 1 end with hypotheses 2p, 2p + 1), then the four warps in
@@ -1137,9 +1131,11 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
         // (bounded) before the tensor memory is released.
         if (tid == 0) {
             flag_error(P, kErrTimeout);
+            // Copies still in flight complete the buffers' current phases; the
+            // last MMA issued completes the phase before the current parity.
             mbar_wait(&bars[0], ph0, kMaxPolls);
             mbar_wait(&bars[1], ph1, kMaxPolls);
-            mbar_wait(&bars[2], phm, kMaxPolls);
+            mbar_wait(&bars[2], phm ^ 1u, kMaxPolls);
         }
     }
     tc_fence_before();
