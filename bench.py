@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=10.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
+    ap.add_argument("--tensor", action="store_true",
+                    help="score with the tensor-core shape (8192-point chunks) instead of autotuning")
     ap.add_argument("--case", default="", choices=["", "plain", "scoring", "batch64", "precision"],
                     help="scoring: one N=20000 frame, exactly 4096 samples; batch64: the batched workload's "
                          "first 64 frames in one graph (small cases for ncu)")
@@ -414,8 +416,13 @@ def run_case_batch64(args):
     from turboransac_b200 import Batch, Context, RansacOptions_cuda, scenes
     frames = scenes.batched_frames(64)
     ctx = Context(0, 2 << 30)
-    b = Batch(ctx, frames, RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0))
-    best, _ = b.autotune(repeats=2)  # the shape the main bench would take (graph launches only)
+    if args.tensor:  # the tensor-core shape, as the main bench's --tensor
+        b = Batch(ctx, frames, RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0), points_per_iter=128,
+                  chunk_points=8192)
+        best = {"forced": "tensor-core shape, 8192-point chunks"}
+    else:
+        b = Batch(ctx, frames, RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0))
+        best, _ = b.autotune(repeats=2)  # the shape the main bench would take (graph launches only)
     ms = []
     for i in range(args.warmup + args.steps):
         b.run()
@@ -533,10 +540,11 @@ def main():
     frames = scenes.batched_frames(args.frames, first=rank * args.frames)
     ro = RansacOptions_cuda(max_iterations=1000, success_prob=0.9999, max_reproj_error=4.0)
     ctx = Context(local, 6 << 30)
-    batch = Batch(ctx, frames, ro, hyp_per_thread=args.hr)
+    batch = Batch(ctx, frames, ro, hyp_per_thread=args.hr, points_per_iter=128 if args.tensor else 0,
+                  chunk_points=8192 if args.tensor else 0)
     # Scoring shape chosen by the autotuner on this batch (before the timed region).
     tuned = None
-    if not args.hr:
+    if not args.hr and not args.tensor:
         best, tried = batch.autotune(repeats=2)
         default = next(t for t in tried if t["hyp_per_thread"] == 4 and t["points_per_iter"] == 2
                        and t["chunk_points"] == 0)
@@ -574,12 +582,14 @@ def main():
     achieved = FLOP_PER_PAIR * pairs / (score_ms / 1000.0) / 1e12
     peak_fp32 = fp32_peak_tflops(ctx)
     nominal = 148 * 256 * 1965e6 / 1e12
+    # The scoring kernel that ran: the FP32 pass or the tensor-core shape.
+    tensor = args.tensor or bool(tuned and tuned["best"]["points_per_iter"] == 128)
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "k_score_traffic.json")
     if os.path.exists(tpath):
         try:
             tj = json.load(open(tpath))
-            traffic = tj.get("bytes_per_launch_batched")
+            traffic = tj.get("bytes_per_launch_batched_tc" if tensor else "bytes_per_launch_batched")
         except Exception:
             traffic = None
 
@@ -674,12 +684,17 @@ def main():
             "config": {"workload": WORKLOAD, "global_batch": world * args.frames,
                        "l2": "flushed before every timed step (256 MiB write)",
                        "engine_steps_per_batch": steps_per_run, "parallelism": f"replicas x{world}",
-                       "scoring_shape": tuned},
+                       "scoring_shape": tuned if tuned else
+                       ({"forced": "tensor-core shape, 8192-point chunks"} if args.tensor else
+                        {"forced": f"hyp_per_thread={args.hr}"})},
             "success_rate": succ,
             "pairs_scored_per_batch": pairs,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32 if peak_fp32 else None, "traffic": traffic,
-                         "kernel": "k_score", "flop_per_pair": FLOP_PER_PAIR,
+                         "kernel": "k_score_tc" if tensor else "k_score", "flop_per_pair": FLOP_PER_PAIR,
+                         "accounting": ("27 FP32-equivalent FLOP per pair: the projection's 18 on the tensor "
+                                        "cores (tcgen05 TF32, split operands), the rest on the FP32 pipe")
+                                       if tensor else "27 FP32 FLOP per pair on the FP32 pipe",
                          "peak_source": "FP32 FMA peak measured in this run (packed-FMA kernel); "
                                         f"nominal {nominal:.1f} TFLOP/s at 1965 MHz",
                          "launch_ms_avg": score_ms / max(score_launches, 1)},
