@@ -546,8 +546,7 @@ def main():
     tuned = None
     if not args.hr and not args.tensor:
         best, tried = batch.autotune(repeats=2)
-        default = next(t for t in tried if t["hyp_per_thread"] == 4 and t["points_per_iter"] == 2
-                       and t["chunk_points"] == 0)
+        default = next(t for t in tried if t["points_per_iter"] == 128 and t["chunk_points"] == 0)
         tuned = {"best": best, "default_ms": default["ms"], "candidates": len(tried)}
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 

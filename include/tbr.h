@@ -98,16 +98,18 @@ typedef struct tbr_ext_options {
     uint64_t seed;                /* Philox key of the sampler (0 = ransac.seed) */
     const int32_t *replay_idx;    /* host: replayed triples, replay_count*3 int32 */
     int64_t replay_count;
-    int32_t hyp_per_thread;       /* scoring tile: 0 = auto, else 2, 4, 6 or 8 hypotheses per lane */
+    int32_t hyp_per_thread;       /* scoring tile: 0 = default (the tensor-core kernel), else 2, 4, 6
+                                     or 8 hypotheses per lane of the FP32 kernel */
     int32_t chunk_points;         /* scoring tile: 0 = auto, else points per work item */
     /* Stop rule K = ceil(3 log(1-p) / log(1-w^3)) beyond the int range: the
      * reference's double->int assignment (turbo_ransac.cu:231) is undefined
      * there and x86 yields INT_MIN, ending the loop after one round.
      * 0 (default): saturate -- keep sampling up to the cap; 1: reproduce x86. */
     int32_t stop_rule_x86_quirk;
-    int32_t points_per_iter;      /* scoring tile: 0 = auto, else 2 or 4 points per inner step;
-                                     128 = tensor-core scoring (tcgen05 MMA over 128-point tiles,
-                                     32 hypotheses per block; overrides hyp_per_thread) */
+    int32_t points_per_iter;      /* scoring tile: 0 = default, 2 or 4 points per inner step of the
+                                     FP32 kernel (an FP32 field alone selects the FP32 kernel, the
+                                     other field then 4 / 2), 128 = tensor-core scoring (tcgen05 MMA
+                                     over 128-point tiles, 32 hypotheses per block; the default) */
 } tbr_ext_options;
 
 /* Results of one estimate. The reference returns RansacStats_cuda unfilled except

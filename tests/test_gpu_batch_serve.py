@@ -279,7 +279,7 @@ def test_tensor_scoring_batch_matches_fp32_shape(ctx):
     sizes) gives the FP32 shape's results: the FP64 re-rank decides, the filter
     only has to keep the best within its band."""
     fr = mixed_frames() + [scenes.make_frame(30000, 0.15, 1.0, 9300), scenes.make_frame(700, 0.5, 2.0, 9301)]
-    b = Batch(ctx, fr, RO)
+    b = Batch(ctx, fr, RO, hyp_per_thread=4, points_per_iter=2)
     b.run()
     b.sync()
     ref = b.results()

@@ -21,12 +21,14 @@ def cam_of(f):
     return Camera_cuda(1, 640, 480, list(f.K))
 
 
-# Scoring shape on the tensor cores (tcgen05, TF32 split operands).
-TENSOR = {"hyp_per_thread": 2, "points_per_iter": 128}
+# Scoring shapes: on the tensor cores (tcgen05, TF32 split operands; the
+# default) and on the FP32 pipe.
+TENSOR = {"points_per_iter": 128}
+FP32 = {"hyp_per_thread": 4, "points_per_iter": 2}
 
 
-@pytest.mark.parametrize("shape", [None, TENSOR, dict(TENSOR, chunk_points=256)],
-                         ids=["fp32", "tensor", "tensor-chunk256"])
+@pytest.mark.parametrize("shape", [None, FP32, dict(FP32, hyp_per_thread=8), dict(TENSOR, chunk_points=256)],
+                         ids=["default", "fp32", "fp32-hr8", "tensor-chunk256"])
 def test_debug_scores_counts_vs_oracle(ctx, oracle, shape):
     f = scenes.plain_frame(1)
     S = 512
@@ -85,14 +87,15 @@ def test_scoring_bound_config_matches_oracle(ctx, oracle):
     np.testing.assert_array_equal(inl, o["inliers"])
 
 
-def test_tensor_scoring_matches_oracle(ctx, oracle):
-    """The tensor-core scoring shape decides like the FP64 pipeline: the
-    scoring-bound frame (4096 samples, 15 % inliers, N = 20000) and a frame
-    that needs many rounds give the oracle's samples, selection and pose."""
+@pytest.mark.parametrize("shape", [TENSOR, FP32], ids=["tensor", "fp32"])
+def test_scoring_shapes_match_oracle(ctx, oracle, shape):
+    """Both scoring kernels decide like the FP64 pipeline: the scoring-bound
+    frame (4096 samples, 15 % inliers, N = 20000) and a frame that needs many
+    rounds give the oracle's samples, selection and pose."""
     f = scenes.scoring_frame(0)
     ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
     st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
-                                               force_samples=4096, **TENSOR)
+                                               force_samples=4096, **shape)
     o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=4096, force_samples=4096, threads=8)
     d, info = st.details, o["info"]
     assert d["hypotheses"] == info.ransac.hypotheses
@@ -103,7 +106,7 @@ def test_tensor_scoring_matches_oracle(ctx, oracle):
     f = scenes.make_frame(3000, 0.10, 1.0, 4242)
     ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
     st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam_of(f), ro, BundleOptions_cuda(), seed=f.seed,
-                                               **TENSOR)
+                                               **shape)
     o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
     d, info = st.details, o["info"]
     assert d["samples"] == info.ransac.samples and d["best_sample"] == info.ransac.best_sample

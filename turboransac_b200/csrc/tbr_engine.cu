@@ -111,8 +111,10 @@ struct RunOptions {
     double trials_mult = 3.0;
     int skip_refine = 0;
     int quirk = 0;
-    int hr = 4;
-    int pp = 2;
+    // Scoring shape: hr = 1 is the tensor-core kernel (32 hypotheses per block,
+    // pp = kTcPP), the default; hr = 2, 4, 6, 8 with pp = 2 or 4 the FP32 kernels.
+    int hr = 1;
+    int pp = kTcPP;
     int chunk_points = 0;
     int max_rounds_step = 0;
     // LM (compat: default BundleOptions_cuda with loss_scale = 1/f)
@@ -132,13 +134,18 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
         o.quirk = ext->stop_rule_x86_quirk;
         o.force_samples = ext->force_samples;
         if (ext->max_total_samples > 0) o.max_total = ext->max_total_samples;
-        if (ext->hyp_per_thread == 2 || ext->hyp_per_thread == 4 || ext->hyp_per_thread == 6 ||
-            ext->hyp_per_thread == 8)
-            o.hr = ext->hyp_per_thread;
-        if (ext->points_per_iter == 2 || ext->points_per_iter == 4) o.pp = ext->points_per_iter;
-        if (ext->points_per_iter == kTcPP) {  // tensor-core scoring: 32 hypotheses per block
-            o.pp = kTcPP;
+        // An FP32 shape is asked for by either of its fields; the other takes
+        // its FP32 default (hr 4, pp 2). points_per_iter = kTcPP asks for the
+        // tensor-core kernel whatever hyp_per_thread says.
+        const int hpt = ext->hyp_per_thread, ppi = ext->points_per_iter;
+        const bool fp32_hr = hpt == 2 || hpt == 4 || hpt == 6 || hpt == 8;
+        const bool fp32_pp = ppi == 2 || ppi == 4;
+        if (ppi == kTcPP) {
             o.hr = 1;
+            o.pp = kTcPP;
+        } else if (fp32_hr || fp32_pp) {
+            o.hr = fp32_hr ? hpt : 4;
+            o.pp = fp32_pp ? ppi : 2;
         }
         o.chunk_points = ext->chunk_points;
     }
@@ -402,7 +409,7 @@ class Engine {
     // Scoring kernel variant: HR hypotheses per lane = 2*HP, PP points per iteration.
     void launch_score(const Pools &Q, int hr, int pp, cudaStream_t st) {
         const int threads = kScoreWarps * 32;
-        if (pp == kTcPP) k_score_tc<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);
+        if (hr == 1) k_score_tc<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);  // (pp == kTcPP)
         else if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
         else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
         else if (hr == 6 && pp == 4) k_score<3, 4><<<score_grid[5], threads, 0, st>>>(Q);
@@ -410,7 +417,7 @@ class Engine {
         else if (pp == 4) k_score<2, 4><<<score_grid[2], threads, 0, st>>>(Q);
         else k_score<2, 2><<<score_grid[1], threads, 0, st>>>(Q);
     }
-    int pp = 2;  // points per iteration of the scoring kernel (HR = 4)
+    int pp = kTcPP;  // points per iteration of the scoring kernel (kTcPP: the tensor-core kernel)
 
     // RANSAC part of a step (plan .. finalize).
     void launch_ransac(const Pools &Q, int n_active, int hr, cudaStream_t st, Profile *prof = nullptr) {
