@@ -569,8 +569,10 @@ __global__ void k_score_plan(Pools P) {
     if (act) {
         HB = 32 * f->hr;
         nhb = (f->hyp_count + HB - 1) / HB;
-        // About 8 items per warp slot of the GPU; at least 2 staging blocks per item.
-        const double target_items = 8.0 * P.num_sms * 16;
+        // About 8 items per warp slot of the GPU (FP32 kernels, one warp per
+        // item) or per 4 CTA slots (the tensor-core kernel, a CTA per item with
+        // a larger fixed cost per item); at least 2 staging blocks per item.
+        const double target_items = f->hr == 1 ? 8.0 * P.num_sms * 4 : 8.0 * P.num_sms * 16;
         const double pairs_per_item = fmax((double)pairs_total / target_items, 2.0 * kSub * HB);
         cb = (int)ceil(pairs_per_item / ((double)HB * kSub));
         if (f->chunk_points > 0) cb = max(1, f->chunk_points / kSub);
