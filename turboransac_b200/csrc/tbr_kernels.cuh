@@ -835,18 +835,18 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
 
 // ------------------------------------------------ tensor-core scoring --
 // The same filter with the projection on the 5th-generation tensor cores:
-// for a tile of 128 points and a block of 64 hypotheses, one tcgen05.mma
-// (kind::tf32, M = 128 points, N = 192 = z2 | z0 | z1 rows of the 64
-// hypotheses, K = 16) writes every z of the tile into tensor memory, and the
-// epilogue (one thread per point) does the reciprocal, the residuals, the
-// saturating r^2 and the sum per hypothesis. TF32 keeps 11 significant bits,
+// for a tile of 128 points and a block of 32 hypotheses, one tcgen05.mma pair
+// (kind::tf32, M = 128 points, N = 96 = z2 | z0 | z1 rows of the 32
+// hypotheses, K = 16 in two steps of 8) writes every z of the tile into tensor
+// memory, and the epilogue (one thread per point) does the reciprocal, the
+// residuals, the saturating r^2 and the sum per hypothesis. TF32 keeps 11 significant bits,
 // so each operand is split into a hi part (rounded to nearest TF32) and the
 // rounded remainder, and K carries all four cross terms
 //   A row (point)      = [Xh Yh Zh 1 | Xl Yl Zl 0 | Xh Yh Zh 1 | Xl Yl Zl 0]
 //   B row (hyp. row c) = [ch0..ch3   | ch0..ch2 0 | cl0..cl3   | cl0..cl2 0]
 // whose products are exact in FP32 and sum to c . [X 1] with an error of the
 // order of FP32 rounding (the remainders' own rounding is 2^-23 relative).
-// Selected by the scoring shape hyp_per_thread = 2, points_per_iter = 128.
+// The default scoring shape (FrameDev::hr = 1, points_per_iter = 128).
 constexpr int kTcHyp = 32;        // hypotheses per item (HB at HR = 1)
 constexpr int kTcN = 3 * kTcHyp;   // MMA N: z2 | z0 | z1 rows of the block
 constexpr int kTcPts = 128;       // MMA M: points per tile
