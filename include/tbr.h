@@ -329,6 +329,13 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D,
                                    float *scores32, int64_t *counts, int64_t cap,
                                    int64_t *n_hyp, const tbr_ext_options *ext);
 
+/* Failure-path check (no reference counterpart): one kernel waits on an
+ * mbarrier that nothing completes, giving up after `polls` tries (1 .. 2^22)
+ * as every wait of the engine's kernels does after its own limit. Returns
+ * TBR_ERR_TIMEOUT, read from the device's error word like any expired wait;
+ * the context stays usable. Used by the tests. */
+tbr_status tbr_debug_bounded_wait(tbr_context *ctx, uint32_t polls);
+
 /* --------------------------------------------------------- no allocation --
  * No counterpart in the reference. FP64 truncated-MSAC scores and inlier counts
  * of n_poses poses (n_poses*12 doubles, [R | t] row-major) over n device-resident

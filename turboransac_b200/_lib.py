@@ -112,7 +112,7 @@ EXPORTS = [
     "tbr_bundle_adjust", "tbr_estimate_batch", "tbr_batch_create", "tbr_batch_run", "tbr_batch_sync",
     "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_batch_autotune", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
     "tbr_server_submit_nocopy", "tbr_server_get_stats", "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
-    "tbr_debug_score_samples", "tbr_msac_score_noalloc",
+    "tbr_debug_score_samples", "tbr_debug_bounded_wait", "tbr_msac_score_noalloc",
 ]
 
 
@@ -162,6 +162,7 @@ def lib() -> C.CDLL:
     L.tbr_server_destroy.argtypes = [vp]
     L.tbr_debug_score_samples.argtypes = [vp, vp, vp, C.c_int64, vp, C.c_double, vp, C.c_int64, vp,
                                           vp, vp, vp, C.c_int64, C.POINTER(C.c_int64), vp]
+    L.tbr_debug_bounded_wait.argtypes = [vp, C.c_uint32]
     L.tbr_msac_score_noalloc.argtypes = [vp, vp, C.c_int64, vp, C.c_int32, C.c_double, vp, vp, vp]
     for name in EXPORTS:
         fn = getattr(L, name)

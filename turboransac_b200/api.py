@@ -243,6 +243,12 @@ class Context:
                                                C.byref(st)))
         return CameraPose_cuda(q, t), st.as_dict()
 
+    def debug_bounded_wait(self, polls: int = 1 << 16):
+        """Failure-path check (tbr_debug_bounded_wait): a device wait that nothing
+        completes gives up after `polls` tries; raises TbrError (TIMEOUT)."""
+        with self._lock:
+            check(_lib.lib().tbr_debug_bounded_wait(self._h, polls))
+
     def debug_score_samples(self, points2D, points3D, K, max_reproj_error, triples, counts=False, shape=None):
         """Per-hypothesis (ids, FP64 poses (H,3,4), FP32 scores in tau^2 units, counts or None).
         shape: a scoring shape (dict with hyp_per_thread, points_per_iter,

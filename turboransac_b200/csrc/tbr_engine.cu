@@ -2530,6 +2530,22 @@ static std::unordered_map<int, NoAllocScratch *> g_noalloc_ptr;
 
 }  // namespace tbr
 
+tbr_status tbr_debug_bounded_wait(tbr_context *ctx, uint32_t polls) {
+    if (!ctx || polls < 1 || polls > (1u << 22)) return fail(TBR_ERR_INVALID_ARG, "polls must be in [1, 2^22]");
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    TBR_CUDA(cudaSetDevice(E.device));
+    TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
+    k_debug_bounded_wait<<<1, 32, 0, E.stream>>>(E.P.counters, polls);
+    TBR_CUDA(cudaGetLastError());
+    TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
+    TBR_CUDA(cudaStreamSynchronize(E.stream));
+    if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    return TBR_OK;
+}
+
 extern "C" tbr_status tbr_msac_score_noalloc(const double *x_dev, const double *X_dev, int64_t n,
                                               const double *poses_dev, int32_t n_poses, double sq_threshold,
                                               double *scores_dev, int64_t *counts_dev, void *stream) {

@@ -1886,6 +1886,17 @@ __global__ void __cluster_dims__(kLMCluster, 1, 1) __launch_bounds__(kLMThreads,
 // are taken by k_inliers right away.
 __global__ void k_tick(Pools P) { P.counters[kCSteps] += 1; }
 
+// Failure-path check: a wait on an mbarrier that nothing ever completes, with
+// `polls` tries, must give up and leave the timeout bit for the host.
+__global__ void k_debug_bounded_wait(unsigned long long *counters, uint32_t polls) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+        if (!mbar_wait(&bar, 0u, polls)) atomicOr(&counters[kCError], kErrTimeout);
+    }
+}
+
 // Serving: the status of every active frame in one array (one copy to the host).
 __global__ void k_gather_status(Pools P, int32_t *out) {
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < P.n_active; a += gridDim.x * blockDim.x)
