@@ -1154,8 +1154,8 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
     if (host_devs) *host_devs = A.devs;
     if (device_points) {
         std::vector<IngestTile> t;
-        for (size_t i = 0; i < fr.size(); ++i)
-            add_frame_tiles(t, E, A.devs[i], fr[i].n, fr[i].uv, fr[i].xyz, ingest_tile_bytes(fr));
+        const size_t tile = ingest_tile_bytes(fr);
+        for (size_t i = 0; i < fr.size(); ++i) add_frame_tiles(t, E, A.devs[i], fr[i].n, fr[i].uv, fr[i].xyz, tile);
         size_t off = 0;
         const int64_t *d = put_table(E, (char *)E.h_stage + rec, off, t);
         if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
