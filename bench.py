@@ -96,7 +96,9 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{gpu}.csv")
+        # Raw samples: a temporary file unless TBR_CLOCKS_DIR names a directory to keep them in.
+        import tempfile
+        self.path = os.path.join(os.environ.get("TBR_CLOCKS_DIR", tempfile.gettempdir()), f"clocks_gpu{gpu}.csv")
 
     def __enter__(self):
         try:

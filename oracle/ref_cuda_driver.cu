@@ -1,5 +1,6 @@
 /*
- * Timing driver for the reference's own CUDA build (BASELINE INFRASTRUCTURE).
+ * Timing driver for the reference's own CUDA build (measurement infrastructure:
+ * the comparison arm, not part of the product).
  *
  * Linked with the reference's unmodified sources (Module/TbrCudaPnP/src/
  * entry.cu, turbo_ransac.cu, ba.cu) by `make -C oracle refcuda`; the binary

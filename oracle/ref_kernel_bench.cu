@@ -1,6 +1,7 @@
 /*
  * The reference's RANSAC kernel launched directly, for a scoring-bound timing
- * (BASELINE INFRASTRUCTURE, built into oracle/_ref by `make -C oracle refcuda`).
+ * (measurement infrastructure for the comparison arm, built into oracle/_ref by
+ * `make -C oracle refcuda`).
  *
  * The reference cannot switch its early stop off, so its whole call cannot
  * score an exact sample count; this harness reproduces the launch sequence of

@@ -1,5 +1,6 @@
 """Runs the reference's own CUDA build (oracle/_ref/tbr_refcuda, made by
-`make -C oracle refcuda`) on a list of frames -- BASELINE INFRASTRUCTURE.
+`make -C oracle refcuda`) on a list of frames -- measurement infrastructure for
+the comparison arm, not part of the product.
 
 Each frame is one call of the reference's estimate_absolute_pose_cuda
 (entry.cu:28-144), timed around the whole call on the host clock as
