@@ -39,7 +39,7 @@ FLOP_PER_PAIR = 27  # projection 9 FMA, reciprocal, 2 residual FMA, r^2, score a
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--frames", type=int, default=256)
@@ -106,6 +106,10 @@ class ClockSampler:
             self.f = open(self.path, "w")
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-i", str(self.gpu), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            # The sampler is running (its first sample is in) before the timed region starts.
+            t0 = time.time()
+            while time.time() - t0 < 2.0 and os.path.getsize(self.path) == 0:
+                time.sleep(0.01)
         except Exception:
             self.p = None
         return self
