@@ -148,6 +148,9 @@ void tbr_default_bundle_options(tbr_bundle_options *opts);
 /* device: CUDA ordinal. workspace_bytes: device memory the context may use
  * (0 = 1 GiB). The workspace is allocated once and reused by every call. */
 tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context **out);
+/* Destroy every batch made on the context first (a batch uses the context's
+ * workspace and stream); a server takes only the device from its context and
+ * may outlive it. */
 void tbr_context_destroy(tbr_context *ctx);
 
 /* estimate_absolute_pose_cuda (entry.h:13-19). Host buffers:
@@ -226,7 +229,7 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
 tbr_status tbr_batch_run(tbr_batch *b);      /* asynchronous on the context stream */
 tbr_status tbr_batch_sync(tbr_batch *b);     /* waits; returns the first device error */
 tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results);
-void tbr_batch_destroy(tbr_batch *b);
+void tbr_batch_destroy(tbr_batch *b);        /* before its context's tbr_context_destroy */
 
 /* Per-kernel device time of one batch run, stepped from the host with a CUDA
  * event pair around every kernel launch on the context stream (slower than

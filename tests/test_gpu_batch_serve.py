@@ -315,3 +315,27 @@ def test_server_tensor_scoring_shape_matches_plain(ctx):
         d, pose = ref[ids[r["id"]]]
         assert r["status"] == 0
         same(r, r["q"], r["t"], d, pose)
+
+
+def test_context_close_releases_its_batches_first(ctx):
+    """Closing a context closes the batches made on it (they use its workspace);
+    a server takes only the device and keeps working after its context closes."""
+    from turboransac_b200 import Context
+    f = scenes.make_frame(800, 0.5, 1.0, 31001)
+    d, pose = plain(ctx, f)
+    c2 = Context(0, 1 << 30)
+    b = Batch(c2, [f], RO)
+    srv = Server(c2, budget_bytes=1 << 30, max_slots=4)
+    b.run()
+    b.sync()
+    (r,) = b.results()
+    same(r, r["q"], r["t"], d, pose)
+    c2.close()
+    assert b._h is None
+    b.close()  # a second close is a no-op
+    rid = srv.submit(f)
+    srv.drain()
+    (s,) = srv.poll()
+    assert s["id"] == rid and s["status"] == 0
+    same(s, s["q"], s["t"], d, pose)
+    srv.close()

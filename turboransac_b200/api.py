@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import threading
+import weakref
 
 import numpy as np
 
@@ -148,6 +149,7 @@ class Context:
         check(L.tbr_context_create(device, workspace_bytes, C.byref(h)))
         self._h = h
         self._lock = threading.Lock()
+        self._batches = weakref.WeakSet()  # destroyed before the context (they use its workspace)
 
     @property
     def handle(self):
@@ -155,6 +157,8 @@ class Context:
 
     def close(self):
         if self._h:
+            for b in list(self._batches):
+                b.close()
             _lib.lib().tbr_context_destroy(self._h)
             self._h = None
 
@@ -401,6 +405,7 @@ class Batch:
         with ctx._lock:
             check(_lib.lib().tbr_batch_create(ctx.handle, arr, self.n, C.byref(ro), C.byref(ext), C.byref(h)))
         self._h = h
+        ctx._batches.add(self)
 
     def run(self):
         check(_lib.lib().tbr_batch_run(self._h))
