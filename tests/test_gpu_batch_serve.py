@@ -339,3 +339,39 @@ def test_context_close_releases_its_batches_first(ctx):
     assert s["id"] == rid and s["status"] == 0
     same(s, s["q"], s["t"], d, pose)
     srv.close()
+
+
+def test_batched_calls_reject_what_the_plain_call_rejects(ctx):
+    """max_iterations < 1, a threshold <= 0 and non-positive focal lengths are
+    INVALID_ARG in every batched entry point, as in the plain call; the context
+    keeps working."""
+    import dataclasses
+
+    import torch
+
+    from turboransac_b200 import TbrError, estimate_batch_device
+    f = scenes.make_frame(500, 0.5, 1.0, 31002)
+    bad_cam = dataclasses.replace(f, K=np.array([0.0, 525.0, 319.5, 239.5]))
+    bad_opts = [RansacOptions_cuda(max_iterations=0, max_reproj_error=4.0),
+                RansacOptions_cuda(max_iterations=1000, max_reproj_error=0.0)]
+    from turboransac_b200 import DeviceFrame
+    df, dbad = DeviceFrame(f), DeviceFrame(bad_cam)
+    for ro in bad_opts:
+        with pytest.raises(TbrError):
+            estimate_batch(ctx, [f, f], ro)
+        with pytest.raises(TbrError):
+            estimate_batch_device(ctx, [df], ro)
+        with pytest.raises(TbrError):
+            Batch(ctx, [f], ro)
+        with pytest.raises(TbrError):
+            Server(ctx, budget_bytes=1 << 30, max_slots=4, ransac_opt=ro)
+    with pytest.raises(TbrError):
+        estimate_batch(ctx, [f, bad_cam], RO)
+    with pytest.raises(TbrError):
+        estimate_batch_device(ctx, [dbad], RO)
+    with pytest.raises(TbrError):
+        Batch(ctx, [bad_cam], RO)
+    torch.cuda.synchronize()
+    (r,) = estimate_batch(ctx, [f], RO)
+    d, pose = plain(ctx, f)
+    same(r, r["q"], r["t"], d, pose)

@@ -80,3 +80,12 @@ def test_results_unpack_as_dicts_or_one_record_array():
         assert r["status"] == i and r["samples"] == 1000 * (i + 1) and r["num_inliers"] == 10 + i
         np.testing.assert_array_equal(r["t"], [0.0, 0.0, float(i)])
         assert r["q"][0] == 1.0
+
+
+def test_camera_parameters_are_the_four_pinhole_values():
+    cam = api.Camera_cuda(1, 640, 480, [525.0, 526.0, 319.5, 239.5])
+    K = api._camera_K(cam)
+    assert K.dtype == np.float64 and K.flags.c_contiguous and list(K) == [525.0, 526.0, 319.5, 239.5]
+    for bad in ([525.0, 319.5, 239.5], [525.0, 525.0, 319.5, 239.5, 0.0]):
+        with pytest.raises(ValueError):
+            api._camera_K(api.Camera_cuda(1, 640, 480, bad))

@@ -133,6 +133,16 @@ class CameraPose_cuda:
         return -self.R().T @ self.t
 
 
+def _camera_K(camera):
+    """(fx, fy, cx, cy): the four PINHOLE parameters the reference's camera
+    reads (camera.cuh:24-67); any other count is refused here, before the C
+    call reads four values."""
+    K = np.ascontiguousarray(camera.params, np.float64).reshape(-1)
+    if K.shape[0] != 4:
+        raise ValueError(f"camera.params must hold (fx, fy, cx, cy), got {K.shape[0]} values")
+    return K
+
+
 def _f64(a, cols):
     a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
     if a.ndim != 2 or a.shape[1] != cols:
@@ -198,7 +208,7 @@ class Context:
             rep = np.ascontiguousarray(np.asarray(replay, np.int32).reshape(-1, 3))
             ext.replay_idx = rep.ctypes.data
             ext.replay_count = rep.shape[0]
-        K = np.asarray(camera.params, np.float64)
+        K = _camera_K(camera)
         q = np.zeros(4)
         t = np.zeros(3)
         inl = np.zeros(x.shape[0], np.uint8)
@@ -230,7 +240,7 @@ class Context:
                       opt: BundleOptions_cuda | None = None, weights=None, honor_options=False):
         x = _f64(x, 2)
         X = _f64(X, 3)
-        K = np.asarray(camera.params, np.float64)
+        K = _camera_K(camera)
         q = np.array(pose.q, np.float64)
         t = np.array(pose.t, np.float64)
         bo = (opt or BundleOptions_cuda()).to_c()

@@ -1397,6 +1397,24 @@ static tbr_status estimate_frames_chunked(tbr_context *ctx, const std::vector<Fr
     return TBR_OK;
 }
 
+// Argument checks shared by the batched entry points, the same as the plain
+// call's: at least one sample per round, a positive threshold, and per frame
+// three correspondences, both arrays and positive focal lengths.
+static tbr_status check_ransac(const tbr_ransac_options &ro) {
+    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations (samples per round) must be >= 1");
+    if (!(ro.max_reproj_error > 0)) return fail(TBR_ERR_INVALID_ARG, "max_reproj_error must be > 0");
+    return TBR_OK;
+}
+static tbr_status check_frame(const tbr_frame_desc &d) {
+    if (d.n < 3 || !d.points2D || !d.points3D) return fail(TBR_ERR_INVALID_ARG, "bad frame");
+    if (!(d.K[0] > 0) || !(d.K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "bad camera");
+    return TBR_OK;
+}
+static FrameHost frame_host(const tbr_frame_desc &d, const tbr_ransac_options &ro) {
+    return {d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
+            d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0};
+}
+
 extern "C" {
 
 tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
@@ -1406,13 +1424,12 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
     tbr_ransac_options ro;
     tbr_default_ransac_options(&ro);
     if (ransac_opt) ro = *ransac_opt;
+    if (tbr_status c = check_ransac(ro)) return c;
     RunOptions o = make_run_options(&ro, nullptr, ext);
     std::vector<FrameHost> fr;
     for (int i = 0; i < n_frames; ++i) {
-        const tbr_frame_desc &d = frames[i];
-        if (d.n < 3 || !d.points2D || !d.points3D) return fail(TBR_ERR_INVALID_ARG, "bad frame");
-        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
-                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+        if (tbr_status c = check_frame(frames[i])) return c;
+        fr.push_back(frame_host(frames[i], ro));
     }
     std::lock_guard<std::mutex> lk(ctx->E.mu);
     std::vector<FrameResult> res;
@@ -1438,14 +1455,13 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
     tbr_ransac_options ro;
     tbr_default_ransac_options(&ro);
     if (ransac_opt) ro = *ransac_opt;
-    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations must be >= 1");
+    if (tbr_status c = check_ransac(ro)) return c;
     RunOptions o = make_run_options(&ro, nullptr, ext);
     Engine &E = ctx->E;
     std::vector<FrameHost> fr;
     for (int i = 0; i < n_frames; ++i) {
         const tbr_frame_desc &d = frames[i];
-        if (d.n < 3 || !d.points2D || !d.points3D || !(d.K[0] > 0) || !(d.K[1] > 0))
-            return fail(TBR_ERR_INVALID_ARG, "bad frame");
+        if (tbr_status c = check_frame(d)) return c;
         for (const void *p : {(const void *)d.points2D, (const void *)d.points3D}) {
             cudaPointerAttributes a;
             if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -1455,8 +1471,7 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
             if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != E.device)
                 return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory of the context's GPU");
         }
-        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
-                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+        fr.push_back(frame_host(d, ro));
     }
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1534,6 +1549,7 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     // (ba.cu:111-130, jaco.cuh:36,123); with honor_options the loss type and
     // the weights are applied.
     if (!ctx || !x || !X || !K || !q || !t || n < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    if (!(K[0] > 0) || !(K[1] > 0)) return fail(TBR_ERR_INVALID_ARG, "focal lengths must be positive");
     tbr_bundle_options bo;
     tbr_default_bundle_options(&bo);
     if (opt) bo = *opt;
@@ -1665,14 +1681,11 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
     tbr_ransac_options ro;
     tbr_default_ransac_options(&ro);
     if (ransac_opt) ro = *ransac_opt;
-    if (ro.max_iterations < 1) return fail(TBR_ERR_INVALID_ARG, "max_iterations must be >= 1");
+    if (tbr_status c = check_ransac(ro)) return c;
     std::vector<FrameHost> fr;
     for (int i = 0; i < n_frames; ++i) {
-        const tbr_frame_desc &d = frames[i];
-        if (d.n < 3 || !d.points2D || !d.points3D || !(d.K[0] > 0) || !(d.K[1] > 0))
-            return fail(TBR_ERR_INVALID_ARG, "bad frame");
-        fr.push_back({d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
-                      d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0});
+        if (tbr_status c = check_frame(frames[i])) return c;
+        fr.push_back(frame_host(frames[i], ro));
     }
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
@@ -2238,9 +2251,9 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
         return st;
     }
     s->ro = cfg->ransac;
-    if (s->ro.max_iterations < 1) {
+    if (tbr_status c = check_ransac(s->ro)) {
         delete s;
-        return fail(TBR_ERR_INVALID_ARG, "ransac.max_iterations must be >= 1");
+        return c;
     }
     s->o = make_run_options(&s->ro, nullptr, &cfg->ext);
     // Serving: bounded rounds per step so that one heavy frame cannot hold a
