@@ -410,3 +410,28 @@ def test_batched_workload_full_size(ctx, oracle):
            if res[i]["samples"] != smp[i] or qa(res[i]["q"], q[i]) >= 1e-6
            or np.abs(np.asarray(res[i]["t"]) - t[i]).max() >= 1e-6]
     assert not bad, bad
+
+
+def test_serving_workload_matches_plain_and_sample_cap_matches_oracle(ctx, oracle):
+    """Requests of the serving workload (N log-uniform [300, 50000], w down to
+    0.05) plus a 5 %-inlier frame that runs into the 100000-sample cap: the
+    server (rounds per step bounded for serving) returns the plain call's
+    results, and the capped frame equals the FP64 oracle's sample count and pose."""
+    fr = [scenes.serving_request(i) for i in range(40)] + [scenes.make_frame(20000, 0.05, 1.0, 9400)]
+    ref = [plain(ctx, f) for f in fr]
+    srv = Server(ctx, budget_bytes=4 << 30, max_slots=64)
+    ids = {srv.submit(f): i for i, f in enumerate(fr)}
+    srv.drain()
+    got = srv.poll(1024)
+    srv.close()
+    assert len(got) == len(fr)
+    for r in got:
+        d, pose = ref[ids[r["id"]]]
+        assert r["status"] == 0
+        same(r, r["q"], r["t"], d, pose)
+    d, pose = ref[-1]
+    assert d["samples"] == 100000
+    f = fr[-1]
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
+    assert o["info"].ransac.samples == 100000 and o["info"].ransac.best_sample == d["best_sample"]
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
