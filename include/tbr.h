@@ -185,7 +185,11 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
 /* ---------------------------------------------------------------- batch --
  * Many frames of uneven size in one persistent, CUDA-graph-captured launch
  * sequence. A frame is described by host pointers; the call copies them in,
- * runs every frame to completion and copies results out. */
+ * runs every frame to completion and copies results out. Every batched entry
+ * point (here, the batch object and the server) refuses with
+ * TBR_ERR_INVALID_ARG what the plain call refuses: max_iterations < 1,
+ * max_reproj_error <= 0 in the options, and a frame with n < 3, a NULL array
+ * or a focal length <= 0. */
 typedef struct tbr_frame_desc {
     const double *points2D;   /* n*2 pixels */
     const double *points3D;   /* n*3 */
