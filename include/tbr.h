@@ -126,7 +126,10 @@ typedef struct tbr_stats {
     int32_t best_solution;
     int32_t steps;                /* engine steps used */
     int64_t candidates_rescored;  /* hypotheses re-ranked in FP64 */
-    int32_t candidate_overflow;   /* 1 if the FP64 re-rank candidate cap was hit */
+    int32_t candidate_overflow;   /* 1 if a single round had more FP64 re-rank candidates than
+                                     fit (4096; possible only with more than 1024 samples per
+                                     round) and one inside the FP32 error band was dropped: the
+                                     selection may then differ from the FP64 pipeline's */
     int32_t lm_iterations;
     int32_t lm_invalid_steps;
     double lm_initial_cost;
@@ -355,8 +358,13 @@ tbr_status tbr_debug_bounded_wait(tbr_context *ctx, uint32_t polls);
  * fixed array of about 400 KB compiled into the library, which every GPU that
  * loads the library keeps until the process exits. Limits and rules:
  *  - at most 1024 poses per call (larger requests fail with TBR_ERR_INVALID_ARG);
+ *    sq_threshold must be positive and finite (else TBR_ERR_INVALID_ARG);
+ *  - the device of `stream` must be the current device (else TBR_ERR_INVALID_ARG);
  *  - the first call on each device looks up the array's device address (with
  *    that device current), so make that first call before any stream capture;
+ *    the address is kept for the life of the process, so after a
+ *    cudaDeviceReset (which unloads the library's device code) the call must
+ *    not be used again on that device;
  *  - all calls share the array: calls that overlap on the GPU (different
  *    streams, or other threads) race -- order them on one stream or with events. */
 tbr_status tbr_msac_score_noalloc(const double *x_dev, const double *X_dev, int64_t n,

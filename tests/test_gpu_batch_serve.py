@@ -397,6 +397,7 @@ def test_batched_workload_full_size(ctx, oracle):
     ok = 0
     for f, a, c in zip(fr, res, host):
         assert a["status"] == 0 and c["status"] == 0
+        assert a["candidate_overflow"] == 0 and c["candidate_overflow"] == 0
         assert a["samples"] == c["samples"] and a["best_sample"] == c["best_sample"]
         assert a["num_inliers"] == c["num_inliers"]
         np.testing.assert_array_equal(a["q"], c["q"])
@@ -428,6 +429,7 @@ def test_serving_workload_matches_plain_and_sample_cap_matches_oracle(ctx, oracl
     for r in got:
         d, pose = ref[ids[r["id"]]]
         assert r["status"] == 0
+        assert r["candidate_overflow"] == 0 and d["candidate_overflow"] == 0
         same(r, r["q"], r["t"], d, pose)
     d, pose = ref[-1]
     assert d["samples"] == 100000

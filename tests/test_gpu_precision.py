@@ -23,6 +23,7 @@ def test_precision_slice_within_fp64_tolerance(ctx, oracle):
     b.sync()
     res = b.results()
     b.close()
+    assert all(r["status"] == 0 and r["candidate_overflow"] == 0 for r in res)
     oq, ot, _ = oracle.estimate_batch(frames, threads=os.cpu_count() or 1)
     rep = bench.precision_report(frames, res, oq, ot)
     allr = rep["all"]

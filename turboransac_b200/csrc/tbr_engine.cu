@@ -2564,11 +2564,21 @@ extern "C" tbr_status tbr_msac_score_noalloc(const double *x_dev, const double *
                                               double *scores_dev, int64_t *counts_dev, void *stream) {
     if (!x_dev || !X_dev || !poses_dev || !scores_dev || !counts_dev || n < 1 || n_poses < 0)
         return fail(TBR_ERR_INVALID_ARG, "tbr_msac_score_noalloc: bad arguments");
+    if (!(sq_threshold > 0.0) || !std::isfinite(sq_threshold))
+        return fail(TBR_ERR_INVALID_ARG, "tbr_msac_score_noalloc: sq_threshold must be positive and finite");
     if (n_poses > kNoAllocMaxPoses)
         return fail(TBR_ERR_INVALID_ARG, "tbr_msac_score_noalloc: at most 1024 poses per call (fixed scratch size)");
     if (n_poses == 0) return TBR_OK;
     int dev = 0;
     TBR_CUDA(cudaGetDevice(&dev));
+    if (stream) {  // the scratch address is the current device's: the stream must belong to it
+        int sdev = -1;
+        TBR_CUDA(cudaStreamGetDevice((cudaStream_t)stream, &sdev));
+        if (sdev != dev)
+            return fail(TBR_ERR_INVALID_ARG,
+                        "tbr_msac_score_noalloc: the stream belongs to device " + std::to_string(sdev) +
+                            " but device " + std::to_string(dev) + " is current; make the stream's device current");
+    }
     NoAllocScratch *sc = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mu);

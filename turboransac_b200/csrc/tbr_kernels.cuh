@@ -103,11 +103,13 @@ struct __align__(16) FrameDev {
     int64_t min_samples;  // no stop before this many samples (honoured min_iterations; else 0)
     double prosac_TN;     // PROSAC: samples after which it draws uniformly
     int32_t prosac;       // 1: PROSAC sampling (honoured progressive_sampling), table in Pools::prosac64
-    int32_t prosac_pad;
+    int32_t split;        // > 0: at most this many rounds (forced mode: samples) per step, set when a
+                          // step's re-rank candidates did not fit (k_select); results do not change
     int64_t force_samples;
     double log_missing, trials_mult;
     int32_t skip_refine, hr;  // hr: hypotheses per lane in the scoring pass (2 * HP)
-    int32_t quirk, pad1;      // stop rule: 1 = x86 int-conversion quirk of the reference  // hr: hypotheses per lane in the scoring pass
+    int32_t quirk;            // stop rule: 1 = x86 int-conversion quirk of the reference
+    int32_t redo;             // 1: this step's candidates did not fit; k_finalize discards the step
     int64_t lm_max_iter;
     double lm_cam[4];  // camera of the LM residual: K/f for the estimate path, K for bundle_adjust
     double lm_inv_sq_thr, lm_grad_tol, lm_step_tol, lm_lambda0, lm_min_lambda, lm_max_lambda;
@@ -391,6 +393,7 @@ __global__ void k_plan(Pools P) {
         if (f->status == kRansac) {
             if (f->force_samples > 0) {
                 samples = f->force_samples - f->samples_done;
+                if (f->split > 0) samples = min(samples, (int64_t)f->split);
                 rounds = 1;
                 div = f->force_samples;
             } else {
@@ -409,6 +412,7 @@ __global__ void k_plan(Pools P) {
                 // so a stop bound that shrinks once a better model turns up wastes
                 // at most the last step's overshoot.
                 if (f->steps >= 1) r = min(r, (int64_t)4 << min(f->steps - 1, 5));
+                if (f->split > 0) r = min(r, (int64_t)f->split);
                 if (r < 1) r = 1;
                 rounds = r;
                 samples = r * f->B;
@@ -1146,18 +1150,41 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
 }
 
 // ---------------------------------------------------------- candidates -----
-// Candidates for the exact FP64 re-rank: every hypothesis whose FP32 score is
-// within a band of the running minimum (over this step's rounds so far and the
-// best of earlier steps). The band, 2^-12 of the score plus one tau^2, is far
-// wider than the FP32-vs-FP64 score difference, so the FP64 best of every round
-// that can change the running best -- including every exact tie -- is among
-// the candidates. Above kMaxCandFrame candidates the band is halved (up to 7
-// times) before the overflow flag is raised.
+// Candidates for the exact FP64 re-rank: every hypothesis whose FP32 score s
+// lies within a band of the running minimum thr of its round (over this
+// step's rounds so far and the best of earlier steps), s <= thr + thr/4096 + 1
+// (scores in tau^2 units). The FP32 score of a hypothesis is within 1e-5 of
+// its FP64 score relative (tested), so the FP64 best of every round that can
+// change the running best -- including every exact tie -- lies inside the
+// safe band thr + thr/32768 + 1/2, twice that error on both sides with an
+// absolute margin, and the candidate band contains the safe band. The band is
+// never narrowed. When more than kMaxCandFrame hypotheses fall inside it:
+//   * a step of several rounds (forced mode: more than kSplitSamples samples)
+//     is redone: the frame's later steps are limited to one round (forced:
+//     kSplitSamples samples), which bounds the candidates by 4 * B, and
+//     k_finalize discards this step. A frame's samples, selection and stop
+//     point do not depend on how its rounds are grouped into steps, so this
+//     changes no result;
+//   * a single round (B > kMaxCandFrame / 4) keeps the kMaxCandFrame smallest
+//     keys (margin above thr in safe-band units, then sample id): the same
+//     subset on every run, alone or in a mix; if that drops a hypothesis
+//     inside the safe band, the frame's overflow flag is raised.
+// A step whose candidates do not fit the step's shared pool is redone as
+// well (the pool is claimed in launch order, which only delays a frame).
+constexpr int kSplitSamples = kMaxCandFrame / 4;
+__device__ __forceinline__ unsigned long long cand_key(float s, float t, float inv_safe, int64_t id,
+                                                       int64_t first) {
+    const float u = fmaxf((s - t) * inv_safe, 0.0f);
+    return ((unsigned long long)__float_as_uint(u) << 32) | (unsigned long long)(uint32_t)(id - 4 * first);
+}
+
 __global__ void k_select(Pools P) {
-    __shared__ float thr[kMaxRoundsPerStep];
+    __shared__ float thr[kMaxRoundsPerStep], inv_safe[kMaxRoundsPerStep];
     __shared__ int rh[kMaxRoundsPerStep];
-    __shared__ int cnt[8];
-    __shared__ int level, fill;
+    __shared__ unsigned hist[256];
+    __shared__ int cnt0, fill, mode, drop_safe;
+    __shared__ unsigned need;
+    __shared__ unsigned long long kstar;
     __shared__ long long base;
     const int slot = P.active[blockIdx.x];
     FrameDev &f = P.frames[slot];
@@ -1170,57 +1197,114 @@ __global__ void k_select(Pools P) {
             const float rm = k == ~0ull ? __int_as_float(0x7f800000) : __uint_as_float((unsigned)(k >> 32));
             pm = fminf(pm, rm);
             thr[r] = pm;
+            inv_safe[r] = __frcp_rn(pm * (1.0f / 32768.0f) + 0.5f);
         }
+        cnt0 = 0;
         fill = 0;
+        drop_safe = 0;
     }
-    if (threadIdx.x < 8) cnt[threadIdx.x] = 0;
     for (int r = threadIdx.x; r < kMaxRoundsPerStep; r += blockDim.x) rh[r] = 0;
     __syncthreads();
     const int nh = f.hyp_count;
     const int64_t hb = f.hyp_base;
-    int my[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int my = 0;
     for (int i = threadIdx.x; i < nh; i += blockDim.x) {
         const float s = P.hS32[hb + i];
         const int64_t r = ((P.hId[hb + i] >> 2) - f.step_first) / f.step_div;
         const float pm = thr[r];
-        const float band = pm * (1.0f / 4096.0f) + 1.0f;
         atomicAdd(&rh[r], 1);
-#pragma unroll
-        for (int l = 0; l < 8; ++l) my[l] += (s <= pm + band * (1.0f / (float)(1 << l))) ? 1 : 0;
+        my += (s <= pm + (pm * (1.0f / 4096.0f) + 1.0f)) ? 1 : 0;
     }
-#pragma unroll
-    for (int l = 0; l < 8; ++l) {
-        const int v = warp_sum(my[l]);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&cnt[l], v);
-    }
+    my = warp_sum(my);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&cnt0, my);
     __syncthreads();
     for (int r = threadIdx.x; r < kMaxRoundsPerStep; r += blockDim.x) f.round_hyps[r] = rh[r];
     if (threadIdx.x == 0) {
-        int lv = 7;
-        for (int l = 0; l < 8; ++l)
-            if (cnt[l] <= kMaxCandFrame) { lv = l; break; }
-        level = lv;
-        int want = min(cnt[lv], kMaxCandFrame);
-        long long b0 = (long long)atomicAdd(&P.counters[kCCandNext], (unsigned long long)want);
-        if (b0 + want > P.cand_cap) want = (int)max(0LL, (long long)P.cand_cap - b0);
-        f.overflow |= (cnt[7] > kMaxCandFrame || want < min(cnt[lv], kMaxCandFrame)) ? 1 : 0;
+        const bool forced = f.force_samples > 0;
+        const bool splittable = forced ? f.step_samples > kSplitSamples : f.step_rounds > 1;
+        int want = cnt0, md = 0;                 // 0: every candidate
+        if (cnt0 > kMaxCandFrame) {
+            if (splittable) {
+                f.split = forced ? kSplitSamples : 1;
+                want = 0;
+                md = 2;                          // redo the step
+            } else {
+                want = kMaxCandFrame;
+                md = 1;                          // the smallest keys
+            }
+        }
+        long long b0 = 0;
+        if (want > 0) {
+            b0 = (long long)atomicAdd(&P.counters[kCCandNext], (unsigned long long)want);
+            if (b0 + want > P.cand_cap) {        // the step's pool is exhausted: redo
+                want = 0;
+                md = 2;
+            }
+        }
+        if (md == 2) f.redo = 1;
+        mode = md;
+        need = (unsigned)want;
+        kstar = ~0ull;
         base = b0;
         f.cand_base = b0;
         f.cand_count = want;
     }
     __syncthreads();
-    const float scale = 1.0f / (float)(1 << level);
+    if (mode == 2 || need == 0) return;
+    if (mode == 1) {
+        // Radix select (8 bits per pass) of the need-th smallest key among
+        // the candidates; keys are distinct (the id part), so exactly `need`
+        // keys are <= kstar.
+        unsigned long long prefix = 0;
+        for (int pass = 0; pass < 8; ++pass) {
+            const int shift = 56 - 8 * pass;
+            const unsigned long long hi_mask = pass == 0 ? 0ull : (~0ull << (shift + 8));
+            for (int b = threadIdx.x; b < 256; b += blockDim.x) hist[b] = 0;
+            __syncthreads();
+            for (int i = threadIdx.x; i < nh; i += blockDim.x) {
+                const float s = P.hS32[hb + i];
+                const int64_t id = P.hId[hb + i];
+                const int64_t r = ((id >> 2) - f.step_first) / f.step_div;
+                const float pm = thr[r];
+                if (!(s <= pm + (pm * (1.0f / 4096.0f) + 1.0f))) continue;
+                const unsigned long long key = cand_key(s, pm, inv_safe[r], id, f.step_first);
+                if ((key & hi_mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned cum = 0, want_rank = need;
+                int b = 0;
+                for (; b < 255; ++b) {
+                    if (cum + hist[b] >= want_rank) break;
+                    cum += hist[b];
+                }
+                need = want_rank - cum;
+                kstar = prefix | ((unsigned long long)b << shift);
+            }
+            __syncthreads();
+            prefix = kstar;
+        }
+    }
+    const unsigned long long kmax = mode == 1 ? kstar : ~0ull;
     const int cap = f.cand_count;
     for (int i = threadIdx.x; i < nh; i += blockDim.x) {
         const float s = P.hS32[hb + i];
-        const int64_t r = ((P.hId[hb + i] >> 2) - f.step_first) / f.step_div;
+        const int64_t id = P.hId[hb + i];
+        const int64_t r = ((id >> 2) - f.step_first) / f.step_div;
         const float pm = thr[r];
-        const float band = pm * (1.0f / 4096.0f) + 1.0f;
-        if (s <= pm + band * scale) {
-            const int c = atomicAdd(&fill, 1);
-            if (c < cap) P.cHyp[base + c] = i;
+        if (!(s <= pm + (pm * (1.0f / 4096.0f) + 1.0f))) continue;
+        if (mode == 1) {
+            const unsigned long long key = cand_key(s, pm, inv_safe[r], id, f.step_first);
+            if (key > kmax) {
+                if (__uint_as_float((unsigned)(key >> 32)) <= 1.0f) drop_safe = 1;
+                continue;
+            }
         }
+        const int c = atomicAdd(&fill, 1);
+        if (c < cap) P.cHyp[base + c] = i;
     }
+    __syncthreads();
+    if (threadIdx.x == 0 && drop_safe) f.overflow = 1;
 }
 
 __global__ void k_rescore_plan(Pools P) {
@@ -1367,6 +1451,16 @@ __global__ void __launch_bounds__(256) k_finalize(Pools P) {
     if (f.status != kRansac) return;
     if (f.step_samples == 0) {  // waiting for hypothesis capacity
         if (threadIdx.x == 0) atomicAdd(&P.counters[kCStillRansac], 1ull);
+        return;
+    }
+    const int redo = f.redo;
+    __syncthreads();
+    if (redo) {  // the step's re-rank candidates did not fit (k_select): its rounds run again
+        if (threadIdx.x == 0) {
+            f.redo = 0;
+            f.steps += 1;
+            atomicAdd(&P.counters[kCStillRansac], 1ull);
+        }
         return;
     }
     for (int r = threadIdx.x; r < kMaxRoundsPerStep; r += blockDim.x) {
