@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--frames", type=int, default=256)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=10.0)
+    ap.add_argument("--serve-seconds", type=float, default=60.0)
     ap.add_argument("--hr", type=int, default=0, help="scoring hypotheses per thread (4/8, 0 = auto)")
     ap.add_argument("--tensor", action="store_true",
                     help="score with the tensor-core shape (8192-point chunks) instead of autotuning")
@@ -164,7 +164,7 @@ def cpu_baseline(frames, seconds_target=15.0):
     m = min(m, len(frames))
     sample = frames[:m]
     t0 = time.perf_counter()
-    o.estimate_batch(sample, threads=cores)
+    oq, ot, osmp = o.estimate_batch(sample, threads=cores)
     dt = time.perf_counter() - t0
     # one core, on a smaller sample (~5 s)
     m1 = int(max(1, min(len(frames), 5.0 / max(per_frame_wall * cores, 1e-6))))
@@ -178,7 +178,65 @@ def cpu_baseline(frames, seconds_target=15.0):
         pass
     return {"value": m / dt, "unit": "frames/s", "cores": cores, "kind": "port",
             "sample": f"first {m} frames of the batched workload, FP64 oracle, {cores} threads over frames",
-            "seconds": dt, "one_core": {"value": m1 / dt1, "frames": m1}, "cpu_model": model}
+            "seconds": dt, "one_core": {"value": m1 / dt1, "frames": m1}, "cpu_model": model}, (oq, ot, osmp)
+
+
+def precision_vs_oracle(frames, res, oracle_out):
+    """Deviation of the GPU poses from the FP64 oracle's on the same frames and
+    samples (the oracle run timed as the CPU baseline)."""
+    import numpy as np
+    oq, ot, osmp = oracle_out
+    m = len(oq)
+    rep = precision_report(frames[:m], res[:m], oq, ot)["all"]
+    rep["frames"] = m
+    rep["same_sample_count"] = float(np.mean([int(res[i]["samples"]) == int(osmp[i]) for i in range(m)]))
+    rep["bar"] = "1e-6 rad / 1e-6 m against the FP64 CPU pipeline on identical Philox samples"
+    return rep
+
+
+def config0_plain(ctx, reps=3):
+    """Plain single frames (N=2000, 40 % inliers, the reference's call): latency."""
+    import numpy as np
+
+    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, RansacOptions_cuda, scenes
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    frames = [scenes.plain_frame(i) for i in range(64)]
+    lat, gpu, ok = [], [], 0
+    for rep in range(1 + reps):
+        for f in frames:
+            t0 = time.perf_counter()
+            st, pose, _ = ctx.estimate_absolute_pose(f.uv, f.xyz, Camera_cuda(1, 640, 480, list(f.K)), ro,
+                                                     BundleOptions_cuda(), seed=f.seed)
+            dt = 1000.0 * (time.perf_counter() - t0)
+            if rep:
+                lat.append(dt)
+                gpu.append(st.details["gpu_ms"])
+                ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
+                ok += (ae < 5.0 and te < 5.0)
+    return {"config": "plain frame: N=2000, 40 % inliers, sigma 1 px, 4 px, 1000 samples/round, p=0.9999",
+            "calls": len(lat), "frames_per_s": len(lat) / (sum(lat) / 1000.0),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "gpu_p50_ms": float(np.percentile(gpu, 50)), "success_rate": ok / len(lat)}
+
+
+def config1_scoring(ctx, reps=5, hr=0):
+    """Scoring-bound single frame: N=20000, 15 % inliers, exactly 4096 samples."""
+    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, RansacOptions_cuda, scenes
+    f = scenes.scoring_frame(0)
+    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
+    cam = Camera_cuda(1, 640, 480, list(f.K))
+    ms = []
+    for i in range(2 + reps):
+        st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, BundleOptions_cuda(), seed=f.seed,
+                                                   force_samples=4096, hyp_per_thread=hr)
+        if i >= 2:
+            ms.append(st.details["gpu_ms"])
+    d = st.details
+    pairs = d["hypotheses"] * f.n
+    return {"config": "scoring-bound frame: N=20000, 15 % inliers, exactly 4096 samples (early stop off)",
+            "samples": d["samples"], "hypotheses": d["hypotheses"], "pairs": pairs,
+            "gpu_ms_per_call": statistics.mean(ms), "pairs_per_s": pairs / (statistics.mean(ms) / 1000.0),
+            "candidate_overflow": d["candidate_overflow"]}
 
 
 def run_serving(ctx, seconds, rate=2000.0, pool=600, budget=8 << 30, shape=None):
@@ -272,7 +330,7 @@ def run_plain_serving(ctx, reqs, count=200):
             "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
 
 
-def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30, shape=None):
+def run_serving_capacity(ctx, reqs, repeats=10, budget=8 << 30, shape=None):
     """Served throughput at saturation: the serving requests submitted at once
     (repeats x the pool), completion rate of the continuous-batching server."""
     import numpy as np
@@ -296,6 +354,7 @@ def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30, shape=None):
         if not g:
             break
         got += g
+    sst = srv.stats()
     srv.close()
     lat = np.array([g["latency_ms"] for g in got])
     ok = 0
@@ -305,7 +364,10 @@ def run_serving_capacity(ctx, reqs, repeats=3, budget=8 << 30, shape=None):
         ok += (g["status"] == 0 and ae < 5.0 and te < 5.0)
     return {"frames_per_s": len(got) / dt, "requests": len(got), "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "success_rate": ok / max(len(got), 1),
-            "load": f"{repeats} x {len(reqs)} serving requests submitted at once"}
+            "load": f"{repeats} x {len(reqs)} serving requests submitted at once", "seconds": dt,
+            "server": {"steps": sst["steps"], "mean_resident": sst["resident_sum"] / max(sst["steps"], 1),
+                       "device_wait_ms": sst["device_wait_ms"], "host_stage_ms": sst["host_stage_ms"],
+                       "host_retire_ms": sst["host_retire_ms"], "host_launch_ms": sst["host_launch_ms"]}}
 
 
 def run_reference(args, world, rank):
@@ -317,24 +379,33 @@ def run_reference(args, world, rank):
     from oracle.oracle import Oracle
     o = Oracle()
     cores = os.cpu_count() or 1
-    m = min(len(frames), max(cores, 16))
-    sample = frames[:m]
+    # Every step estimates all frames of the workload (the same frames, seeds and
+    # samples as the GPU arm). If a step is slow on this host, fewer warm-up
+    # steps keep the run within a few minutes; the timed steps are all run.
     times = []
-    for i in range(args.warmup + args.steps):
+    t_start = time.perf_counter()
+    warm = args.warmup
+    i = 0
+    while len(times) < args.steps:
         t0 = time.perf_counter()
-        o.estimate_batch(sample, threads=cores)
+        o.estimate_batch(frames, threads=cores)
         dt = time.perf_counter() - t0
-        if i >= args.warmup:
+        if i >= warm:
             times.append(dt)
-    fps = m * len(times) / sum(times)
+        elif (args.warmup + args.steps) * dt > 240.0:
+            warm = min(warm, 1)
+        i += 1
+    fps = len(frames) * len(times) / sum(times)
     rcuda = reference_cuda_build(frames, args)
     line = {"metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.mean(times), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "global_batch": m, "sample": f"first {m} frames"},
-            "impl": "reference",
+            "warmup": min(warm, i - len(times)), "ms_per_step": 1000.0 * statistics.mean(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "global_batch": len(frames), "parallelism": "host threads"},
+            "impl": "reference", "same_config": True,
             "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": cores, "kind": "port",
-                             "sample": f"first {m} frames of the batched workload per step, {cores} threads"},
+                             "sample": f"all {len(frames)} frames of the batched workload per step, "
+                                       f"FP64 oracle (same algorithm, same samples), {cores} threads over frames",
+                             "seconds_total": time.perf_counter() - t_start},
             "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "reference_cuda": rcuda}
     print(json.dumps(line), flush=True)
@@ -372,48 +443,17 @@ def reference_cuda_build(frames, args):
 
 def run_case_plain(args):
     """Plain single frames (N=2000, 40 % inliers, the reference's call): latency."""
-    import numpy as np
-
-    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda, scenes
+    from turboransac_b200 import Context
     ctx = Context(0, 1 << 30)
-    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
-    frames = [scenes.plain_frame(i) for i in range(64)]
-    lat, gpu, ok = [], [], 0
-    for rep in range(1 + max(1, args.steps // 5)):
-        for f in frames:
-            t0 = time.perf_counter()
-            st, pose, _ = ctx.estimate_absolute_pose(f.uv, f.xyz, Camera_cuda(1, 640, 480, list(f.K)), ro,
-                                                     BundleOptions_cuda(), seed=f.seed)
-            dt = 1000.0 * (time.perf_counter() - t0)
-            if rep:
-                lat.append(dt)
-                gpu.append(st.details["gpu_ms"])
-                ae, te = scenes.pose_error(pose.R(), pose.t, f.R_gt, f.t_gt)
-                ok += (ae < 5.0 and te < 5.0)
-    print(json.dumps({"case": "plain", "frames": len(lat), "frames_per_s": len(lat) / (sum(lat) / 1000.0),
-                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                      "gpu_p50_ms": float(np.percentile(gpu, 50)), "success_rate": ok / len(lat)}), flush=True)
+    print(json.dumps(dict(case="plain", **config0_plain(ctx, reps=max(1, args.steps // 5)))), flush=True)
     ctx.close()
 
 
 def run_case_scoring(args):
     """Scoring-bound single frame: N=20000, 15 % inliers, exactly 4096 samples."""
-    from turboransac_b200 import BundleOptions_cuda, Camera_cuda, Context, RansacOptions_cuda, scenes
-    f = scenes.scoring_frame(0)
+    from turboransac_b200 import Context
     ctx = Context(0, 2 << 30)
-    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
-    cam = Camera_cuda(1, 640, 480, list(f.K))
-    ms = []
-    for i in range(args.warmup + args.steps):
-        st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, cam, ro, BundleOptions_cuda(), seed=f.seed,
-                                                   force_samples=4096, hyp_per_thread=args.hr)
-        if i >= args.warmup:
-            ms.append(st.details["gpu_ms"])
-    d = st.details
-    pairs = d["hypotheses"] * f.n
-    print(json.dumps({"case": "scoring", "n": f.n, "samples": d["samples"], "hypotheses": d["hypotheses"],
-                      "pairs": pairs, "gpu_ms_per_call": statistics.mean(ms),
-                      "pairs_per_s_call": pairs / (statistics.mean(ms) / 1000.0)}), flush=True)
+    print(json.dumps(dict(case="scoring", **config1_scoring(ctx, reps=args.steps, hr=args.hr))), flush=True)
     ctx.close()
 
 
@@ -589,14 +629,8 @@ def main():
     nominal = 148 * 256 * 1965e6 / 1e12
     # The scoring kernel that ran: the FP32 pass or the tensor-core shape.
     tensor = args.tensor or bool(tuned and tuned["best"]["points_per_iter"] == 128)
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "k_score_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            tj = json.load(open(tpath))
-            traffic = tj.get("bytes_per_launch_batched_tc" if tensor else "bytes_per_launch_batched")
-        except Exception:
-            traffic = None
+    kernel = "k_score_tc2" if tensor else "k_score"
+    traffic, traffic_source = stored_traffic(kernel)
 
     # e2e: public call, host buffers in, results out, every step. Inputs in
     # page-locked host memory (as a data loader would hand them over); the
@@ -658,9 +692,12 @@ def main():
         plain = {"frames_per_s": len(lat) / (sum(lat) / 1000.0), "p50_ms": float(np.percentile(lat, 50)),
                  "p99_ms": float(np.percentile(lat, 99)), "frames": len(lat)}
 
-    cpu = None
+    cpu = precision = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(frames)
+        cpu, oracle_out = cpu_baseline(frames)
+        precision = precision_vs_oracle(frames, res, oracle_out)
+    c0 = config0_plain(ctx) if not args.no_plain else None
+    c1 = config1_scoring(ctx)
 
     serving = None
     if args.serve_seconds > 0:
@@ -696,7 +733,8 @@ def main():
             "pairs_scored_per_batch": pairs,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32 if peak_fp32 else None, "traffic": traffic,
-                         "kernel": "k_score_tc" if tensor else "k_score", "flop_per_pair": FLOP_PER_PAIR,
+                         "traffic_source": traffic_source,
+                         "kernel": kernel, "flop_per_pair": FLOP_PER_PAIR, "pairs_per_s": pairs / (score_ms / 1000.0),
                          "accounting": ("27 FP32-equivalent FLOP per pair: the projection's 18 on the tensor "
                                         "cores (tcgen05 TF32, split operands), the rest on the FP32 pipe")
                                        if tensor else "27 FP32 FLOP per pair on the FP32 pipe",
@@ -713,6 +751,10 @@ def main():
                                   "d2h_bytes_per_step": d2h,
                                   "inputs": "correspondences already in device memory (CUDA tensors)"},
             "plain_call": plain,
+            "config0_plain": c0,
+            "config1_scoring": c1,
+            "precision": precision,
+            "candidate_overflow_frames": int(sum(int(r["candidate_overflow"]) for r in res)),
             "serving": serving,
             "speedup_vs_plain": (value / plain["frames_per_s"]) if plain else None,
             # per graph launch: the reset, per engine step 8 RANSAC kernels + 3
@@ -725,6 +767,20 @@ def main():
     ctx.close()
     if pg is not None:
         pg.destroy_process_group()
+
+
+def stored_traffic(kernel: str):
+    """DRAM bytes per launch of the scoring kernel on this workload, from the
+    ncu capture summarised under profiles/ (ncu does not run inside the bench):
+    (bytes, a note naming the capture and its date) or (None, why)."""
+    tpath = os.path.join(ROOT, "profiles", "k_score_traffic.json")
+    try:
+        k = json.load(open(tpath))["kernels"][kernel]
+        return k["bytes_per_launch"], (f"not measured in this run: ncu dram__bytes_read.sum + "
+                                       f"dram__bytes_write.sum per {kernel} launch, captured {k['captured']} "
+                                       f"({k['summary']})")
+    except Exception:
+        return None, f"no stored ncu capture of {kernel} on this workload"
 
 
 def fp32_peak_tflops(ctx) -> float | None:

@@ -21,7 +21,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libtbr_refhost.so")
-REF_SRC = "/root/reference/Module/TbrCudaPnP"
+# The reference tree (the TurboRANSAC checkout): TBR_REF_TREE, by default where
+# this build environment mounts it.
+REF_TREE = os.environ.get("TBR_REF_TREE", "/root/reference")
+REF_SRC = os.path.join(REF_TREE, "Module", "TbrCudaPnP")
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _ip32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")

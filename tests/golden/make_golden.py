@@ -13,7 +13,7 @@ Runs the reference's header code and entry.cu compiled on the host
   entry.npz      estimate_absolute_pose_cuda post-RANSAC path with an injected RANSAC
                  pose (entry.cu:28-144): inlier mask and refined (q, t)
 
-Usage: python tests/golden/make_golden.py   (needs /root/reference; run once)
+Usage: python tests/golden/make_golden.py   (needs the reference tree, TBR_REF_TREE; run once)
 """
 from __future__ import annotations
 

@@ -78,11 +78,11 @@ def test_shim_matches_python_api():
             ctx.close()
 
 
-REF_MAIN = "/root/reference/TbrMain/src/main.cu"
+REF_MAIN = os.path.join(os.environ.get("TBR_REF_TREE", "/root/reference"), "TbrMain", "src", "main.cu")
 TBRMAIN = os.path.join(ROOT, "oracle", "_ref", "TbrMain")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference tree not present")
+@pytest.mark.skipif(not os.path.exists(REF_MAIN), reason="reference tree (TBR_REF_TREE) not present")
 def test_reference_evaluator_compiles_unchanged():
     """TbrMain/src/main.cu, untouched, builds against the drop-in headers and libtbr.so."""
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "tbrmain"], check=True)
