@@ -151,9 +151,11 @@ void tbr_default_bundle_options(tbr_bundle_options *opts);
 /* device: CUDA ordinal. workspace_bytes: device memory the context may use
  * (0 = 1 GiB). The workspace is allocated once and reused by every call. */
 tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context **out);
-/* Destroy every batch made on the context first (a batch uses the context's
- * workspace and stream); a server takes only the device from its context and
- * may outlive it. */
+/* Also frees every batch made on the context that is still alive (a batch
+ * uses the context's workspace and stream): those handles are dead afterwards,
+ * and tbr_batch_destroy on one is a no-op, any other call on one returns
+ * TBR_ERR_INVALID_ARG. A server takes only the device from its context and may
+ * outlive it. */
 void tbr_context_destroy(tbr_context *ctx);
 
 /* estimate_absolute_pose_cuda (entry.h:13-19). Host buffers:
@@ -236,7 +238,7 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
 tbr_status tbr_batch_run(tbr_batch *b);      /* asynchronous on the context stream */
 tbr_status tbr_batch_sync(tbr_batch *b);     /* waits; returns the first device error */
 tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results);
-void tbr_batch_destroy(tbr_batch *b);        /* before its context's tbr_context_destroy */
+void tbr_batch_destroy(tbr_batch *b);        /* no-op if its context already freed it */
 
 /* Per-kernel device time of one batch run, stepped from the host with a CUDA
  * event pair around every kernel launch on the context stream (slower than

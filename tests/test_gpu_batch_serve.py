@@ -50,6 +50,29 @@ def test_batch_graph_matches_plain_calls(ctx):
     b.close()
 
 
+def test_lm_on_a_warp_equals_lm_on_a_cta(ctx):
+    """A frame below 2048 inliers that finishes RANSAC before a batch's last
+    step is refined on one warp beside the next step's RANSAC; a plain call
+    refines it on a CTA after its last step. Both paths take the same sums in
+    the same order: the poses are equal bit for bit."""
+    fr = mixed_frames()
+    ref = [plain(ctx, f) for f in fr]
+    b = Batch(ctx, fr, RO)
+    b.run()
+    b.sync()
+    res = b.results()
+    b.close()
+    last = max(r["steps"] for r in res)
+    checked = 0
+    for r, (d, pose) in zip(res, ref):
+        if r["num_inliers"] < 2048 and r["steps"] < last:
+            assert r["lm_iterations"] == d["lm_iterations"]
+            np.testing.assert_array_equal(r["q"], pose.q)
+            np.testing.assert_array_equal(r["t"], pose.t)
+            checked += 1
+    assert checked >= 3, checked
+
+
 def test_estimate_batch_host_buffers(ctx):
     fr = mixed_frames()[:8]
     out = estimate_batch(ctx, fr, RO, masks=True)
@@ -339,6 +362,29 @@ def test_context_close_releases_its_batches_first(ctx):
     assert s["id"] == rid and s["status"] == 0
     same(s, s["q"], s["t"], d, pose)
     srv.close()
+
+
+def test_context_destroy_frees_live_batches_through_the_c_abi(ctx):
+    """A C caller that destroys the context before its batch: the context frees
+    the batch, later calls on the dead handle are refused and its destroy is a
+    no-op (no use after free)."""
+    from turboransac_b200 import Context, _lib
+    L = _lib.lib()
+    f = scenes.make_frame(800, 0.5, 1.0, 31002)
+    c2 = Context(0, 1 << 30)
+    b = Batch(c2, [f], RO)
+    h = b._h
+    c2._batches.discard(b)  # as a C caller: only the C library knows about the batch
+    L.tbr_context_destroy(c2.handle)
+    c2._h = None
+    assert L.tbr_batch_run(h) == 1 and b"destroyed" in L.tbr_last_error()
+    res = (_lib.FrameResultC * 1)()
+    assert L.tbr_batch_results(h, res) == 1
+    L.tbr_batch_destroy(h)  # no-op
+    b._h = None
+    d, pose = plain(ctx, f)  # other contexts are unaffected
+    (r,) = estimate_batch(ctx, [f], RO)
+    same(r, r["q"], r["t"], d, pose)
 
 
 def test_batched_calls_reject_what_the_plain_call_rejects(ctx):

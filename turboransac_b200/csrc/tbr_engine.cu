@@ -299,6 +299,7 @@ class Engine {
         P.active = d_active;
         P.num_sms = num_sms;
         P.lm_cluster_min = kLMClusterMin;
+        P.lm_warp_max = kLMWarpMax;
         TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
         TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
         TBR_CUDA(cudaMallocHost(&h_results, sizeof(FrameResult) * kMaxActive));
@@ -445,6 +446,7 @@ class Engine {
         auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
         beg(8); k_inliers<<<n_active, 1024, 0, st>>>(Q); end(8);
         beg(9);
+        if (Q.lm_warp_max > 0) k_lm_warp<<<(n_active + kLMWarpFrames - 1) / kLMWarpFrames, kLMWarpFrames * 32, 0, st>>>(Q);
         k_lm_small<<<n_active, kLMSmallThreads, 0, st>>>(Q);
         k_lm<<<n_active * kLMCluster, kLMThreads, 0, st>>>(Q);
         end(9);
@@ -553,6 +555,7 @@ class Engine {
             if (ok) {
                 Pools Qt = Q;  // nothing runs beside the last step's refinement
                 Qt.lm_cluster_min = kLMClusterMinTail;
+                Qt.lm_warp_max = 0;
                 launch_refine(Qt, n, stream);
                 ok = cudaStreamEndCapture(stream, &tail) == cudaSuccess;
             }
@@ -1222,6 +1225,9 @@ struct tbr_context {
     Engine E;
 };
 
+struct tbr_batch;
+static void destroy_context_batches(tbr_context *ctx);
+
 // =================================================================== C ABI ==
 extern "C" {
 
@@ -1270,7 +1276,11 @@ tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context 
     return TBR_OK;
 }
 
-void tbr_context_destroy(tbr_context *ctx) { delete ctx; }
+void tbr_context_destroy(tbr_context *ctx) {
+    if (!ctx) return;
+    destroy_context_batches(ctx);
+    delete ctx;
+}
 
 static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
                                   std::vector<FrameResult> &res, std::vector<uint8_t *> masks,
@@ -1658,6 +1668,17 @@ struct tbr_batch {
     Engine::Profile prof;
 };
 
+// Live batches. Destroying a context frees the batches made on it; their
+// handles then stay known as dead, so that a later call on one is refused
+// instead of touching freed memory.
+static std::mutex g_batches_mu;
+static std::unordered_map<tbr_batch *, tbr_context *> g_batches;
+
+static bool live_batch(tbr_batch *b) {
+    std::lock_guard<std::mutex> lk(g_batches_mu);
+    return b && g_batches.count(b) != 0;
+}
+
 static void batch_free(tbr_batch *b) {
     if (!b) return;
     Engine &E = b->ctx->E;
@@ -1671,10 +1692,27 @@ static void batch_free(tbr_batch *b) {
     for (auto &e : b->prof.ev)
         if (e) cudaEventDestroy(e);
     for (size_t i = 0; i < b->slots.size(); ++i) {
-        E.blocks.release(b->blk_off[i], b->n_blocks[i]);
+        if (i < b->blk_off.size()) E.blocks.release(b->blk_off[i], b->n_blocks[i]);
         E.free_slots.push_back(b->slots[i]);
     }
     delete b;
+}
+
+static void destroy_context_batches(tbr_context *ctx) {
+    std::vector<tbr_batch *> mine;
+    {
+        std::lock_guard<std::mutex> lk(g_batches_mu);
+        for (auto it = g_batches.begin(); it != g_batches.end();) {
+            if (it->second == ctx) {
+                mine.push_back(it->first);
+                it = g_batches.erase(it);
+            } else {
+                ++it;
+            }
+        }
+    }
+    std::lock_guard<std::mutex> lk(ctx->E.mu);
+    for (tbr_batch *b : mine) batch_free(b);
 }
 
 extern "C" {
@@ -1699,9 +1737,15 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
     b->ctx = ctx;
     b->o = make_run_options(&ro, nullptr, ext);
     int64_t max_n = 0;
-    tbr_status st = admit_frames(E, fr, b->o, b->slots, max_n);
+    std::vector<FrameDev> devs;
+    tbr_status st = admit_frames(E, fr, b->o, b->slots, max_n, &devs);
+    for (size_t i = 0; i < b->slots.size() && i < devs.size(); ++i) {  // what batch_free releases
+        b->ns.push_back(devs[i].n);
+        b->blk_off.push_back(devs[i].blk_off);
+        b->n_blocks.push_back(devs[i].n_blocks);
+    }
     if (st) {
-        delete b;
+        batch_free(b);
         return st;
     }
     // The batch keeps its own active list so that other calls on the context
@@ -1717,19 +1761,11 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
     b->Q.n_active = n_frames;
     E.launch_prep(b->Q, n_frames, max_n);
     // Snapshot the prepared frame states (AABB centre included).
-    std::vector<FrameDev> hf(n_frames);
     for (int i = 0; i < n_frames; ++i)
         cudaMemcpyAsync(b->d_init + i, E.P.frames + b->slots[i], sizeof(FrameDev), cudaMemcpyDeviceToDevice, E.stream);
-    for (int i = 0; i < n_frames; ++i)
-        cudaMemcpyAsync(&hf[i], E.P.frames + b->slots[i], sizeof(FrameDev), cudaMemcpyDeviceToHost, E.stream);
     if (cudaStreamSynchronize(E.stream) != cudaSuccess) {
         batch_free(b);
         return fail(TBR_ERR_CUDA, "batch upload failed");
-    }
-    for (int i = 0; i < n_frames; ++i) {
-        b->ns.push_back(hf[i].n);
-        b->blk_off.push_back(hf[i].blk_off);
-        b->n_blocks.push_back(hf[i].n_blocks);
     }
     E.pp = b->o.pp;
     bool ok = E.build_loop_graph(b->Q, n_frames, b->o.hr, b->d_init, &b->graph, &b->exec);
@@ -1739,13 +1775,17 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
         batch_free(b);
         return fail(TBR_ERR_CUDA, "graph capture failed");
     }
+    {
+        std::lock_guard<std::mutex> lk(g_batches_mu);
+        g_batches[b] = ctx;
+    }
     *out = b;
     return TBR_OK;
 }
 
 tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *entries, int32_t max,
                               int32_t *n_out, tbr_tune_entry *best) {
-    if (!b || repeats < 1 || max < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    if (!live_batch(b) || repeats < 1 || max < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1753,18 +1793,20 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
     struct Shape {
         int hr, pp;
     };
-    // The compiled FP32 scoring variants x point-chunk sizes, then the
-    // tensor-core shape (32 hypotheses per block) with planned and long chunks.
+    // Hypotheses per block x point tile per work item: 32 (the tensor-core
+    // kernel) and 64 / 128 / 192 / 256 (the compiled FP32 variants, 2 / 4 / 6 / 8
+    // per lane, with 2 or 4 points per inner step) x tiles of 128, 256 and 512
+    // points, plus tiles sized from the step's work (0) and longer ones.
     const Shape shapes[6] = {{2, 4}, {4, 2}, {4, 4}, {6, 2}, {6, 4}, {8, 2}};
-    const int chunks[5] = {0, 256, 512, 1024, 2048};
+    const int chunks[6] = {0, 128, 256, 512, 1024, 2048};
+    const int tc_chunks[5] = {0, 128, 256, 512, 8192};
     struct Cand {
         int hr, pp, chunk;
     };
     std::vector<Cand> cands;
     for (const Shape &sh : shapes)
         for (int chunk : chunks) cands.push_back({sh.hr, sh.pp, chunk});
-    cands.push_back({1, kTcPP, 0});
-    cands.push_back({1, kTcPP, 8192});
+    for (int chunk : tc_chunks) cands.push_back({1, kTcPP, chunk});
     std::vector<tbr_tune_entry> tried;
     cudaEvent_t t0, t1;
     TBR_CUDA(cudaEventCreate(&t0));
@@ -1835,7 +1877,7 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
 }
 
 tbr_status tbr_batch_run(tbr_batch *b) {
-    if (!b) return fail(TBR_ERR_INVALID_ARG, "NULL batch");
+    if (!live_batch(b)) return fail(TBR_ERR_INVALID_ARG, "NULL or destroyed batch");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1847,7 +1889,7 @@ tbr_status tbr_batch_run(tbr_batch *b) {
 }
 
 tbr_status tbr_batch_sync(tbr_batch *b) {
-    if (!b) return fail(TBR_ERR_INVALID_ARG, "NULL batch");
+    if (!live_batch(b)) return fail(TBR_ERR_INVALID_ARG, "NULL or destroyed batch");
     Engine &E = b->ctx->E;
     TBR_CUDA(cudaStreamSynchronize(E.stream));
     TBR_CUDA(cudaMemcpy(E.h_counters, b->Q.counters, 8 * kCNum, cudaMemcpyDeviceToHost));
@@ -1857,7 +1899,7 @@ tbr_status tbr_batch_sync(tbr_batch *b) {
 }
 
 tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results) {
-    if (!b || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    if (!live_batch(b) || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaStreamSynchronize(E.stream));
@@ -1877,7 +1919,7 @@ tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results) {
 
 tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max, int32_t *n_out,
                              uint64_t *pairs_scored) {
-    if (!b || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    if (!live_batch(b) || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1920,7 +1962,11 @@ tbr_status tbr_measure_fp32_peak(tbr_context *ctx, double *tflops) {
 }
 
 void tbr_batch_destroy(tbr_batch *b) {
-    if (!b) return;
+    {
+        // (the handle is erased first: a concurrent tbr_context_destroy then skips it)
+        std::lock_guard<std::mutex> lk(g_batches_mu);
+        if (!b || !g_batches.erase(b)) return;  // NULL, or already freed with its context
+    }
     std::lock_guard<std::mutex> lk(b->ctx->E.mu);
     batch_free(b);
 }
@@ -1993,6 +2039,7 @@ struct tbr_server {
     bool stop = false;
     std::thread worker;
     int32_t *d_status = nullptr, *h_status = nullptr;
+    FrameResult *h_res = nullptr;  // every resident frame's result after the step in flight (pinned)
     int32_t *d_prep = nullptr;
     PinnedBuffer stage[2];   // admission staging, alternating between steps
     int cur = 0;
@@ -2100,12 +2147,9 @@ static tbr_status server_step(tbr_server *s) {
         for (int i = 0; i < na; ++i)
             if (s->h_status[i] == kDone) fin.push_back(i);
         if (!fin.empty()) {
-            std::vector<FrameResult> res(fin.size());
-            std::vector<int> fslots(fin.size());
-            for (size_t k = 0; k < fin.size(); ++k) fslots[k] = s->resident[fin[k]].slot;
-            tbr_status fst = fetch_results(E, fslots, res.data());
-            if (fst) return fst;
-            for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &res[k], TBR_OK);
+            // The step gathered every resident frame's result (s->h_res, in
+            // resident order): no second round trip.
+            for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &s->h_res[fin[k]], TBR_OK);
             std::vector<Resident> keep;
             std::vector<bool> gone(na, false);
             for (int i : fin) gone[i] = true;
@@ -2174,12 +2218,20 @@ static tbr_status server_step(tbr_server *s) {
             TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_join, 0));
             k_tick<<<1, 1, 0, E.stream>>>(E.P);
         } else {
-            // Few: RANSAC, then the refinement of what finished, in this step.
-            E.launch_step(E.P, na, s->o.hr);
+            // Few: RANSAC, then the refinement of what finished, in this step
+            // (each frame's LM on a CTA or a cluster, for latency).
+            Pools Ql = E.P;
+            Ql.lm_warp_max = 0;
+            Ql.lm_cluster_min = kLMClusterMinTail;
+            E.launch_step(Ql, na, s->o.hr);
         }
         k_gather_status<<<(na + 255) / 256, 256, 0, E.stream>>>(E.P, s->d_status);
+        k_gather_results<<<(int)std::min<size_t>(1024, (na * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0,
+                           E.stream>>>(E.P.results, E.d_active, na, E.d_res_stage);
         TBR_CUDA(cudaGetLastError());
         TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaMemcpyAsync(s->h_res, E.d_res_stage, sizeof(FrameResult) * na, cudaMemcpyDeviceToHost,
+                                 E.stream));
         TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
         s->step_in_flight = true;
         s->ws.steps++;
@@ -2268,7 +2320,8 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
     if (cfg->max_queue > 0) s->max_queue = cfg->max_queue;
     if (cudaMalloc(&s->d_status, 4 * kMaxActive) != cudaSuccess ||
         cudaMalloc(&s->d_prep, 4 * kMaxActive) != cudaSuccess ||
-        cudaMallocHost(&s->h_status, 4 * kMaxActive) != cudaSuccess) {
+        cudaMallocHost(&s->h_status, 4 * kMaxActive) != cudaSuccess ||
+        cudaMallocHost(&s->h_res, sizeof(FrameResult) * kMaxActive) != cudaSuccess) {
         delete s;
         return fail(TBR_ERR_OOM, "server allocation failed");
     }
@@ -2382,6 +2435,7 @@ void tbr_server_destroy(tbr_server *s) {
     if (s->d_status) cudaFree(s->d_status);
     if (s->d_prep) cudaFree(s->d_prep);
     if (s->h_status) cudaFreeHost(s->h_status);
+    if (s->h_res) cudaFreeHost(s->h_res);
     delete s;
 }
 
