@@ -39,7 +39,9 @@ def test_forced_step_beyond_cap_is_split_and_matches_oracle(ctx, oracle):
     assert d["hypotheses"] == info.ransac.hypotheses > 4096  # more ties than one step may re-rank
     assert d["samples"] == 4096 == info.ransac.samples
     assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
-    assert abs(d["model_score"] - info.ransac.score) <= 1e-12 * max(info.ransac.score, 1e-300)
+    # every solution fits the three points exactly: the scores are FP64 rounding
+    # noise (~1e-32), where only an absolute bound means anything
+    assert abs(d["model_score"] - info.ransac.score) <= 1e-12 * info.ransac.score + 1e-28
     assert d["candidate_overflow"] == 0
     assert d["steps"] > 1  # the over-full step was redone in smaller ones
     np.testing.assert_array_equal(inl, o["inliers"])
