@@ -2038,12 +2038,21 @@ struct tbr_server {
     uint64_t in_flight = 0;  // submitted and not yet completed
     bool stop = false;
     std::thread worker;
-    int32_t *d_status = nullptr, *h_status = nullptr;
-    FrameResult *h_res = nullptr;  // every resident frame's result after the step in flight (pinned)
-    int32_t *d_prep = nullptr;
-    PinnedBuffer stage[2];   // admission staging, alternating between steps
-    int cur = 0;
-    bool step_in_flight = false;
+    int32_t *d_status = nullptr, *d_prep = nullptr;
+    // Host side of the steps in flight (at most two), per buffer b: the
+    // resident frames' statuses and results at the end of the step (pinned),
+    // its counters, its active list, and an event after its downloads.
+    int32_t *h_status[2] = {}, *h_active[2] = {};
+    FrameResult *h_res[2] = {};
+    unsigned long long *h_cnt[2] = {};
+    cudaEvent_t ev_done[2] = {};
+    struct InFlight {
+        int buf;                     // host buffers b
+        int stage;                   // admission staging buffer it uploads from (-1: none)
+        std::vector<uint64_t> ids;   // request ids in active-list order
+    };
+    std::deque<InFlight> inflight;
+    PinnedBuffer stage[2];   // admission staging; a step in flight holds the one it uploads from
     tbr_server_stats stats{};  // guarded by mu
     tbr_server_stats ws{};     // the worker's own counters, published into stats after each step
     tbr_status error = TBR_OK;
@@ -2072,19 +2081,70 @@ static void server_complete(tbr_server *s, Resident &r, const FrameResult *res, 
     s->cv_done.notify_all();
 }
 
-// Resident frames from which a serving step overlaps refinement with RANSAC.
+// Resident frames from which a serving step overlaps refinement with RANSAC,
+// and from which the loop keeps a second step queued on the device.
 constexpr int kServerOverlapFrames = 16;
 
-// One iteration of the request loop, pipelined with the device:
-//   A. while the previous step runs, take queued requests that fit the free
-//      slots and point blocks and copy them into pinned staging;
-//   B. wait for that step, retire the frames it finished;
-//   C. upload the staged frames, prepare them, and launch the next step over
+// Retires the oldest step in flight: waits for it, then completes the frames it
+// finished that are still resident (a frame that finished earlier may show up
+// again in a later step's snapshot, which was taken before its retirement).
+static tbr_status server_retire_oldest(tbr_server *s) {
+    Engine &E = s->E;
+    tbr_server::InFlight st = std::move(s->inflight.front());
+    s->inflight.pop_front();
+    auto t0 = std::chrono::steady_clock::now();
+    TBR_CUDA(cudaEventSynchronize(s->ev_done[st.buf]));
+    s->ws.device_wait_ms += ms_since(t0);
+    if (s->h_cnt[st.buf][kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    t0 = std::chrono::steady_clock::now();
+    std::unordered_map<uint64_t, size_t> pos;
+    for (size_t i = 0; i < s->resident.size(); ++i) pos[s->resident[i].req->id] = i;
+    std::vector<bool> gone(s->resident.size(), false);
+    bool any = false;
+    for (size_t i = 0; i < st.ids.size(); ++i) {
+        if (s->h_status[st.buf][i] != kDone) continue;
+        auto it = pos.find(st.ids[i]);
+        if (it == pos.end() || gone[it->second]) continue;  // retired or cancelled already
+        Resident &r = s->resident[it->second];
+        server_complete(s, r, &s->h_res[st.buf][i], TBR_OK);
+        E.blocks.release(r.blk_off, r.n_blocks);
+        E.free_slots.push_back(r.slot);
+        gone[it->second] = true;
+        any = true;
+    }
+    if (any) {
+        std::vector<Resident> keep;
+        for (size_t i = 0; i < s->resident.size(); ++i)
+            if (!gone[i]) keep.push_back(std::move(s->resident[i]));
+        s->resident.swap(keep);
+    }
+    s->ws.host_retire_ms += ms_since(t0);
+    return TBR_OK;
+}
+
+// One iteration of the request loop, pipelined with the device. With many
+// resident frames two steps are kept in flight, so the device always has a
+// queued step while the host retires, stages and launches:
+//   1. if two steps are in flight, retire the older one;
+//   2. take queued requests that fit the free slots and point blocks and copy
+//      them into a staging buffer no step in flight uploads from;
+//   3. with few resident frames (latency first) retire the step in flight too;
+//   4. upload the staged frames, prepare them, and launch the next step over
 //      every resident frame without waiting for it.
+// Device writes of a new step (records, points) are ordered after the steps in
+// flight on the one stream, so a slot or block freed by a retirement can be
+// reused at once.
 static tbr_status server_step(tbr_server *s) {
     Engine &E = s->E;
-    // ---- A: stage admissions ----
+    while (s->inflight.size() >= 2) {
+        tbr_status st = server_retire_oldest(s);
+        if (st) return st;
+    }
+    // ---- stage admissions ----
     auto t0 = std::chrono::steady_clock::now();
+    int sb = 0;
+    for (auto &f : s->inflight)
+        if (f.stage == sb) sb = 1;
     std::vector<std::unique_ptr<ServerRequest>> newreq;
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -2092,7 +2152,7 @@ static tbr_status server_step(tbr_server *s) {
         // One step admits at most a staging buffer's worth (always at least one
         // request), so that staging keeps overlapping the device's steps.
         size_t staged = 0;
-        const size_t stage_cap = s->stage[s->cur].bytes;
+        const size_t stage_cap = s->stage[sb].bytes;
         while (!s->queue.empty() && (int)newreq.size() < (int)E.free_slots.size()) {
             auto &q = s->queue.front();
             if (q->cancelled) {
@@ -2121,7 +2181,7 @@ static tbr_status server_step(tbr_server *s) {
         std::vector<FrameHost> fh;
         for (auto &r : newreq)
             fh.push_back({r->U(), r->Xw(), r->n, {r->K[0], r->K[1], r->K[2], r->K[3]}, r->seed, r->thr, nullptr, 0});
-        PinnedBuffer &buf = s->stage[s->cur];
+        PinnedBuffer &buf = s->stage[sb];
         tbr_status st = buf.ensure(stage_bytes(fh));
         if (st) return st;
         st = stage_frames(E, fh, s->o, (char *)buf.p, A);
@@ -2134,38 +2194,13 @@ static tbr_status server_step(tbr_server *s) {
         }
     }
     s->ws.host_stage_ms += ms_since(t0);
-    // ---- B: finish the step in flight ----
-    if (s->step_in_flight) {
-        t0 = std::chrono::steady_clock::now();
-        TBR_CUDA(cudaStreamSynchronize(E.stream));
-        s->step_in_flight = false;
-        s->ws.device_wait_ms += ms_since(t0);
-        if (E.h_counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
-        t0 = std::chrono::steady_clock::now();
-        const int na = (int)s->resident.size();
-        std::vector<int> fin;
-        for (int i = 0; i < na; ++i)
-            if (s->h_status[i] == kDone) fin.push_back(i);
-        if (!fin.empty()) {
-            // The step gathered every resident frame's result (s->h_res, in
-            // resident order): no second round trip.
-            for (size_t k = 0; k < fin.size(); ++k) server_complete(s, s->resident[fin[k]], &s->h_res[fin[k]], TBR_OK);
-            std::vector<Resident> keep;
-            std::vector<bool> gone(na, false);
-            for (int i : fin) gone[i] = true;
-            for (int i = 0; i < na; ++i) {
-                if (gone[i]) {
-                    E.blocks.release(s->resident[i].blk_off, s->resident[i].n_blocks);
-                    E.free_slots.push_back(s->resident[i].slot);
-                } else {
-                    keep.push_back(std::move(s->resident[i]));
-                }
-            }
-            s->resident.swap(keep);
-        }
-        s->ws.host_retire_ms += ms_since(t0);
+    // ---- few (or no) resident frames: finish the step in flight first ----
+    const size_t will_resident = s->resident.size() + A.slots.size();
+    if (!s->inflight.empty() && will_resident < (size_t)kServerOverlapFrames) {
+        tbr_status st = server_retire_oldest(s);
+        if (st) return st;
     }
-    // ---- cancels of resident frames (no step in flight here) ----
+    // ---- cancels of resident frames ----
     {
         std::vector<uint64_t> ids;
         {
@@ -2182,7 +2217,7 @@ static tbr_status server_step(tbr_server *s) {
                     break;
                 }
     }
-    // ---- C: upload admissions, launch the next step ----
+    // ---- upload admissions, launch the next step ----
     t0 = std::chrono::steady_clock::now();
     if (!A.slots.empty()) {
         tbr_status st = upload_staged(E, A);
@@ -2196,14 +2231,21 @@ static tbr_status server_step(tbr_server *s) {
         for (size_t i = 0; i < A.slots.size(); ++i)
             s->resident.push_back({std::move(newreq[i]), A.slots[i], A.devs[i].blk_off, A.devs[i].n_blocks});
         s->ws.admitted += (int64_t)A.slots.size();
-        s->cur ^= 1;
     }
     if (!s->resident.empty()) {
         const int na = (int)s->resident.size();
-        tbr_status st = E.ensure_stage(8 * na + 4096);
-        if (st) return st;
-        int32_t *ha = (int32_t *)E.h_stage;
-        for (int i = 0; i < na; ++i) ha[i] = s->resident[i].slot;
+        int b = 0;
+        for (auto &f : s->inflight)
+            if (f.buf == b) b = 1;
+        int32_t *ha = s->h_active[b];
+        tbr_server::InFlight fl;
+        fl.buf = b;
+        fl.stage = A.slots.empty() ? -1 : sb;
+        fl.ids.resize(na);
+        for (int i = 0; i < na; ++i) {
+            ha[i] = s->resident[i].slot;
+            fl.ids[i] = s->resident[i].req->id;
+        }
         TBR_CUDA(cudaMemcpyAsync(E.d_active, ha, 4 * na, cudaMemcpyHostToDevice, E.stream));
         E.P.n_active = na;
         if (na >= kServerOverlapFrames) {
@@ -2229,11 +2271,12 @@ static tbr_status server_step(tbr_server *s) {
         k_gather_results<<<(int)std::min<size_t>(1024, (na * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0,
                            E.stream>>>(E.P.results, E.d_active, na, E.d_res_stage);
         TBR_CUDA(cudaGetLastError());
-        TBR_CUDA(cudaMemcpyAsync(s->h_status, s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
-        TBR_CUDA(cudaMemcpyAsync(s->h_res, E.d_res_stage, sizeof(FrameResult) * na, cudaMemcpyDeviceToHost,
+        TBR_CUDA(cudaMemcpyAsync(s->h_status[b], s->d_status, 4 * na, cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaMemcpyAsync(s->h_res[b], E.d_res_stage, sizeof(FrameResult) * na, cudaMemcpyDeviceToHost,
                                  E.stream));
-        TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
-        s->step_in_flight = true;
+        TBR_CUDA(cudaMemcpyAsync(s->h_cnt[b], E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+        TBR_CUDA(cudaEventRecord(s->ev_done[b], E.stream));
+        s->inflight.push_back(std::move(fl));
         s->ws.steps++;
         s->ws.resident_sum += na;
     }
@@ -2255,10 +2298,11 @@ static void server_loop(tbr_server *s) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv.wait_for(lk, std::chrono::milliseconds(50), [&] {
-                return s->stop || !s->queue.empty() || !s->resident.empty() || !s->cancel_ids.empty();
+                return s->stop || !s->queue.empty() || !s->resident.empty() || !s->inflight.empty() ||
+                       !s->cancel_ids.empty();
             });
             if (s->stop) break;
-            if (s->queue.empty() && s->resident.empty() && !s->step_in_flight) {
+            if (s->queue.empty() && s->resident.empty() && s->inflight.empty()) {
                 s->cancel_ids.clear();  // nothing resident to cancel
                 continue;
             }
@@ -2266,7 +2310,7 @@ static void server_loop(tbr_server *s) {
         tbr_status st = server_step(s);
         if (st) {
             cudaStreamSynchronize(s->E.stream);
-            s->step_in_flight = false;
+            s->inflight.clear();
             std::lock_guard<std::mutex> lk(s->mu);
             s->error = st;
             s->error_msg = g_last_error;
@@ -2295,6 +2339,19 @@ static void server_loop(tbr_server *s) {
     cudaStreamSynchronize(s->E.stream);
 }
 
+static void server_free(tbr_server *s) {
+    if (s->d_status) cudaFree(s->d_status);
+    if (s->d_prep) cudaFree(s->d_prep);
+    for (int b = 0; b < 2; ++b) {
+        if (s->h_status[b]) cudaFreeHost(s->h_status[b]);
+        if (s->h_active[b]) cudaFreeHost(s->h_active[b]);
+        if (s->h_res[b]) cudaFreeHost(s->h_res[b]);
+        if (s->h_cnt[b]) cudaFreeHost(s->h_cnt[b]);
+        if (s->ev_done[b]) cudaEventDestroy(s->ev_done[b]);
+    }
+    delete s;
+}
+
 extern "C" {
 
 tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr_server **out) {
@@ -2318,21 +2375,26 @@ tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr
     s->o.max_rounds_step = 64;
     s->E.pp = s->o.pp;
     if (cfg->max_queue > 0) s->max_queue = cfg->max_queue;
-    if (cudaMalloc(&s->d_status, 4 * kMaxActive) != cudaSuccess ||
-        cudaMalloc(&s->d_prep, 4 * kMaxActive) != cudaSuccess ||
-        cudaMallocHost(&s->h_status, 4 * kMaxActive) != cudaSuccess ||
-        cudaMallocHost(&s->h_res, sizeof(FrameResult) * kMaxActive) != cudaSuccess) {
-        delete s;
+    bool ok = cudaMalloc(&s->d_status, 4 * kMaxActive) == cudaSuccess &&
+              cudaMalloc(&s->d_prep, 4 * kMaxActive) == cudaSuccess;
+    for (int b = 0; b < 2 && ok; ++b)
+        ok = cudaMallocHost(&s->h_status[b], 4 * kMaxActive) == cudaSuccess &&
+             cudaMallocHost(&s->h_active[b], 4 * kMaxActive) == cudaSuccess &&
+             cudaMallocHost(&s->h_res[b], sizeof(FrameResult) * kMaxActive) == cudaSuccess &&
+             cudaMallocHost(&s->h_cnt[b], 8 * kCNum) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s->ev_done[b], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        server_free(s);
         return fail(TBR_ERR_OOM, "server allocation failed");
     }
     // Staging for one step's admissions, sized up front (128 MiB each).
     for (auto &b : s->stage)
         if (b.ensure(128ull << 20) != TBR_OK) {
-            delete s;
+            server_free(s);
             return fail(TBR_ERR_OOM, "server staging allocation failed");
         }
     if (s->E.ensure_stage(1 << 20) != TBR_OK) {
-        delete s;
+        server_free(s);
         return fail(TBR_ERR_OOM, "server staging allocation failed");
     }
     cudaMemsetAsync(s->E.P.counters, 0, 8 * kCNum, s->E.stream);
@@ -2432,11 +2494,7 @@ void tbr_server_destroy(tbr_server *s) {
     }
     if (s->worker.joinable()) s->worker.join();
     cudaStreamSynchronize(s->E.stream);
-    if (s->d_status) cudaFree(s->d_status);
-    if (s->d_prep) cudaFree(s->d_prep);
-    if (s->h_status) cudaFreeHost(s->h_status);
-    if (s->h_res) cudaFreeHost(s->h_res);
-    delete s;
+    server_free(s);
 }
 
 tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, const double *points3D,
