@@ -8,7 +8,7 @@ more candidates than fit:
   * a step of many forced samples whose hypotheses all tie (n = 3: every sample
     is a permutation of the one triple, every P3P solution fits all points) is
     redone in smaller steps and gives the FP64 oracle's selection, unflagged;
-  * a single round of 2048 such samples cannot be split: the kept subset is
+  * a single round of 4096 such samples cannot be split: the kept subset is
     the same on every run and alone or in a batch, and the flag is raised.
 """
 import dataclasses
@@ -50,7 +50,7 @@ def test_forced_step_beyond_cap_is_split_and_matches_oracle(ctx, oracle):
 
 def test_single_round_beyond_cap_is_flagged_and_deterministic(ctx):
     f = tied_frame()
-    ro = RansacOptions_cuda(max_iterations=2048, max_reproj_error=4.0)
+    ro = RansacOptions_cuda(max_iterations=4096, max_reproj_error=4.0)
     runs = [ctx.estimate_absolute_pose(f.uv, f.xyz, CAM, ro, BundleOptions_cuda(), seed=9) for _ in range(2)]
     (st0, p0, m0), (st1, p1, m1) = runs
     d0, d1 = st0.details, st1.details

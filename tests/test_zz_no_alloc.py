@@ -62,8 +62,13 @@ def test_noalloc_scores_match_existing_entry_point_and_oracle_twice(oracle):
     focal = 0.5 * (f.K[0] + f.K[1])
     allowed = np.array([near_threshold(poses[k], xn, f.xyz, focal).sum() for k in range(H)])
     o_s, o_c = _oracle_scores(oracle, xn, f.xyz, poses, sq)
-    # A first call loads the library's device code; after it no call may change free device memory.
+    # A first round loads the device code it uses (this library's and torch's
+    # fill and copy kernels); after it no call may change free device memory.
+    scores.fill_(-1.0)
+    counts.fill_(-1)
     assert _call(L, x_d, X_d, f.n, P_d, H, sq, scores, counts, stream) == 0, L.tbr_last_error()
+    torch.cuda.synchronize(dev)
+    scores.cpu(), counts.cpu()
     torch.cuda.synchronize(dev)
     free0 = torch.cuda.mem_get_info(dev)[0]
     for call in range(2):

@@ -299,7 +299,6 @@ class Engine {
         P.active = d_active;
         P.num_sms = num_sms;
         P.lm_cluster_min = kLMClusterMin;
-        P.lm_warp_max = kLMWarpMax;
         TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
         TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
         TBR_CUDA(cudaMallocHost(&h_results, sizeof(FrameResult) * kMaxActive));
@@ -446,7 +445,6 @@ class Engine {
         auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
         beg(8); k_inliers<<<n_active, 1024, 0, st>>>(Q); end(8);
         beg(9);
-        if (Q.lm_warp_max > 0) k_lm_warp<<<(n_active + kLMWarpFrames - 1) / kLMWarpFrames, kLMWarpFrames * 32, 0, st>>>(Q);
         k_lm_small<<<n_active, kLMSmallThreads, 0, st>>>(Q);
         k_lm<<<n_active * kLMCluster, kLMThreads, 0, st>>>(Q);
         end(9);
@@ -555,7 +553,6 @@ class Engine {
             if (ok) {
                 Pools Qt = Q;  // nothing runs beside the last step's refinement
                 Qt.lm_cluster_min = kLMClusterMinTail;
-                Qt.lm_warp_max = 0;
                 launch_refine(Qt, n, stream);
                 ok = cudaStreamEndCapture(stream, &tail) == cudaSuccess;
             }
@@ -2263,7 +2260,6 @@ static tbr_status server_step(tbr_server *s) {
             // Few: RANSAC, then the refinement of what finished, in this step
             // (each frame's LM on a CTA or a cluster, for latency).
             Pools Ql = E.P;
-            Ql.lm_warp_max = 0;
             Ql.lm_cluster_min = kLMClusterMinTail;
             E.launch_step(Ql, na, s->o.hr);
         }

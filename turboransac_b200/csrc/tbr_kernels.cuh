@@ -148,7 +148,6 @@ struct Pools {
     int32_t n_active;
     int32_t num_sms;
     int64_t lm_cluster_min;  // inliers from which a frame's LM runs on a CTA cluster
-    int64_t lm_warp_max;     // inliers below which a frame's LM runs on one warp (0: never)
     // per point (blocks * kSub entries)
     const double *uv64;  // raw pixels (2/pt)
     const double *X64;   // world points (3/pt)
@@ -1967,14 +1966,13 @@ __device__ __forceinline__ void kahan_add(float &s, float &c, float x) {
 
 // Block-wide FP64 sum of NV values per thread; every thread gets the result in
 // out[] (shared). Uses 32*NV doubles of scratch.
-// Warp reduce-scatter by recursive halving: at width h a lane trades the half
-// of its 2h partial sums that its partner (lane ^ h) keeps, so after
-// 16 + 8 + 4 + 2 + 1 exchanges lane k holds the warp's sum of value k
-// (returned; lanes from NV on return 0).
 template <int NV>
-__device__ __forceinline__ double warp_reduce_scatter_d(const double (&v)[NV]) {
+__device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, double *out) {
     static_assert(NV <= 32, "one value per lane after the warp reduction");
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // Warp reduce-scatter by recursive halving: at width h a lane trades the
+    // half of its 2h partial sums that its partner (lane ^ h) keeps, so after
+    // 16 + 8 + 4 + 2 + 1 exchanges lane k holds the warp's sum of value k.
     double a[32];
 #pragma unroll
     for (int k = 0; k < 32; ++k) a[k] = k < NV ? v[k] : 0.0;
@@ -1988,14 +1986,7 @@ __device__ __forceinline__ double warp_reduce_scatter_d(const double (&v)[NV]) {
             a[k] = keep + __shfl_xor_sync(0xffffffffu, give, h);
         }
     }
-    return a[0];
-}
-
-template <int NV>
-__device__ __forceinline__ void block_sum_d(double (&v)[NV], double *scratch, double *out) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const double a0 = warp_reduce_scatter_d<NV>(v);
-    if (lane < NV) scratch[w * NV + lane] = a0;
+    if (lane < NV) scratch[w * NV + lane] = a[0];
     __syncthreads();
     if (threadIdx.x < NV) {
         double s = 0.0;
@@ -2015,13 +2006,7 @@ enum LMLoss : int32_t { kLossCauchy = 0, kLossTruncated = 1, kLossHuber = 2, kLo
 // triangle (jaco.cuh:173-200) and J^T W r (:202-209) accumulated in FP32 with
 // Kahan compensation. The Jacobian uses the world coordinates of the
 // reference's parameterisation (rotation post-multiplied, translation t + R dt).
-// out[0] = cost, out[1..27] = accumulators.
-// VW = 0: the CTA's threads share the points (thread k takes i0 + k, stride
-// blockDim.x), block totals. VW > 0: one warp does the same work as a CTA of
-// VW warps -- virtual warp w's lanes take i0 + 32 w + lane, stride 32 VW, and
-// the virtual warps' totals are added in order -- so its result is the CTA's
-// bit for bit.
-template <int VW = 0>
+// out[0] = cost, out[1..27] = accumulators (block totals).
 __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, const double *q, const double *t,
                         const double *cam, double inv_sq_thr, int loss, double thr, bool weighted,
                         double *scratch, double *out) {
@@ -2031,14 +2016,12 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
                 r12 = (float)R[5], r20 = (float)R[6], r21 = (float)R[7], r22 = (float)R[8];
     const float fx = (float)cam[0], fy = (float)cam[1];
     const float isq = (float)inv_sq_thr;
-    // One thread's share: inliers first, first + stride, ...
-    auto thread_sums = [&](int64_t first, int64_t stride, double (&dv)[kLMSums]) {
-        double cost = 0.0;
-        float Sv[27], Cc[27];
+    double cost = 0.0;
+    float Sv[27], Cc[27];
 #pragma unroll
-        for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
+    for (int k = 0; k < 27; ++k) Sv[k] = Cc[k] = 0.0f;
 #pragma unroll 2  // two points per thread in flight: the FP64 division and log1p chains overlap
-        for (int64_t i = i0 + first; i < i1; i += stride) {
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int64_t o = base + i;
         const double X0d = P.lX64[3 * o], X1d = P.lX64[3 * o + 1], X2d = P.lX64[3 * o + 2];
         const double Z0 = R[0] * X0d + R[1] * X1d + R[2] * X2d + t[0];
@@ -2116,26 +2099,12 @@ __device__ void lm_pass(const Pools &P, int64_t base, int64_t i0, int64_t i1, co
             dZ02 * wx + dZ12 * wy};
 #pragma unroll
         for (int k = 0; k < 27; ++k) kahan_add(Sv[k], Cc[k], v[k]);
-        }
-        dv[0] = cost;
-#pragma unroll
-        for (int k = 0; k < 27; ++k) dv[1 + k] = (double)Sv[k] - (double)Cc[k];
-    };
-    if constexpr (VW == 0) {
-        double dv[kLMSums];
-        thread_sums(threadIdx.x, blockDim.x, dv);
-        block_sum_d<kLMSums>(dv, scratch, out);
-    } else {
-        const int lane = threadIdx.x & 31;
-        double tot = 0.0;  // lane k: value k, summed over the virtual warps in order
-        for (int w = 0; w < VW; ++w) {
-            double dv[kLMSums];
-            thread_sums(32 * w + lane, 32 * VW, dv);
-            tot += warp_reduce_scatter_d<kLMSums>(dv);
-        }
-        if (lane < kLMSums) out[lane] = tot;
-        __syncwarp();
     }
+    double dv[kLMSums];
+    dv[0] = cost;
+#pragma unroll
+    for (int k = 0; k < 27; ++k) dv[1 + k] = (double)Sv[k] - (double)Cc[k];
+    block_sum_d<kLMSums>(dv, scratch, out);
 }
 
 // 6x6 Cholesky solve of the damped normal equations (lm_utils.cuh:14-100),
@@ -2167,106 +2136,13 @@ __device__ __forceinline__ void cholesky_solve6(const double *A, const double *b
     }
 }
 
-// Levenberg-Marquardt state of one frame and its serial steps (one thread),
-// with the control flow of lm.cuh:15-171: damping, the accept rule, the lambda
-// schedule, the removal of damping after a rejected step, and both stop tests.
-struct LMState {
-    double J[36], g[6], Jc[28], q[4], t[3], qn[4], tn[3];
-    double cost, lambda;
-    int brk, recompute, iters, invalid;
-};
-
-// After the pass at the starting pose (totals T).
-__device__ __forceinline__ void lm_start(LMState &S, const FrameDev &f, const double *q0, const double *t0,
-                                         const double *T) {
-    for (int k = 0; k < 4; ++k) S.q[k] = q0[k];
-    for (int k = 0; k < 3; ++k) S.t[k] = t0[k];
-    S.cost = T[0];
-    for (int k = 0; k < 27; ++k) S.Jc[k] = T[1 + k];
-    S.Jc[27] = 0.0;
-    S.lambda = f.lm_lambda0;
-    S.recompute = 1;
-    S.iters = 0;
-    S.invalid = 0;
-}
-
-// Damped normal equations -> candidate pose (qn, tn); brk set by the gradient
-// (lm.cuh:243-248) or step test.
-__device__ __forceinline__ void lm_propose(LMState &S, const FrameDev &f) {
-    S.brk = 0;
-    if (S.recompute) {
-        // J from the pass at the current pose (lower triangle in the
-        // reference's order).
-        const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
-                                {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
-                                {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
-        for (int k = 0; k < 36; ++k) S.J[k] = 0.0;
-        for (int k = 0; k < 21; ++k) S.J[idx[k][0] * 6 + idx[k][1]] = S.Jc[k];
-        double gn = 0.0;
-        for (int k = 0; k < 6; ++k) {
-            S.g[k] = S.Jc[21 + k];
-            gn += S.g[k] * S.g[k];
-        }
-        if (sqrt(gn) < f.lm_grad_tol) S.brk = 1;
-    }
-    for (int k = 0; k < 6; ++k) S.J[k * 7] += S.lambda;
-    double x[6];
-    cholesky_solve6(S.J, S.g, x);
-    double sn = 0.0;
-    for (int k = 0; k < 6; ++k) {
-        x[k] = -1 * x[k];
-        sn += x[k] * x[k];
-    }
-    if (sqrt(sn) < f.lm_step_tol) S.brk = 1;
-    quat_step_post(S.q, x, S.qn);  // jaco.cuh:288-299
-    double dt[3];
-    quat_rotate(S.q, x[3], x[4], x[5], dt);
-    for (int k = 0; k < 3; ++k) S.tn[k] = S.t[k] + dt[k];
-}
-
-// Accept or reject the candidate from the pass totals T at (qn, tn).
-__device__ __forceinline__ void lm_accept(LMState &S, const FrameDev &f, const double *T) {
-    if (T[0] < S.cost) {
-        for (int k = 0; k < 4; ++k) S.q[k] = S.qn[k];
-        for (int k = 0; k < 3; ++k) S.t[k] = S.tn[k];
-        S.lambda = fmax(f.lm_min_lambda, S.lambda / 10);
-        S.cost = T[0];
-        for (int k = 0; k < 27; ++k) S.Jc[k] = T[1 + k];
-        S.recompute = 1;
-    } else {
-        ++S.invalid;
-        for (int k = 0; k < 6; ++k) S.J[k * 7] -= S.lambda;
-        S.lambda = fmin(f.lm_max_lambda, S.lambda * 10);
-        S.recompute = 0;
-    }
-    ++S.iters;
-}
-
-__device__ __forceinline__ void lm_finish(const LMState &S, const FrameDev &f, FrameResult &res) {
-    for (int k = 0; k < 4; ++k) res.q[k] = S.q[k];
-    for (int k = 0; k < 3; ++k) res.t[k] = S.t[k];
-    res.lm_iters = S.iters;
-    res.lm_invalid = S.invalid;
-    res.lm_cost = S.cost;
-    res.samples = f.samples_done;
-    res.rounds = f.rounds_done;
-    res.hypotheses = f.hyps_done;
-    res.ransac_inliers = f.found ? f.best_count : 0;
-    res.num_inliers = f.num_inliers;
-    res.model_score = f.found ? f.best_score : DBL_MAX;
-    res.best_sample = f.found ? f.best_sample : -1;
-    res.best_sol = f.found ? f.best_sol : -1;
-    res.steps = f.steps;
-    res.rescored = f.rescored;
-    res.overflow = f.overflow;
-    res.status = kDone;
-}
-
-// One frame per cluster of CL CTAs, each owning a slice of the inliers.
-// Every candidate pose gets one fused pass (cost and, for the case it is
-// accepted, the normal equations at it), so an iteration costs one pass and
-// two cluster barriers. Sums cross the block and cluster in FP64 in a fixed
-// order; the solve, the step and the acceptance test are FP64.
+// Levenberg-Marquardt with the control flow of lm.cuh:15-171 -- damping, the
+// accept rule, the lambda schedule, the removal of damping after a rejected
+// step, and both stop tests -- one frame per cluster of CL CTAs, each owning a
+// slice of the inliers. Every candidate pose gets one fused pass (cost and, for
+// the case it is accepted, the normal equations at it), so an iteration costs
+// one pass and two cluster barriers. Sums cross the block and cluster in FP64 in
+// a fixed order; the solve, the step and the acceptance test are FP64.
 template <int CL>
 __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     namespace cg = cooperative_groups;
@@ -2274,7 +2150,9 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     __shared__ double scratch[32 * kLMSums];
     __shared__ double part[kLMSums];  // this CTA's pass totals
     __shared__ double tot[kLMSums];   // rank 0: cluster totals
-    __shared__ LMState S;
+    __shared__ double J[36], g[6], Jc[28], q[4], t[3], qn[4], tn[3];
+    __shared__ double cost, lambda;
+    __shared__ int brk, recompute, iters, invalid;
     __shared__ double pq[4], pt[3];  // the pose every CTA evaluates next
     __shared__ int pbrk;
     const int rank = (int)cluster.block_rank();
@@ -2310,25 +2188,63 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     const double *T = CL == 1 ? part : tot;
     if constexpr (CL > 1) cluster_totals();
     if (rank == 0 && threadIdx.x == 0) {
-        lm_start(S, f, pq, pt, T);
-        res.lm_cost0 = S.cost;
+        for (int k = 0; k < 4; ++k) q[k] = pq[k];
+        for (int k = 0; k < 3; ++k) t[k] = pt[k];
+        cost = T[0];
+        for (int k = 0; k < 27; ++k) Jc[k] = T[1 + k];
+        Jc[27] = 0.0;
+        lambda = f.lm_lambda0;
+        recompute = 1;
+        iters = 0;
+        invalid = 0;
+        res.lm_cost0 = cost;
     }
     for (int64_t it = 0; it < max_it; ++it) {
-        if (rank == 0 && threadIdx.x == 0) lm_propose(S, f);
+        if (rank == 0 && threadIdx.x == 0) {
+            brk = 0;
+            if (recompute) {
+                // J from the pass at the current pose (lower triangle in the
+                // reference's order); gradient test of lm.cuh:243-248.
+                const int idx[21][2] = {{0, 0}, {1, 0}, {2, 0}, {3, 0}, {4, 0}, {5, 0}, {1, 1},
+                                        {2, 1}, {3, 1}, {4, 1}, {5, 1}, {2, 2}, {3, 2}, {4, 2},
+                                        {5, 2}, {3, 3}, {4, 3}, {5, 3}, {4, 4}, {5, 4}, {5, 5}};
+                for (int k = 0; k < 36; ++k) J[k] = 0.0;
+                for (int k = 0; k < 21; ++k) J[idx[k][0] * 6 + idx[k][1]] = Jc[k];
+                double gn = 0.0;
+                for (int k = 0; k < 6; ++k) {
+                    g[k] = Jc[21 + k];
+                    gn += g[k] * g[k];
+                }
+                if (sqrt(gn) < f.lm_grad_tol) brk = 1;
+            }
+            for (int k = 0; k < 6; ++k) J[k * 7] += lambda;
+            double x[6];
+            cholesky_solve6(J, g, x);
+            double sn = 0.0;
+            for (int k = 0; k < 6; ++k) {
+                x[k] = -1 * x[k];
+                sn += x[k] * x[k];
+            }
+            if (sqrt(sn) < f.lm_step_tol) brk = 1;
+            quat_step_post(q, x, qn);  // jaco.cuh:288-299
+            double dt[3];
+            quat_rotate(q, x[3], x[4], x[5], dt);
+            for (int k = 0; k < 3; ++k) tn[k] = t[k] + dt[k];
+        }
         if constexpr (CL == 1) {
             // One CTA: the candidate pose and the stop flag are read in place;
             // the pass's own barriers order this thread's next writes to them.
             __syncthreads();
-            if (S.brk) break;
-            lm_pass(P, base, i0, i1, S.qn, S.tn, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0,
-                    scratch, part);
+            if (brk) break;
+            lm_pass(P, base, i0, i1, qn, tn, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch,
+                    part);
         } else {
             cluster.sync();
             if (threadIdx.x == 0) {
-                const LMState *r0 = cluster.map_shared_rank(&S, 0);
-                pbrk = r0->brk;
-                for (int k = 0; k < 4; ++k) pq[k] = r0->qn[k];
-                for (int k = 0; k < 3; ++k) pt[k] = r0->tn[k];
+                pbrk = cluster.map_shared_rank(&brk, 0)[0];
+                const double *rq = cluster.map_shared_rank(qn, 0), *rt = cluster.map_shared_rank(tn, 0);
+                for (int k = 0; k < 4; ++k) pq[k] = rq[k];
+                for (int k = 0; k < 3; ++k) pt[k] = rt[k];
             }
             __syncthreads();
             if (pbrk) break;
@@ -2337,90 +2253,58 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             __syncthreads();
             cluster_totals();
         }
-        if (rank == 0 && threadIdx.x == 0) lm_accept(S, f, T);
+        if (rank == 0 && threadIdx.x == 0) {
+            if (T[0] < cost) {
+                for (int k = 0; k < 4; ++k) q[k] = qn[k];
+                for (int k = 0; k < 3; ++k) t[k] = tn[k];
+                lambda = fmax(f.lm_min_lambda, lambda / 10);
+                cost = T[0];
+                for (int k = 0; k < 27; ++k) Jc[k] = T[1 + k];
+                recompute = 1;
+            } else {
+                ++invalid;
+                for (int k = 0; k < 6; ++k) J[k * 7] -= lambda;
+                lambda = fmin(f.lm_max_lambda, lambda * 10);
+                recompute = 0;
+            }
+            ++iters;
+        }
     }
-    if (rank == 0 && threadIdx.x == 0) lm_finish(S, f, res);
+    if (rank == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) res.q[k] = q[k];
+        for (int k = 0; k < 3; ++k) res.t[k] = t[k];
+        res.lm_iters = iters;
+        res.lm_invalid = invalid;
+        res.lm_cost = cost;
+        res.samples = f.samples_done;
+        res.rounds = f.rounds_done;
+        res.hypotheses = f.hyps_done;
+        res.ransac_inliers = f.found ? f.best_count : 0;
+        res.num_inliers = f.num_inliers;
+        res.model_score = f.found ? f.best_score : DBL_MAX;
+        res.best_sample = f.found ? f.best_sample : -1;
+        res.best_sol = f.found ? f.best_sol : -1;
+        res.steps = f.steps;
+        res.rescored = f.rescored;
+        res.overflow = f.overflow;
+        res.status = kDone;
+    }
     cluster.sync();  // no CTA leaves while rank 0 may still read its shared memory
     if (rank == 0 && threadIdx.x == 0) f.status = kDone;
 }
 
-// One frame per warp, with the arithmetic of the one-CTA path above
-// (kLMSmallThreads threads, emulated as kLMSmallThreads / 32 virtual warps):
-// the same inlier partition, Kahan sums, reduction order and serial steps, so
-// a frame's result does not depend on which of the two runs it. Small frames
-// run this way beside RANSAC so that their LM takes a few SMs, not one each.
-__device__ __forceinline__ void lm_frame_warp(const Pools &P, int slot, LMState &S, double *part, double *pose) {
-    constexpr int VW = kLMSmallThreads / 32;
-    const int lane = threadIdx.x & 31;
-    FrameDev &f = P.frames[slot];
-    FrameResult &res = P.results[slot];
-    const int64_t base = f.blk_off * kSub;
-    const int64_t n = f.num_inliers;
-    const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
-    const double inv_sq_thr = f.lm_inv_sq_thr;
-    const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
-    double *pq = pose, *pt = pose + 4;
-    if (lane == 0) {
-        for (int k = 0; k < 4; ++k) pq[k] = res.q[k];
-        for (int k = 0; k < 3; ++k) pt[k] = res.t[k];
-    }
-    __syncwarp();
-    if (max_it > 0)
-        lm_pass<VW>(P, base, 0, n, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, nullptr, part);
-    else if (lane < kLMSums) part[lane] = 0.0;
-    __syncwarp();
-    if (lane == 0) {
-        lm_start(S, f, pq, pt, part);
-        res.lm_cost0 = S.cost;
-    }
-    for (int64_t it = 0; it < max_it; ++it) {
-        if (lane == 0) lm_propose(S, f);
-        __syncwarp();
-        if (S.brk) break;
-        lm_pass<VW>(P, base, 0, n, S.qn, S.tn, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, nullptr,
-                    part);
-        if (lane == 0) lm_accept(S, f, part);
-        __syncwarp();
-    }
-    if (lane == 0) {
-        lm_finish(S, f, res);
-        f.status = kDone;
-    }
-}
-
-// Frames with fewer inliers than Pools::lm_cluster_min run their LM on one CTA
-// (below Pools::lm_warp_max: on one warp, with the same result), larger ones
-// on a cluster of kLMCluster CTAs. Beside RANSAC (frames finishing in earlier
-// steps) throughput wins: one warp up to kLMWarpMax, one CTA up to
-// kLMClusterMin. After the last step nothing else runs and the LM is the whole
-// remaining time: no warps, clusters from kLMClusterMinTail.
+// Frames with fewer inliers than Pools::lm_cluster_min run their LM on one CTA,
+// larger ones on a cluster of kLMCluster CTAs. Beside RANSAC (frames finishing
+// in earlier steps) throughput wins: one CTA up to kLMClusterMin. After the last
+// step nothing else runs and the LM is the whole remaining time: clusters from
+// kLMClusterMinTail.
 constexpr int64_t kLMClusterMin = 10000;
 constexpr int64_t kLMClusterMinTail = 3000;
-constexpr int64_t kLMWarpMax = 2048;
-constexpr int kLMWarpFrames = 8;  // frames (warps) per CTA of k_lm_warp
-
-__device__ __forceinline__ bool lm_on_warp(const Pools &P, const FrameDev &f) {
-    return f.num_inliers < P.lm_warp_max && !f.lm_force_cluster;
-}
-
-__global__ void __launch_bounds__(kLMWarpFrames * 32) k_lm_warp(Pools P) {
-    __shared__ LMState S[kLMWarpFrames];
-    __shared__ double part[kLMWarpFrames][kLMSums];
-    __shared__ double pose[kLMWarpFrames][8];
-    const int w = threadIdx.x >> 5;
-    const int a = blockIdx.x * kLMWarpFrames + w;
-    if (a >= P.n_active) return;
-    const int slot = P.active[a];
-    const FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending || !lm_on_warp(P, f)) return;  // uniform across the warp
-    lm_frame_warp(P, slot, S[w], part[w], pose[w]);
-}
 
 __global__ void __launch_bounds__(kLMSmallThreads, 1) k_lm_small(Pools P) {
     const int slot = P.active[blockIdx.x];
     const FrameDev &f = P.frames[slot];
-    if (f.status != kLMPending || f.num_inliers >= P.lm_cluster_min || f.lm_force_cluster || lm_on_warp(P, f))
-        return;
+    if (f.status != kLMPending || f.num_inliers >= P.lm_cluster_min || f.lm_force_cluster) return;
     lm_frame<1>(P, slot);
 }
 
