@@ -1175,72 +1175,32 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
     if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcCols));
 }
 
-// ------------------------------------- tensor-core scoring, pipelined --
-// The tensor-core filter with its stages overlapped. The A operand of every
-// staging block (the point's TF32 hi and lo parts, K = 8) and the points'
-// -x/tau, -y/tau are built once at admission (k_prep_pack), so a 128-point
-// tile lands in shared memory by two bulk copies into a ring of kTc2Stages
-// stages, with no thread work and no CTA barrier. The 32-hypothesis B operand
-// is kept as two halves of 16 hypotheses (N = 48: z2 | z0 | z1 rows), each
-// accumulating in its own 64-column TMEM slot, and every half is two MMAs
-// (hi and lo parts of the hypothesis, K = 8 each) on the same A tile:
+// ------------------------------- tensor-core scoring, staged operands --
+// The tensor-core filter with the A operand built once at admission: every
+// staging block carries the points' TF32 hi and lo parts (K = 8, k_prep_pack)
+// and their -x/tau, -y/tau, so a 128-point tile lands in shared memory by two
+// bulk copies into a 3-stage ring and the MMA reads it there: no thread
+// builds or fences the A tile, and a tile costs one CTA barrier (the
+// accumulator is free again). The two MMAs of a tile use the same A tile with
+// the hi and lo halves of the hypothesis rows:
 //   z = [Bh | Bh'] . [Ah | Al] + [Bl | Bl'] . [Ah | Al],
-// the four cross terms of the split products (exact in FP32). Thread 0
-// issues the MMA of the next tile's half h as soon as every warp has read
-// slot h into registers (the `empty` barrier), so the tensor core works on
-// tile i + 1 while the epilogue computes tile i. The epilogue takes one
-// reciprocal per two depths (Montgomery's batched inverse: 1/a = b / (ab),
-// 1/b = a / (ab)); depths are raised to 2^-63 (a point behind the camera
-// gets a residual of ~2^63 x its lateral offset and saturates) and, by the
-// bounds the staging puts on points and poses, stay below 2^63, so the
-// product is a normal FP32 number.
-constexpr int kTc2Stages = 4;
+// the four cross terms of the split products, exact in FP32. The epilogue
+// takes one reciprocal per two depths (Montgomery's batched inverse:
+// 1/a = b / (ab), 1/b = a / (ab)); depths are raised to 2^-63 (a point
+// behind the camera gets a residual of ~2^63 x its lateral offset and
+// saturates) and, by the bounds the staging puts on points and poses, stay
+// below 2^63, so the product is a normal FP32 number.
+constexpr int kTc2Stages = 3;
 constexpr int kTc2StageBytes = 2 * kTcABlockFloats * 4 + 2 * kSub * 8;  // A 4096 + N 1024
 constexpr int kTc2OffB = kTc2Stages * kTc2StageBytes;
 constexpr int kTc2OffRed = kTc2OffB + 3 * kTcHyp * 16 * 4;               // B: 96 rows x 16 K
 constexpr int kTc2OffCtl = kTc2OffRed + 4 * kTcHyp * 4;
-constexpr int kTc2HalfN = 3 * kTcHyp / 2;                                // 48
-constexpr uint32_t kTc2Idesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTc2HalfN >> 3) << 17) |
-                               ((uint32_t)(kTcPts >> 4) << 24);
 constexpr float kTc2DepthFloor = 0x1p-63f;
 static_assert(kTc2OffCtl + 128 <= kTcSmem, "tensor-core scoring shared memory");
 
 __device__ __forceinline__ uint64_t tc_desc_sbo(const void *smem, uint32_t sbo) {
     return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
            ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
-}
-__device__ __forceinline__ void tc2_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-    const uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kTc2Idesc), "r"(accumulate), "r"(m0), "r"(m1), "r"(m2), "r"(m3));
-}
-
-// B operand of hypothesis block hb in two halves: thread t < 96 writes
-// component t / 32 (z2, z0, z1) of hypothesis hb * 32 + t % 32 into row
-// 48 * half + 16 * component + (t % 16) (zero rows past the count).
-__device__ __forceinline__ void tc2_build_b(float *sB, const Pools &P, const FrameDev &f, int hb) {
-    const int t = threadIdx.x;
-    if (t >= 3 * kTcHyp) return;
-    const int j = t & 31, comp = t >> 5;
-    const int i = hb * kTcHyp + j;
-    const int cb = comp == 0 ? 8 : (comp == 1 ? 0 : 4);  // z2 | z0 | z1
-    const float *src = P.hP32 + 12 * (f.hyp_base + i) + cb;
-    float hi[4], lo[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float c = i < f.hyp_count ? __ldg(src + k) : 0.0f;
-        hi[k] = tf32_rn(c);
-        lo[k] = tf32_rn(c - hi[k]);
-    }
-    const int n = kTc2HalfN * (j >> 4) + 16 * comp + (j & 15);
-    char *rb = reinterpret_cast<char *>(sB);
-    *reinterpret_cast<float4 *>(rb + tc_off(n, 0)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-    *reinterpret_cast<float4 *>(rb + tc_off(n, 4)) = make_float4(hi[0], hi[1], hi[2], 0.0f);
-    *reinterpret_cast<float4 *>(rb + tc_off(n, 8)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
-    *reinterpret_cast<float4 *>(rb + tc_off(n, 12)) = make_float4(lo[0], lo[1], lo[2], 0.0f);
 }
 
 __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
@@ -1249,9 +1209,8 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
     float *sB = reinterpret_cast<float *>(tc_smem + kTc2OffB);
     float *red = reinterpret_cast<float *>(tc_smem + kTc2OffRed);  // [4][32]
     uint64_t *afull = reinterpret_cast<uint64_t *>(tc_smem + kTc2OffCtl);  // [kTc2Stages]: tile landed
-    uint64_t *full = afull + kTc2Stages;                                   // [2]: MMA of half h done
-    uint64_t *empty = full + 2;                                            // [2]: every warp read slot h
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(empty + 2);
+    uint64_t *mbar = afull + kTc2Stages;                                   // MMA done
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
     volatile int *err = reinterpret_cast<volatile int *>(tslot + 1);       // a wait gave up
     int *ctl = reinterpret_cast<int *>(tslot + 2);                          // [4]
     long long *run = reinterpret_cast<long long *>(tslot + 6);              // [2]
@@ -1259,10 +1218,7 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
     if (tid == 0) {
         *err = 0;
         for (int s = 0; s < kTc2Stages; ++s) mbar_init(&afull[s], 1);
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init(&empty[0], 4);
-        mbar_init(&empty[1], 4);
+        mbar_init(mbar, 1);
         fence_mbar_init();
     }
     if (w == 0) {
@@ -1275,12 +1231,11 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
     tc_fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);  // this warp's 32 lanes
-    // Phase parities every thread expects next: copies per stage (bit s), MMA
-    // halves (bit h), reads of slot h (bit h, waited on by thread 0 only).
-    uint32_t pa = 0, pf = 0, pe = 0;
-    // Thread 0: parity of the next copy / commit it issues, and which are in
-    // flight (issued, completion not yet seen), for the drain on an error.
-    uint32_t na = 0, nf = 0, fly_a = 0, fly_f = 0;
+    // Phase parity every thread expects next: per stage (bit s), and of the
+    // MMA barrier. Thread 0 also tracks what is in flight (issued, completion
+    // not yet seen) and the parity each will complete, for the drain on an error.
+    uint32_t pa = 0, pm = 0, fly_a = 0, par_a = 0, par_m = 0;
+    bool fly_m = false;
     int64_t gt = 0;  // tiles this CTA started (a tile's stage is its number mod kTc2Stages)
     const int64_t total = (int64_t)P.counters[kCScoreTotal];
     const int64_t ctas = gridDim.x;
@@ -1309,18 +1264,13 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
         const int nch = f.n_chunks;
         const int hb = (int)(local / nch), ch = (int)(local % nch);
         const int nh = f.hyp_count;
-        if (a != cur_a || hb != cur_hb) {  // every MMA of the previous item has completed
-            tc2_build_b(sB, P, f, hb);
-            cur_a = a;
-            cur_hb = hb;
-        }
         const int b0 = ch * f.chunk_blocks;
         const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
         const int ntiles = (b1 - b0 + 1) / 2;
         const float *gA = P.tcA + (f.blk_off + b0) * kTcABlockFloats;
         const float2 *gN = P.tcN + (f.blk_off + b0) * kSub;
         auto tile_blocks = [&](int i) { return min(2, b1 - b0 - 2 * i); };
-        auto issue_copy = [&](int i) {  // thread 0: tile i into its stage
+        auto issue_copy = [&](int i) {  // thread 0: tile i into its stage (free: its last reader is done)
             const int s = (int)((gt + i) % kTc2Stages);
             const int nb = tile_blocks(i);
             char *dst = stg + s * kTc2StageBytes;
@@ -1330,82 +1280,64 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
                          &afull[s]);
             bulk_copy_tx(dst + 2 * kTcABlockFloats * 4, gN + (int64_t)(2 * i) * kSub, (uint32_t)(nb * kSub * 8),
                          &afull[s]);
-            na ^= 1u << s;
+            // Every earlier use of stage s has been waited for: its waiters'
+            // next parity is the one this copy completes.
             fly_a |= 1u << s;
-        };
-        auto issue_mma = [&](int i, int h) {  // thread 0: tile i landed, slot h free
-            const int s = (int)((gt + i) % kTc2Stages);
-            const uint64_t da = tc_desc_sbo(stg + s * kTc2StageBytes, 256);
-            const char *bb = reinterpret_cast<const char *>(sB) + (kTc2HalfN / 8) * 512 * h;
-            tc2_mma(tmem + 64u * h, da, tc_desc_sbo(bb, 512), 0u);
-            tc2_mma(tmem + 64u * h, da, tc_desc_sbo(bb + 256, 512), 1u);
-            tc_commit(&full[h]);
-            nf ^= 1u << h;
-            fly_f |= 1u << h;
+            par_a = (par_a & ~(1u << s)) | (pa & (1u << s));
         };
         if (tid == 0 && !*err)
-            for (int i = 0; i < min(kTc2Stages, ntiles); ++i) issue_copy(i);
-        fence_proxy_async();  // the B operand, written by threads, is read by the tensor core
-        __syncthreads();
-        if (tid == 0 && !*err) {
-            const int s = (int)(gt % kTc2Stages);
-            if (!mbar_wait(&afull[s], (pa >> s) & 1u, kMaxPolls)) {
-                *err = 1;
-            } else {
-                fly_a &= ~(1u << s);
-                tc_fence_after();
-                issue_mma(0, 0);
-                issue_mma(0, 1);
-            }
+            for (int i = 0; i < min(kTc2Stages - 1, ntiles); ++i) issue_copy(i);
+        if (a != cur_a || hb != cur_hb) {  // every MMA of the previous item has completed
+            tc_build_b(sB, P, f, hb);
+            cur_a = a;
+            cur_hb = hb;
+            fence_proxy_async();  // the B operand, written by threads, is read by the tensor core
         }
+        __syncthreads();
         uint64_t acc[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) acc[j] = 0ull;
         for (int i = 0; i < ntiles; ++i) {
             const int s = (int)((gt + i) % kTc2Stages);
-            if (!*err && !mbar_wait(&afull[s], (pa >> s) & 1u, kMaxPolls)) *err = 1;
+            // The stage of tile i - 1 is free (the barrier closing that tile):
+            // it takes tile i + kTc2Stages - 1.
+            if (tid == 0 && !*err && i + kTc2Stages - 1 < ntiles) issue_copy(i + kTc2Stages - 1);
+            bool landed = false;
+            if (!*err) {
+                landed = mbar_wait(&afull[s], (pa >> s) & 1u, kMaxPolls);
+                if (!landed) *err = 1;
+            }
             pa ^= 1u << s;
+            if (tid == 0) {
+                if (landed) fly_a &= ~(1u << s);
+                if (!*err) {
+                    tc_fence_after();
+                    const uint64_t da = tc_desc_sbo(stg + s * kTc2StageBytes, 256);
+                    tc_mma(tmem, da, tc_desc(sB), 0u);
+                    tc_mma(tmem, da, tc_desc(reinterpret_cast<char *>(sB) + 256), 1u);
+                    tc_commit(mbar);
+                    fly_m = true;
+                    par_m = pm;
+                }
+            }
             const int64_t p0 = (int64_t)(b0 + 2 * i) * kSub;
             const int cnt = (int)min((int64_t)tile_blocks(i) * kSub, f.n - p0);
             const bool v = tid < cnt;
             const float2 nn = reinterpret_cast<const float2 *>(stg + s * kTc2StageBytes + 2 * kTcABlockFloats * 4)[tid];
             const uint64_t nx2 = f2pack(nn.x, nn.x), ny2 = f2pack(nn.y, nn.y);
+            if (!*err) {
+                if (!mbar_wait(mbar, pm, kMaxPolls)) *err = 1;
+                else if (tid == 0) fly_m = false;
+            }
+            pm ^= 1u;
+            tc_fence_after();
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                if (!*err) {
-                    if (!mbar_wait(&full[h], (pf >> h) & 1u, kMaxPolls)) *err = 1;
-                    else if (tid == 0) fly_f &= ~(1u << h);
-                }
-                pf ^= 1u << h;
-                tc_fence_after();
+            for (int gq = 0; gq < 2; ++gq) {
                 float z2[16], z0[16], z1[16];
-                tc_ld16(trow + 64u * h, z2);
-                tc_ld16(trow + 64u * h + 16u, z0);
-                tc_ld16(trow + 64u * h + 32u, z1);
+                tc_ld16(trow + (uint32_t)(16 * gq), z2);
+                tc_ld16(trow + (uint32_t)(kTcHyp + 16 * gq), z0);
+                tc_ld16(trow + (uint32_t)(2 * kTcHyp + 16 * gq), z1);
                 tc_wait_ld();
-                tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&empty[h]);
-                if (tid == 0 && i + 1 < ntiles && !*err) {
-                    // Slot h is free once every warp has read it; then the next
-                    // tile's half h (its stage waited for with the first half).
-                    bool go = mbar_wait(&empty[h], (pe >> h) & 1u, kMaxPolls);
-                    if (go && h == 0) {
-                        const int s1 = (int)((gt + i + 1) % kTc2Stages);
-                        go = mbar_wait(&afull[s1], (pa >> s1) & 1u, kMaxPolls);
-                        if (go) fly_a &= ~(1u << s1);
-                    }
-                    if (!go) {
-                        *err = 1;
-                    } else {
-                        tc_fence_after();
-                        issue_mma(i + 1, h);
-                        // Both MMAs of tile i have completed (this thread saw
-                        // full[1] of tile i): its stage takes tile i + kTc2Stages.
-                        if (h == 1 && i + kTc2Stages < ntiles) issue_copy(i + kTc2Stages);
-                    }
-                }
-                pe ^= 1u << h;
                 if (v) {
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
@@ -1419,15 +1351,16 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
                         float r0a, r0b, sa, sb;
                         f2unpack(r0, r0a, r0b);
                         f2unpack(r1s, sa, sb);
-                        acc[8 * h + q] =
-                            f2add(acc[8 * h + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
+                        acc[8 * gq + q] =
+                            f2add(acc[8 * gq + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
                     }
                 }
             }
+            tc_fence_before();
+            __syncthreads();  // the accumulator and this tile's stage are free again
         }
         gt += ntiles;
-        __syncthreads();
-        if (*err) ok = false;  // written before the barrier, so every thread reads the same
+        if (*err) ok = false;  // written before the last barrier, so every thread reads the same
         if (!ok) break;
         // Chunk partials: the warp's 32 hypotheses over its 32 points (lanes
         // 2p, 2p + 1 end with hypotheses 2p, 2p + 1), then the four warps in
@@ -1476,13 +1409,12 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
         __syncthreads();  // red and ctl are reused by the next item
     }
     if (!ok && tid == 0) {
-        // Give up: record it and let the copies and MMAs in flight land
+        // Give up: record it and let the copies and the MMA in flight land
         // (bounded) before the tensor memory is released.
         flag_error(P, kErrTimeout);
         for (int s = 0; s < kTc2Stages; ++s)
-            if (fly_a & (1u << s)) mbar_wait(&afull[s], ((na >> s) & 1u) ^ 1u, kMaxPolls);
-        for (int h = 0; h < 2; ++h)
-            if (fly_f & (1u << h)) mbar_wait(&full[h], ((nf >> h) & 1u) ^ 1u, kMaxPolls);
+            if (fly_a & (1u << s)) mbar_wait(&afull[s], (par_a >> s) & 1u, kMaxPolls);
+        if (fly_m) mbar_wait(mbar, par_m, kMaxPolls);
     }
     tc_fence_before();
     __syncthreads();
