@@ -1184,18 +1184,15 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
 // accumulator is free again). The two MMAs of a tile use the same A tile with
 // the hi and lo halves of the hypothesis rows:
 //   z = [Bh | Bh'] . [Ah | Al] + [Bl | Bl'] . [Ah | Al],
-// the four cross terms of the split products, exact in FP32. The epilogue
-// takes one reciprocal per two depths (Montgomery's batched inverse:
-// 1/a = b / (ab), 1/b = a / (ab)); depths are raised to 2^-63 (a point
-// behind the camera gets a residual of ~2^63 x its lateral offset and
-// saturates) and, by the bounds the staging puts on points and poses, stay
-// below 2^63, so the product is a normal FP32 number.
+// the four cross terms of the split products, exact in FP32. The epilogue is
+// the FP32 filter's: a depth below 2^-100 is raised to 2^-100 before its
+// reciprocal (a point behind the camera saturates), the residuals, the
+// saturating r^2 and the per-hypothesis sums.
 constexpr int kTc2Stages = 3;
 constexpr int kTc2StageBytes = 2 * kTcABlockFloats * 4 + 2 * kSub * 8;  // A 4096 + N 1024
 constexpr int kTc2OffB = kTc2Stages * kTc2StageBytes;
 constexpr int kTc2OffRed = kTc2OffB + 3 * kTcHyp * 16 * 4;               // B: 96 rows x 16 K
 constexpr int kTc2OffCtl = kTc2OffRed + 4 * kTcHyp * 4;
-constexpr float kTc2DepthFloor = 0x1p-63f;
 static_assert(kTc2OffCtl + 128 <= kTcSmem, "tensor-core scoring shared memory");
 
 __device__ __forceinline__ uint64_t tc_desc_sbo(const void *smem, uint32_t sbo) {
@@ -1341,10 +1338,9 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
                 if (v) {
 #pragma unroll
                     for (int q = 0; q < 8; ++q) {
-                        const float da = fmaxf(z2[2 * q], kTc2DepthFloor);
-                        const float db = fmaxf(z2[2 * q + 1], kTc2DepthFloor);
-                        const float ip = rcp_approx(da * db);
-                        const uint64_t inv = f2pack(db * ip, da * ip);
+                        const float ia = rcp_approx(fmaxf(z2[2 * q], kDepthFloor));
+                        const float ib = rcp_approx(fmaxf(z2[2 * q + 1], kDepthFloor));
+                        const uint64_t inv = f2pack(ia, ib);
                         const uint64_t r0 = f2fma(f2pack(z0[2 * q], z0[2 * q + 1]), inv, nx2);
                         const uint64_t r1 = f2fma(f2pack(z1[2 * q], z1[2 * q + 1]), inv, ny2);
                         const uint64_t r1s = f2mul(r1, r1);
