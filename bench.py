@@ -629,7 +629,7 @@ def main():
     nominal = 148 * 256 * 1965e6 / 1e12
     # The scoring kernel that ran: the FP32 pass or the tensor-core shape.
     tensor = args.tensor or bool(tuned and tuned["best"]["points_per_iter"] == 128)
-    kernel = "k_score_tc2" if tensor else "k_score"
+    kernel = "k_score_tc" if tensor else "k_score"
     traffic, traffic_source = stored_traffic(kernel)
 
     # e2e: public call, host buffers in, results out, every step. Inputs in

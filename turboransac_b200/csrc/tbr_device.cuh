@@ -483,22 +483,6 @@ __device__ __forceinline__ void bulk_load(void *dst_smem, const void *src_gmem, 
         "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
-// One arrival that expects `bytes` of transaction (the copies follow, with
-// bulk_copy_tx, onto the same barrier).
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_copy_tx(void *dst_smem, const void *src_gmem, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst_smem)),
-        "l"(src_gmem), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
 // Bounded wait on phase `parity`; returns false if it gave up.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls) {
     const uint32_t a = smem_addr(bar);

@@ -140,9 +140,9 @@ static RunOptions make_run_options(const tbr_ransac_options *ro, const tbr_bundl
         const int hpt = ext->hyp_per_thread, ppi = ext->points_per_iter;
         const bool fp32_hr = hpt == 2 || hpt == 4 || hpt == 6 || hpt == 8;
         const bool fp32_pp = ppi == 2 || ppi == 4;
-        if (ppi == kTcPP || ppi == kTcPP + 1) {
+        if (ppi == kTcPP) {
             o.hr = 1;
-            o.pp = ppi;
+            o.pp = kTcPP;
         } else if (fp32_hr || fp32_pp) {
             o.hr = fp32_hr ? hpt : 4;
             o.pp = fp32_pp ? ppi : 2;
@@ -244,8 +244,7 @@ class Engine {
         P.max_hyps = std::max<int64_t>(P.max_hyps, 4096);
         P.max_parts = P.max_hyps * 32;
         P.max_hb = P.max_hyps / 32 + kMaxActive;
-        const size_t per_block =
-            (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 8 + 8) + kBlockBytes + 4 * kTcABlockFloats + 8 * kSub;
+        const size_t per_block = (size_t)kSub * (16 + 24 + 16 + 1 + 16 + 24 + 8 + 8) + kBlockBytes;
         max_blocks = (int64_t)((rest - (size_t)(P.max_hyps * per_hyp) - P.max_hb * 4) / per_block) - 1;
         if (max_blocks < 64) return fail(TBR_ERR_INVALID_ARG, "workspace too small for points");
         // One allocation, carved with 256-byte alignment.
@@ -268,8 +267,6 @@ class Engine {
         add((void **)&P.lw64, 8 * np);
         add((void **)&P.prosac64, 8 * np);
         add((void **)&P.pts32, (size_t)kBlockBytes * max_blocks);
-        add((void **)&P.tcA, (size_t)4 * kTcABlockFloats * max_blocks);
-        add((void **)&P.tcN, (size_t)8 * kSub * max_blocks);
         add((void **)&P.sample_prefix, 8 * (kMaxActive + 1));
         add((void **)&P.item_prefix, 8 * (kMaxActive + 1));
         add((void **)&P.ritem_prefix, 8 * (kMaxActive + 1));
@@ -312,7 +309,6 @@ class Engine {
             score_grid[v] = num_sms * std::max(occ, 1);
         }
         TBR_CUDA(cudaFuncSetAttribute(k_score_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
-        TBR_CUDA(cudaFuncSetAttribute(k_score_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
         TBR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rescore, 256, 0));
         rescore_grid = num_sms * std::max(occ, 1);
         p3p_grid = num_sms * 8;
@@ -413,8 +409,7 @@ class Engine {
     // Scoring kernel variant: HR hypotheses per lane = 2*HP, PP points per iteration.
     void launch_score(const Pools &Q, int hr, int pp, cudaStream_t st) {
         const int threads = kScoreWarps * 32;
-        if (hr == 1 && pp == kTcPP + 1) k_score_tc<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);
-        else if (hr == 1) k_score_tc2<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);  // (pp == kTcPP)
+        if (hr == 1) k_score_tc<<<4 * num_sms, kTcThreads, kTcSmem, st>>>(Q);  // (pp == kTcPP)
         else if (hr == 2) k_score<1, 4><<<score_grid[0], threads, 0, st>>>(Q);
         else if (hr == 8) k_score<4, 2><<<score_grid[3], threads, 0, st>>>(Q);
         else if (hr == 6 && pp == 4) k_score<3, 4><<<score_grid[5], threads, 0, st>>>(Q);

@@ -158,9 +158,6 @@ struct Pools {
     double *lw64;        // LM: per-point loss multipliers (bundle adjust with honoured weights)
     int64_t *prosac64;   // PROSAC growth table of a frame, one entry per point (T'_k at k - 3)
     float2 *pts32;       // staging blocks: [X|Y|Z|-x/tau|-y/tau] x kSub, each value duplicated
-    float *tcA;          // tensor-core A operand per block: kSub rows [Xh Yh Zh 1 | Xl Yl Zl 0] (TF32 split),
-                         // K-major canonical layout (kTcABlockFloats per block)
-    float2 *tcN;         // per block: kSub x (-x/tau, -y/tau)
     // step prefixes (n_active + 1)
     int64_t *sample_prefix;
     int64_t *item_prefix;
@@ -255,18 +252,6 @@ __device__ __forceinline__ int find_segment(const int64_t *prefix, int n, int64_
     return lo;
 }
 
-// Round to nearest TF32 (10 stored mantissa bits): the operand the tensor core reads.
-__device__ __forceinline__ float tf32_rn(float x) {
-    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
-}
-// Byte offset of element (row r, k) of a K-major operand with 8 K values per
-// row, no swizzle: 8-row x 16-byte core matrices, the two K chunks of a row
-// group adjacent (leading byte offset 128), row groups 256 bytes apart.
-constexpr int kTcABlockFloats = kSub * 8;  // A operand of one staging block (2 KB)
-__device__ __forceinline__ int tc_off8(int r, int k) {
-    return (((r >> 3) * 2 + (k >> 2)) * 128) + (r & 7) * 16 + (k & 3) * 4;
-}
-
 __device__ __forceinline__ void flag_error(const Pools &P, unsigned long long bits) {
     atomicOr(&P.counters[kCError], bits);
 }
@@ -341,27 +326,18 @@ __global__ void k_prep_pack(Pools P) {
             v[4] = (float)(-yn * itau);
             bool finite = true;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) finite = finite && fabsf(v[k]) <= 0x1p40f;
-            if (!finite) {  // non-finite (never an FP64 inlier) or beyond 2^40: outlier for every pose
+            for (int k = 0; k < 5; ++k) finite = finite && fabsf(v[k]) <= 0x1p80f;
+            if (!finite) {  // non-finite (never an FP64 inlier) or beyond 2^80: outlier for every pose
                 v[0] = v[1] = v[2] = 0.0f;
                 v[3] = v[4] = 0x1p100f;
             }
         } else {
             v[0] = v[1] = v[2] = v[3] = v[4] = 0.0f;
         }
-        const int64_t b = f.blk_off + i / kSub;
-        float2 *blk = P.pts32 + b * kBlockFloat2;
+        float2 *blk = P.pts32 + (f.blk_off + i / kSub) * kBlockFloat2;
         const int j = (int)(i % kSub);
 #pragma unroll
         for (int k = 0; k < 5; ++k) blk[k * kSub + j] = make_float2(v[k], v[k]);
-        // Tensor-core operands of the point: row j of the block's A tile.
-        const float xh = tf32_rn(v[0]), yh = tf32_rn(v[1]), zh = tf32_rn(v[2]);
-        char *ra = reinterpret_cast<char *>(P.tcA + b * kTcABlockFloats);
-        const float one = i < f.n ? 1.0f : 0.0f;
-        *reinterpret_cast<float4 *>(ra + tc_off8(j, 0)) = make_float4(xh, yh, zh, one);
-        *reinterpret_cast<float4 *>(ra + tc_off8(j, 4)) =
-            make_float4(tf32_rn(v[0] - xh), tf32_rn(v[1] - yh), tf32_rn(v[2] - zh), 0.0f);
-        P.tcN[b * kSub + j] = make_float2(v[3], v[4]);
     }
 }
 
@@ -561,17 +537,12 @@ __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
                     q32[4 * r + 2] = (float)(S[4 * r + 2] * sc);
                     q32[4 * r + 3] = (float)(tc * sc);
                 }
-                // Bounds of the scoring form: rows 0, 1 (scaled by 1/tau) within 2^40
-                // and their translations within 2^80, so that z0, z1 of a staged point
-                // (within 2^40) stay finite (no inf - inf, no NaN in the filter); the
-                // depth row within 2^20 and its translation within 2^61, so that every
-                // depth is below 5 * 2^60 < 2^63 (the tensor-core filter multiplies two
-                // depths before one reciprocal: their product stays within the normal
-                // FP32 range).
+                // Rotation rows (scaled by 1/tau) within 2^40 and translations within
+                // 2^80 keep every depth of a staged point (within 2^80) below 2^123:
+                // no overflow, so no inf - inf and no NaN in the filter.
 #pragma unroll
                 for (int e = 0; e < 12; ++e)
-                    finite = finite && fabsf(q32[e]) <= (e < 8 ? ((e & 3) == 3 ? 0x1p80f : 0x1p40f)
-                                                                : (e == 11 ? 0x1p61f : 0x1p20f));
+                    finite = finite && fabsf(q32[e]) <= ((e & 3) == 3 ? 0x1p80f : 0x1p40f);
                 // A pose outside that range scores every point as an outlier
                 // (depth -1, lateral offset 1).
 #pragma unroll
@@ -908,6 +879,9 @@ __device__ __forceinline__ uint64_t tc_desc(const void *smem) {
     return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
            ((uint64_t)(512 >> 4) << 32) | (1ull << 46);
 }
+__device__ __forceinline__ float tf32_rn(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+}
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
@@ -1169,248 +1143,6 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
             mbar_wait(&bars[1], ph1, kMaxPolls);
             mbar_wait(&bars[2], phm ^ 1u, kMaxPolls);
         }
-    }
-    tc_fence_before();
-    __syncthreads();
-    if (w == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTcCols));
-}
-
-// ------------------------------- tensor-core scoring, staged operands --
-// The tensor-core filter with the A operand built once at admission: every
-// staging block carries the points' TF32 hi and lo parts (K = 8, k_prep_pack)
-// and their -x/tau, -y/tau, so a 128-point tile lands in shared memory by two
-// bulk copies into a 3-stage ring and the MMA reads it there: no thread
-// builds or fences the A tile, and a tile costs one CTA barrier (the
-// accumulator is free again). The two MMAs of a tile use the same A tile with
-// the hi and lo halves of the hypothesis rows:
-//   z = [Bh | Bh'] . [Ah | Al] + [Bl | Bl'] . [Ah | Al],
-// the four cross terms of the split products, exact in FP32. The epilogue is
-// the FP32 filter's: a depth below 2^-100 is raised to 2^-100 before its
-// reciprocal (a point behind the camera saturates), the residuals, the
-// saturating r^2 and the per-hypothesis sums.
-constexpr int kTc2Stages = 3;
-constexpr int kTc2StageBytes = 2 * kTcABlockFloats * 4 + 2 * kSub * 8;  // A 4096 + N 1024
-constexpr int kTc2OffB = kTc2Stages * kTc2StageBytes;
-constexpr int kTc2OffRed = kTc2OffB + 3 * kTcHyp * 16 * 4;               // B: 96 rows x 16 K
-constexpr int kTc2OffCtl = kTc2OffRed + 4 * kTcHyp * 4;
-static_assert(kTc2OffCtl + 128 <= kTcSmem, "tensor-core scoring shared memory");
-
-__device__ __forceinline__ uint64_t tc_desc_sbo(const void *smem, uint32_t sbo) {
-    return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
-           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
-}
-
-__global__ void __launch_bounds__(kTcThreads, 4) k_score_tc2(Pools P) {
-    extern __shared__ __align__(1024) unsigned char tc_smem[];
-    char *stg = reinterpret_cast<char *>(tc_smem);  // stage s: A tile (4096 B), then N (1024 B)
-    float *sB = reinterpret_cast<float *>(tc_smem + kTc2OffB);
-    float *red = reinterpret_cast<float *>(tc_smem + kTc2OffRed);  // [4][32]
-    uint64_t *afull = reinterpret_cast<uint64_t *>(tc_smem + kTc2OffCtl);  // [kTc2Stages]: tile landed
-    uint64_t *mbar = afull + kTc2Stages;                                   // MMA done
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(mbar + 1);
-    volatile int *err = reinterpret_cast<volatile int *>(tslot + 1);       // a wait gave up
-    int *ctl = reinterpret_cast<int *>(tslot + 2);                          // [4]
-    long long *run = reinterpret_cast<long long *>(tslot + 6);              // [2]
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    if (tid == 0) {
-        *err = 0;
-        for (int s = 0; s < kTc2Stages; ++s) mbar_init(&afull[s], 1);
-        mbar_init(mbar, 1);
-        fence_mbar_init();
-    }
-    if (w == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tslot)),
-                     "r"((uint32_t)kTcCols));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tslot;
-    const uint32_t trow = tmem + ((uint32_t)(w * 32) << 16);  // this warp's 32 lanes
-    // Phase parity every thread expects next: per stage (bit s), and of the
-    // MMA barrier. Thread 0 also tracks what is in flight (issued, completion
-    // not yet seen) and the parity each will complete, for the drain on an error.
-    uint32_t pa = 0, pm = 0, fly_a = 0, par_a = 0, par_m = 0;
-    bool fly_m = false;
-    int64_t gt = 0;  // tiles this CTA started (a tile's stage is its number mod kTc2Stages)
-    const int64_t total = (int64_t)P.counters[kCScoreTotal];
-    const int64_t ctas = gridDim.x;
-    int cur_a = -1, cur_hb = -1;
-    int64_t run_next = 0, run_end = 0;
-    bool ok = true;
-    for (;;) {
-        if (run_next >= run_end) {
-            if (tid == 0) {
-                const int64_t done = (int64_t)*(volatile unsigned long long *)&P.counters[kCScoreNext];
-                const int64_t len = max((int64_t)1, min((int64_t)8, (total - done) / (4 * ctas)));
-                run[0] = (long long)atomicAdd(&P.counters[kCScoreNext], (unsigned long long)len);
-                run[1] = len;
-            }
-            __syncthreads();
-            const int64_t start = run[0], len = run[1];
-            __syncthreads();
-            if (start >= total) break;
-            run_next = start;
-            run_end = min(total, start + len);
-        }
-        const int64_t item = run_next++;
-        const int a = find_segment(P.item_prefix, P.n_active, item);
-        FrameDev &f = P.frames[P.active[a]];
-        const int64_t local = item - P.item_prefix[a];
-        const int nch = f.n_chunks;
-        const int hb = (int)(local / nch), ch = (int)(local % nch);
-        const int nh = f.hyp_count;
-        const int b0 = ch * f.chunk_blocks;
-        const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
-        const int ntiles = (b1 - b0 + 1) / 2;
-        const float *gA = P.tcA + (f.blk_off + b0) * kTcABlockFloats;
-        const float2 *gN = P.tcN + (f.blk_off + b0) * kSub;
-        auto tile_blocks = [&](int i) { return min(2, b1 - b0 - 2 * i); };
-        auto issue_copy = [&](int i) {  // thread 0: tile i into its stage (free: its last reader is done)
-            const int s = (int)((gt + i) % kTc2Stages);
-            const int nb = tile_blocks(i);
-            char *dst = stg + s * kTc2StageBytes;
-            fence_proxy_async();
-            mbar_expect_tx(&afull[s], (uint32_t)(nb * (kTcABlockFloats * 4 + kSub * 8)));
-            bulk_copy_tx(dst, gA + (int64_t)(2 * i) * kTcABlockFloats, (uint32_t)(nb * kTcABlockFloats * 4),
-                         &afull[s]);
-            bulk_copy_tx(dst + 2 * kTcABlockFloats * 4, gN + (int64_t)(2 * i) * kSub, (uint32_t)(nb * kSub * 8),
-                         &afull[s]);
-            // Every earlier use of stage s has been waited for: its waiters'
-            // next parity is the one this copy completes.
-            fly_a |= 1u << s;
-            par_a = (par_a & ~(1u << s)) | (pa & (1u << s));
-        };
-        if (tid == 0 && !*err)
-            for (int i = 0; i < min(kTc2Stages - 1, ntiles); ++i) issue_copy(i);
-        if (a != cur_a || hb != cur_hb) {  // every MMA of the previous item has completed
-            tc_build_b(sB, P, f, hb);
-            cur_a = a;
-            cur_hb = hb;
-            fence_proxy_async();  // the B operand, written by threads, is read by the tensor core
-        }
-        __syncthreads();
-        uint64_t acc[16];
-#pragma unroll
-        for (int j = 0; j < 16; ++j) acc[j] = 0ull;
-        for (int i = 0; i < ntiles; ++i) {
-            const int s = (int)((gt + i) % kTc2Stages);
-            // The stage of tile i - 1 is free (the barrier closing that tile):
-            // it takes tile i + kTc2Stages - 1.
-            if (tid == 0 && !*err && i + kTc2Stages - 1 < ntiles) issue_copy(i + kTc2Stages - 1);
-            bool landed = false;
-            if (!*err) {
-                landed = mbar_wait(&afull[s], (pa >> s) & 1u, kMaxPolls);
-                if (!landed) *err = 1;
-            }
-            pa ^= 1u << s;
-            if (tid == 0) {
-                if (landed) fly_a &= ~(1u << s);
-                if (!*err) {
-                    tc_fence_after();
-                    const uint64_t da = tc_desc_sbo(stg + s * kTc2StageBytes, 256);
-                    tc_mma(tmem, da, tc_desc(sB), 0u);
-                    tc_mma(tmem, da, tc_desc(reinterpret_cast<char *>(sB) + 256), 1u);
-                    tc_commit(mbar);
-                    fly_m = true;
-                    par_m = pm;
-                }
-            }
-            const int64_t p0 = (int64_t)(b0 + 2 * i) * kSub;
-            const int cnt = (int)min((int64_t)tile_blocks(i) * kSub, f.n - p0);
-            const bool v = tid < cnt;
-            const float2 nn = reinterpret_cast<const float2 *>(stg + s * kTc2StageBytes + 2 * kTcABlockFloats * 4)[tid];
-            const uint64_t nx2 = f2pack(nn.x, nn.x), ny2 = f2pack(nn.y, nn.y);
-            if (!*err) {
-                if (!mbar_wait(mbar, pm, kMaxPolls)) *err = 1;
-                else if (tid == 0) fly_m = false;
-            }
-            pm ^= 1u;
-            tc_fence_after();
-#pragma unroll
-            for (int gq = 0; gq < 2; ++gq) {
-                float z2[16], z0[16], z1[16];
-                tc_ld16(trow + (uint32_t)(16 * gq), z2);
-                tc_ld16(trow + (uint32_t)(kTcHyp + 16 * gq), z0);
-                tc_ld16(trow + (uint32_t)(2 * kTcHyp + 16 * gq), z1);
-                tc_wait_ld();
-                if (v) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const float ia = rcp_approx(fmaxf(z2[2 * q], kDepthFloor));
-                        const float ib = rcp_approx(fmaxf(z2[2 * q + 1], kDepthFloor));
-                        const uint64_t inv = f2pack(ia, ib);
-                        const uint64_t r0 = f2fma(f2pack(z0[2 * q], z0[2 * q + 1]), inv, nx2);
-                        const uint64_t r1 = f2fma(f2pack(z1[2 * q], z1[2 * q + 1]), inv, ny2);
-                        const uint64_t r1s = f2mul(r1, r1);
-                        float r0a, r0b, sa, sb;
-                        f2unpack(r0, r0a, r0b);
-                        f2unpack(r1s, sa, sb);
-                        acc[8 * gq + q] =
-                            f2add(acc[8 * gq + q], f2pack(fma_sat(r0a, r0a, sa), fma_sat(r0b, r0b, sb)));
-                    }
-                }
-            }
-            tc_fence_before();
-            __syncthreads();  // the accumulator and this tile's stage are free again
-        }
-        gt += ntiles;
-        if (*err) ok = false;  // written before the last barrier, so every thread reads the same
-        if (!ok) break;
-        // Chunk partials: the warp's 32 hypotheses over its 32 points (lanes
-        // 2p, 2p + 1 end with hypotheses 2p, 2p + 1), then the four warps in
-        // fixed order.
-#pragma unroll
-        for (int o = 16, m = 8; o >= 2; o >>= 1, m >>= 1) {
-            const bool up = (lane & o) != 0;
-#pragma unroll
-            for (int jj = 0; jj < m; ++jj) {
-                const uint64_t keep = up ? acc[m + jj] : acc[jj];
-                const uint64_t send = up ? acc[jj] : acc[m + jj];
-                acc[jj] = f2add(keep, __shfl_xor_sync(0xffffffffu, send, o));
-            }
-        }
-        acc[0] = f2add(acc[0], __shfl_xor_sync(0xffffffffu, acc[0], 1));
-        if ((lane & 1) == 0) {
-            float lo, hi;
-            f2unpack(acc[0], lo, hi);
-            red[w * kTcHyp + lane] = lo;
-            red[w * kTcHyp + lane + 1] = hi;
-        }
-        __syncthreads();
-        float *part = P.part + f.part_base;
-        if (tid < kTcHyp) {
-            const int i = hb * kTcHyp + tid;
-            const float s4 = ((red[tid] + red[kTcHyp + tid]) + red[2 * kTcHyp + tid]) + red[3 * kTcHyp + tid];
-            if (i < nh) part[(int64_t)i * nch + ch] = s4;
-        }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) ctl[2] = (int)atomicAdd(&P.hb_arrive[f.hb_base + hb], 1u);
-        __syncthreads();
-        if (ctl[2] == nch - 1 && tid < kTcHyp) {
-            __threadfence();
-            const int i = hb * kTcHyp + tid;
-            if (i < nh) {
-                float s = 0.0f;
-                for (int q = 0; q < nch; ++q) s += __ldcg(part + (int64_t)i * nch + q);
-                P.hS32[f.hyp_base + i] = s;
-                const int64_t sample = P.hId[f.hyp_base + i] >> 2;
-                const int64_t r = (sample - f.step_first) / f.step_div;
-                const unsigned long long key = ((unsigned long long)__float_as_uint(s) << 32) | (unsigned)i;
-                atomicMin(&f.round_min[r], key);
-            }
-        }
-        __syncthreads();  // red and ctl are reused by the next item
-    }
-    if (!ok && tid == 0) {
-        // Give up: record it and let the copies and the MMA in flight land
-        // (bounded) before the tensor memory is released.
-        flag_error(P, kErrTimeout);
-        for (int s = 0; s < kTc2Stages; ++s)
-            if (fly_a & (1u << s)) mbar_wait(&afull[s], (par_a >> s) & 1u, kMaxPolls);
-        if (fly_m) mbar_wait(mbar, par_m, kMaxPolls);
     }
     tc_fence_before();
     __syncthreads();
