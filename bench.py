@@ -341,6 +341,7 @@ def run_serving_capacity(ctx, reqs, repeats=10, budget=8 << 30, shape=None):
         srv.submit(r)
     srv.drain()
     srv.poll()
+    pairs0 = srv.stats()["pairs_scored"]
     ids = {}
     t0 = time.perf_counter()
     for _ in range(repeats):
@@ -365,6 +366,7 @@ def run_serving_capacity(ctx, reqs, repeats=10, budget=8 << 30, shape=None):
     return {"frames_per_s": len(got) / dt, "requests": len(got), "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "success_rate": ok / max(len(got), 1),
             "load": f"{repeats} x {len(reqs)} serving requests submitted at once", "seconds": dt,
+            "pairs_scored_per_s": (sst["pairs_scored"] - pairs0) / dt,
             "server": {"steps": sst["steps"], "mean_resident": sst["resident_sum"] / max(sst["steps"], 1),
                        "device_wait_ms": sst["device_wait_ms"], "host_stage_ms": sst["host_stage_ms"],
                        "host_retire_ms": sst["host_retire_ms"], "host_launch_ms": sst["host_launch_ms"]}}

@@ -311,6 +311,7 @@ typedef struct tbr_server_stats {
     double device_wait_ms;  /* waiting for the step in flight */
     double host_retire_ms;  /* downloading and publishing results */
     double host_launch_ms;  /* uploads and step launches */
+    int64_t pairs_scored;   /* (hypothesis, point) pairs scored by the steps retired so far */
 } tbr_server_stats;
 
 tbr_status tbr_server_create(tbr_context *ctx, const tbr_server_config *cfg, tbr_server **out);

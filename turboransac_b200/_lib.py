@@ -97,7 +97,8 @@ class TuneEntryC(C.Structure):
 class ServerStatsC(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
                 ("steps", C.c_int64), ("resident_sum", C.c_int64), ("host_stage_ms", C.c_double),
-                ("device_wait_ms", C.c_double), ("host_retire_ms", C.c_double), ("host_launch_ms", C.c_double)]
+                ("device_wait_ms", C.c_double), ("host_retire_ms", C.c_double), ("host_launch_ms", C.c_double),
+                ("pairs_scored", C.c_int64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

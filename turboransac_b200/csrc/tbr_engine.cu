@@ -2088,6 +2088,7 @@ static tbr_status server_retire_oldest(tbr_server *s) {
     TBR_CUDA(cudaEventSynchronize(s->ev_done[st.buf]));
     s->ws.device_wait_ms += ms_since(t0);
     if (s->h_cnt[st.buf][kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    s->ws.pairs_scored = (int64_t)s->h_cnt[st.buf][kCPairsTotal];
     t0 = std::chrono::steady_clock::now();
     std::unordered_map<uint64_t, size_t> pos;
     for (size_t i = 0; i < s->resident.size(); ++i) pos[s->resident[i].req->id] = i;
@@ -2280,6 +2281,7 @@ static tbr_status server_step(tbr_server *s) {
     s->stats.device_wait_ms = s->ws.device_wait_ms;
     s->stats.host_retire_ms = s->ws.host_retire_ms;
     s->stats.host_launch_ms = s->ws.host_launch_ms;
+    s->stats.pairs_scored = s->ws.pairs_scored;
     return TBR_OK;
 }
 
