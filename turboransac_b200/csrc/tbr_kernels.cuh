@@ -845,8 +845,10 @@ __global__ void __launch_bounds__(kScoreWarps * 32) k_score(Pools P) {
 // memory, and the epilogue (one thread per point) does the reciprocal, the
 // residuals, the saturating r^2 and the sum per hypothesis. TF32 keeps 11 significant bits,
 // so each operand is split into a hi part (rounded to nearest TF32) and the
-// rounded remainder, and K carries all four cross terms
-//   A row (point)      = [Xh Yh Zh 1 | Xl Yl Zl 0 | Xh Yh Zh 1 | Xl Yl Zl 0]
+// rounded remainder, and the two MMA steps carry all four cross terms: both
+// read the same A row (K = 8), the first with the hi, the second with the lo
+// half of the hypothesis row
+//   A row (point)      = [Xh Yh Zh 1 | Xl Yl Zl 0]
 //   B row (hyp. row c) = [ch0..ch3   | ch0..ch2 0 | cl0..cl3   | cl0..cl2 0]
 // whose products are exact in FP32 and sum to c . [X 1] with an error of the
 // order of FP32 rounding (the remainders' own rounding is 2^-23 relative).
@@ -874,6 +876,15 @@ constexpr int kTcOffA = 0, kTcOffB = 8192, kTcOffPts = 14336, kTcOffRed = 24576,
 // group adjacent (leading byte offset 128), row groups 512 bytes apart.
 __device__ __forceinline__ int tc_off(int r, int k) {
     return (((r >> 3) * 4 + (k >> 2)) * 128) + (r & 7) * 16 + (k & 3) * 4;
+}
+// K-major operand with 8 K values per row (two 16-byte K chunks, leading byte
+// offset 128, row groups 256 bytes apart).
+__device__ __forceinline__ int tc_off8(int r, int k) {
+    return (((r >> 3) * 2 + (k >> 2)) * 128) + (r & 7) * 16 + (k & 3) * 4;
+}
+__device__ __forceinline__ uint64_t tc_desc_sbo(const void *smem, uint32_t sbo) {
+    return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
 }
 __device__ __forceinline__ uint64_t tc_desc(const void *smem) {
     return (uint64_t)((smem_addr(smem) >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) |
@@ -1034,19 +1045,19 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
                 const float xh = tf32_rn(X), yh = tf32_rn(Y), zh = tf32_rn(Z);
                 const float xl = tf32_rn(X - xh), yl = tf32_rn(Y - yh), zl = tf32_rn(Z - zh);
                 const float one = v ? 1.0f : 0.0f;
+                // K = 8 (the two MMAs read the same A chunks with the hi and the
+                // lo half of the hypothesis rows): row groups 256 bytes apart.
                 char *ra = reinterpret_cast<char *>(sA);
-                *reinterpret_cast<float4 *>(ra + tc_off(tid, 0)) = make_float4(xh, yh, zh, one);
-                *reinterpret_cast<float4 *>(ra + tc_off(tid, 4)) = make_float4(xl, yl, zl, 0.0f);
-                *reinterpret_cast<float4 *>(ra + tc_off(tid, 8)) = make_float4(xh, yh, zh, one);
-                *reinterpret_cast<float4 *>(ra + tc_off(tid, 12)) = make_float4(xl, yl, zl, 0.0f);
+                *reinterpret_cast<float4 *>(ra + tc_off8(tid, 0)) = make_float4(xh, yh, zh, one);
+                *reinterpret_cast<float4 *>(ra + tc_off8(tid, 4)) = make_float4(xl, yl, zl, 0.0f);
             }
             fence_proxy_async();  // the operands, written by threads, are read by the tensor core
             __syncthreads();      // the A tile is complete; staging buffer s is free
             if (tid == 0) {
                 tc_fence_after();
-                tc_mma(tmem, tc_desc(sA), tc_desc(sB), 0u);
-                tc_mma(tmem, tc_desc(reinterpret_cast<char *>(sA) + 256), tc_desc(reinterpret_cast<char *>(sB) + 256),
-                       1u);
+                const uint64_t da = tc_desc_sbo(sA, 256);
+                tc_mma(tmem, da, tc_desc(sB), 0u);
+                tc_mma(tmem, da, tc_desc(reinterpret_cast<char *>(sB) + 256), 1u);
                 tc_commit(&bars[2]);
                 if (i + 2 < ntiles) {
                     fence_proxy_async();
