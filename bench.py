@@ -632,7 +632,7 @@ def main():
     # The scoring kernel that ran: the FP32 pass or the tensor-core shape.
     tensor = args.tensor or bool(tuned and tuned["best"]["points_per_iter"] == 128)
     kernel = "k_score_tc" if tensor else "k_score"
-    traffic, traffic_source = stored_traffic(kernel)
+    traffic, traffic_source, pipes = stored_traffic(kernel, frames)
 
     # e2e: public call, host buffers in, results out, every step. Inputs in
     # page-locked host memory (as a data loader would hand them over); the
@@ -735,7 +735,7 @@ def main():
             "pairs_scored_per_batch": pairs,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak_fp32, "unit": "TFLOP/s",
                          "frac": achieved / peak_fp32 if peak_fp32 else None, "traffic": traffic,
-                         "traffic_source": traffic_source,
+                         "traffic_source": traffic_source, "pipes_ncu": pipes,
                          "kernel": kernel, "flop_per_pair": FLOP_PER_PAIR, "pairs_per_s": pairs / (score_ms / 1000.0),
                          "accounting": ("27 FP32-equivalent FLOP per pair: the projection's 18 on the tensor "
                                         "cores (tcgen05 TF32, split operands), the rest on the FP32 pipe")
@@ -771,18 +771,23 @@ def main():
         pg.destroy_process_group()
 
 
-def stored_traffic(kernel: str):
-    """DRAM bytes per launch of the scoring kernel on this workload, from the
-    ncu capture summarised under profiles/ (ncu does not run inside the bench):
-    (bytes, a note naming the capture and its date) or (None, why)."""
+def stored_traffic(kernel: str, frames):
+    """DRAM bytes of the scoring kernel's first launch on this workload (every
+    frame active), from the ncu capture summarised under profiles/ (ncu does not
+    run inside the bench): bytes per staged point of the captured case times
+    this workload's staged points. Returns (bytes, a note naming the capture
+    and its date, pipe utilisations of that capture) or (None, why, None)."""
     tpath = os.path.join(ROOT, "profiles", "k_score_traffic.json")
     try:
         k = json.load(open(tpath))["kernels"][kernel]
-        return k["bytes_per_launch"], (f"not measured in this run: ncu dram__bytes_read.sum + "
-                                       f"dram__bytes_write.sum per {kernel} launch, captured {k['captured']} "
-                                       f"({k['summary']})")
+        pts = sum(((f.n + 63) // 64) * 64 for f in frames)
+        return int(k["bytes_per_staged_point"] * pts), (
+            f"not measured in this run: first engine step's launch (all frames active), ncu "
+            f"dram__bytes_read.sum + dram__bytes_write.sum of the 64-frame case captured {k['captured']} "
+            f"({k['bytes_per_staged_point']:.1f} B per staged point: each point's 40-byte record and each "
+            f"hypothesis read once) x {pts} staged points; {k['summary']}"), k.get("pipes_first_launch")
     except Exception:
-        return None, f"no stored ncu capture of {kernel} on this workload"
+        return None, f"no stored ncu capture of {kernel} on this workload", None
 
 
 def fp32_peak_tflops(ctx) -> float | None:
