@@ -599,8 +599,11 @@ __global__ void k_score_plan(Pools P) {
         items = (int64_t)nhb * nch;
         parts = (int64_t)f->hyp_count * nch;
         hbs = nhb;
-#pragma unroll 1
-        for (int r = 0; r < kMaxRoundsPerStep; ++r) f->round_min[r] = ~0ull;
+    }
+    // Round minima of every planned frame, reset by the whole block.
+    for (int idx = threadIdx.x; idx < P.n_active * kMaxRoundsPerStep; idx += blockDim.x) {
+        FrameDev &g = P.frames[P.active[idx / kMaxRoundsPerStep]];
+        if (g.step_samples > 0) g.round_min[idx % kMaxRoundsPerStep] = ~0ull;
     }
     int64_t tot;
     const int64_t iexcl = block_exclusive_scan(items, sh, tot);
@@ -615,10 +618,9 @@ __global__ void k_score_plan(Pools P) {
     if (act) f->part_base = pexcl;
     if (a == 0 && tot > P.max_parts) flag_error(P, kErrOverflow);
     const int64_t hexcl = block_exclusive_scan(hbs, sh, tot);
-    if (act) {
-        f->hb_base = hexcl;
-        for (int i = 0; i < hbs; ++i) P.hb_arrive[hexcl + i] = 0;
-    }
+    if (act) f->hb_base = hexcl;
+    // The step's hypothesis-block arrival counters are [0, tot): zeroed by the block.
+    for (int64_t i = threadIdx.x; i < min(tot, P.max_hb); i += blockDim.x) P.hb_arrive[i] = 0;
     if (a == 0 && tot > P.max_hb) flag_error(P, kErrOverflow);
 }
 
@@ -1331,9 +1333,11 @@ __global__ void k_rescore_plan(Pools P) {
             f.n_rchunks = nrc;
             f.rchunk = (f.n + nrc - 1) / nrc;
             items = (int64_t)((f.cand_count + kRescoreGroup - 1) / kRescoreGroup) * nrc;
-            for (int c = 0; c < f.cand_count; ++c) P.c_arrive[f.cand_base + c] = 0;
         }
     }
+    // The step's candidates lie in [0, claimed) of the pool: arrival counters zeroed by the block.
+    const int64_t claimed = min((int64_t)P.counters[kCCandNext], P.cand_cap);
+    for (int64_t c = threadIdx.x; c < claimed; c += blockDim.x) P.c_arrive[c] = 0;
     int64_t tot;
     const int64_t ex = block_exclusive_scan(items, sh, tot);
     if (a < P.n_active) P.ritem_prefix[a] = ex;
