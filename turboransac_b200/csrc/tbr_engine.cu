@@ -197,7 +197,9 @@ class Engine {
     int rescore_grid = 0, p3p_grid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
+    cudaStream_t stream3 = nullptr;             // cluster LM beside the one-CTA LM
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_lm_fork = nullptr, ev_lm_join = nullptr;
     void *d_stage_alias = nullptr;              // device address of the pinned staging buffer
     std::mutex mu;  // one call at a time per context
 
@@ -213,6 +215,9 @@ class Engine {
         if (ev1) cudaEventDestroy(ev1);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_lm_fork) cudaEventDestroy(ev_lm_fork);
+        if (ev_lm_join) cudaEventDestroy(ev_lm_join);
+        if (stream3) cudaStreamDestroy(stream3);
         if (ev_ingest) cudaEventDestroy(ev_ingest);
         if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
@@ -228,6 +233,9 @@ class Engine {
         TBR_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+        TBR_CUDA(cudaStreamCreateWithFlags(&stream3, cudaStreamNonBlocking));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_lm_fork, cudaEventDisableTiming));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_lm_join, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_ingest, cudaEventDisableTiming));
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
@@ -440,8 +448,15 @@ class Engine {
         auto end = [&](int k) { if (prof) { cudaEventRecord(prof->ev[2 * k + 1], st); prof->launches[k]++; } };
         beg(8); k_inliers<<<n_active, 1024, 0, st>>>(Q); end(8);
         beg(9);
+        // The one-CTA and the cluster LM take disjoint frames (by inlier
+        // count): they run side by side, so the branch lasts as long as the
+        // slower of the two, not their sum.
+        cudaEventRecord(ev_lm_fork, st);
+        cudaStreamWaitEvent(stream3, ev_lm_fork, 0);
+        k_lm<<<n_active * kLMCluster, kLMThreads, 0, stream3>>>(Q);
         k_lm_small<<<n_active, kLMSmallThreads, 0, st>>>(Q);
-        k_lm<<<n_active * kLMCluster, kLMThreads, 0, st>>>(Q);
+        cudaEventRecord(ev_lm_join, stream3);
+        cudaStreamWaitEvent(st, ev_lm_join, 0);
         end(9);
     }
     // Host-stepped: RANSAC, close the step, refine what finished.
