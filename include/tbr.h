@@ -154,8 +154,9 @@ tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context 
 /* Also frees every batch made on the context that is still alive (a batch
  * uses the context's workspace and stream): those handles are dead afterwards,
  * and tbr_batch_destroy on one is a no-op, any other call on one returns
- * TBR_ERR_INVALID_ARG. A server takes only the device from its context and may
- * outlive it. */
+ * TBR_ERR_INVALID_ARG. Uncollected tickets (tbr_estimate_batch_submit) are
+ * freed the same way: collect on one returns TBR_ERR_INVALID_ARG. A server
+ * takes only the device from its context and may outlive it. */
 void tbr_context_destroy(tbr_context *ctx);
 
 /* estimate_absolute_pose_cuda (entry.h:13-19). Host buffers:
@@ -227,6 +228,35 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
 tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
                                      const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
                                      void *stream, tbr_frame_result *results, uint8_t *const *inliers);
+
+/* Submitted batches (no reference counterpart; the reference's call,
+ * estimate_absolute_pose_cuda in entry.h:13-19, returns only when its frame is
+ * done): tbr_estimate_batch split into a submit that queues the whole run and
+ * returns, and a collect that waits for it and writes the results. While the
+ * device runs one batch the caller can prepare and submit the next, so the
+ * host work of a call (descriptors, staging, launches, the result round
+ * trip) overlaps the previous batch's device work.
+ *   - Same frames, options, checks and results as tbr_estimate_batch (every
+ *     frame's result is independent of the batch it runs in); at most 1024
+ *     frames per submission.
+ *   - The frames' arrays are read while the batch runs: they must stay valid
+ *     and unchanged until tbr_estimate_batch_collect returns for the ticket.
+ *   - A context has two sets of call buffers. Two submitted batches can have
+ *     device work queued at once; submitting a third first waits for the
+ *     oldest one's device work (its results stay with its ticket).
+ *   - The frames hold their workspace until collected: a submission that does
+ *     not fit beside the uncollected ones fails with TBR_ERR_OOM (points) or
+ *     TBR_ERR_CAPACITY (frame slots).
+ *   - Every other call on the context first waits for the device work of all
+ *     submitted batches (their results stay with their tickets).
+ *   - collect(ticket, results, inliers): results may be NULL (the ticket is
+ *     released without results); inliers as in tbr_estimate_batch. The ticket
+ *     is freed by collect, whatever it returns, and by tbr_context_destroy. */
+typedef struct tbr_ticket tbr_ticket;
+tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                     tbr_ticket **ticket);
+tbr_status tbr_estimate_batch_collect(tbr_ticket *ticket, tbr_frame_result *results, uint8_t *const *inliers);
 
 /* Device-resident batch: upload once (host->device), run many times with the
  * inputs already in HBM, download results. run() launches the captured graph

@@ -201,7 +201,39 @@ class Engine {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_lm_fork = nullptr, ev_lm_join = nullptr;
     void *d_stage_alias = nullptr;              // device address of the pinned staging buffer
+    cudaEvent_t ev_done = nullptr;              // a submitted batch's downloads have landed
+    cudaStream_t stream_out = nullptr;          // inlier masks of a collected batch
     std::mutex mu;  // one call at a time per context
+
+    // Per-call host buffers: h_stage (with its size and device alias),
+    // h_counters, h_results, ev0, ev1 and ev_done above are the bound set;
+    // `spare` holds the other one. Submitted batches use the two sets in turn
+    // (next_set), so that one can be staged while the other's copies and
+    // downloads are still queued; owner[k] is the ticket whose queued work
+    // uses set k (nullptr: none).
+    struct CallBuffers {
+        void *h_stage = nullptr;
+        size_t h_stage_bytes = 0;
+        void *d_stage_alias = nullptr;
+        unsigned long long *h_counters = nullptr;
+        FrameResult *h_results = nullptr;
+        cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
+    };
+    CallBuffers spare;
+    int bound = 0, next_set = 0;
+    ::tbr_ticket *owner[2] = {nullptr, nullptr};
+    void bind_set(int k) {
+        if (k == bound) return;
+        std::swap(h_stage, spare.h_stage);
+        std::swap(h_stage_bytes, spare.h_stage_bytes);
+        std::swap(d_stage_alias, spare.d_stage_alias);
+        std::swap(h_counters, spare.h_counters);
+        std::swap(h_results, spare.h_results);
+        std::swap(ev0, spare.ev0);
+        std::swap(ev1, spare.ev1);
+        std::swap(ev_done, spare.ev_done);
+        bound = k;
+    }
 
     ~Engine() {
         if (stream) cudaStreamSynchronize(stream);
@@ -219,6 +251,14 @@ class Engine {
         if (ev_lm_join) cudaEventDestroy(ev_lm_join);
         if (stream3) cudaStreamDestroy(stream3);
         if (ev_ingest) cudaEventDestroy(ev_ingest);
+        if (ev_done) cudaEventDestroy(ev_done);
+        if (stream_out) cudaStreamDestroy(stream_out);
+        if (spare.h_stage) cudaFreeHost(spare.h_stage);
+        if (spare.h_counters) cudaFreeHost(spare.h_counters);
+        if (spare.h_results) cudaFreeHost(spare.h_results);
+        if (spare.ev0) cudaEventDestroy(spare.ev0);
+        if (spare.ev1) cudaEventDestroy(spare.ev1);
+        if (spare.ev_done) cudaEventDestroy(spare.ev_done);
         if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -237,6 +277,11 @@ class Engine {
         TBR_CUDA(cudaEventCreateWithFlags(&ev_lm_fork, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_lm_join, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_ingest, cudaEventDisableTiming));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
+        TBR_CUDA(cudaStreamCreateWithFlags(&stream_out, cudaStreamNonBlocking));
+        TBR_CUDA(cudaEventCreate(&spare.ev0));
+        TBR_CUDA(cudaEventCreate(&spare.ev1));
+        TBR_CUDA(cudaEventCreateWithFlags(&spare.ev_done, cudaEventDisableTiming));
         if (budget == 0) budget = 1ull << 30;
         max_frames = std::min(frames_cap, kMaxActive);
         // Split: 30 % hypotheses, the rest points, after the per-frame state.
@@ -307,6 +352,8 @@ class Engine {
         TBR_CUDA(cudaMemsetAsync(P.frames, 0, sizeof(FrameDev) * max_frames, stream));
         TBR_CUDA(cudaMallocHost(&h_counters, 8 * kCNum));
         TBR_CUDA(cudaMallocHost(&h_results, sizeof(FrameResult) * kMaxActive));
+        TBR_CUDA(cudaMallocHost(&spare.h_counters, 8 * kCNum));
+        TBR_CUDA(cudaMallocHost(&spare.h_results, sizeof(FrameResult) * kMaxActive));
         blocks.reset(max_blocks);
         for (int i = max_frames - 1; i >= 0; --i) free_slots.push_back(i);
         int occ = 0;
@@ -1230,10 +1277,81 @@ using namespace tbr;
 
 struct tbr_context {
     Engine E;
+    std::vector<tbr_ticket *> tickets;  // submitted, not yet collected
+};
+
+// A submitted batch: its frames' slots and workspace blocks (held until
+// collect), the call-buffer set its queued downloads land in, and, once
+// retired (its device work waited for), its results.
+struct tbr_ticket {
+    tbr_context *ctx = nullptr;
+    int set = -1;  // call-buffer set of its queued work; -1 once retired
+    std::vector<int> slots;
+    std::vector<FrameDev> devs;
+    std::vector<int64_t> ns;
+    std::vector<FrameResult> res;
+    tbr_status st = TBR_OK;
+    std::string msg;
+    float ms = 0.f;
 };
 
 struct tbr_batch;
 static void destroy_context_batches(tbr_context *ctx);
+
+// The device run's verdict from its downloaded counters.
+static tbr_status run_status(const unsigned long long *counters) {
+    if (counters[kCError] & kErrTimeout) return fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
+    if (counters[kCError] & kErrOverflow) return fail(TBR_ERR_INTERNAL, "step limit or capacity exceeded");
+    return TBR_OK;
+}
+
+static void release_frames(Engine &E, const std::vector<int> &slots, const std::vector<FrameDev> &devs) {
+    for (size_t i = 0; i < slots.size(); ++i) {
+        E.blocks.release(devs[i].blk_off, devs[i].n_blocks);
+        E.free_slots.push_back(slots[i]);
+    }
+}
+
+static std::mutex g_tickets_mu;
+static std::unordered_map<tbr_ticket *, tbr_context *> g_tickets;
+
+// Waits for a submitted batch's device work and moves its results out of the
+// call buffers, which are then free for the next submission. Context lock held.
+static void retire_ticket(tbr_ticket *t) {
+    if (t->set < 0) return;
+    Engine &E = t->ctx->E;
+    E.bind_set(t->set);
+    const cudaError_t e = cudaEventSynchronize(E.ev_done);
+    if (e != cudaSuccess) {
+        t->st = TBR_ERR_CUDA;
+        t->msg = std::string("cudaEventSynchronize: ") + cudaGetErrorString(e);
+    } else if ((t->st = run_status(E.h_counters)) != TBR_OK) {
+        t->msg = g_last_error;
+    } else {
+        t->res.assign(E.h_results, E.h_results + t->slots.size());
+        cudaEventElapsedTime(&t->ms, E.ev0, E.ev1);
+    }
+    E.owner[t->set] = nullptr;
+    t->set = -1;
+}
+// Every entry point other than submit and collect starts here (context lock
+// held): the shared call buffers are free afterwards.
+static void retire_tickets(tbr_context *ctx) {
+    for (tbr_ticket *t : ctx->tickets) retire_ticket(t);
+}
+static void destroy_context_tickets(tbr_context *ctx) {
+    std::lock_guard<std::mutex> lk(ctx->E.mu);
+    cudaStreamSynchronize(ctx->E.stream);
+    for (tbr_ticket *t : ctx->tickets) {
+        {
+            std::lock_guard<std::mutex> g(g_tickets_mu);
+            g_tickets.erase(t);
+        }
+        delete t;
+    }
+    ctx->tickets.clear();
+    ctx->E.owner[0] = ctx->E.owner[1] = nullptr;
+}
 
 // =================================================================== C ABI ==
 extern "C" {
@@ -1286,15 +1404,18 @@ tbr_status tbr_context_create(int device, uint64_t workspace_bytes, tbr_context 
 void tbr_context_destroy(tbr_context *ctx) {
     if (!ctx) return;
     destroy_context_batches(ctx);
+    destroy_context_tickets(ctx);
     delete ctx;
 }
 
-static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
-                                  std::vector<FrameResult> &res, std::vector<uint8_t *> masks,
-                                  float *ms_out, int *steps_out, bool device_points = false) {
-    Engine &E = ctx->E;
-    std::vector<int> slots;
-    std::vector<FrameDev> devs;
+// Queues a whole run of the frames on the context's stream and returns: the
+// admission (for a large host batch, ingestion overlapped with the first
+// step), the loop graph, then the results' gather and their download, with the
+// counters, into the bound call buffers (ev0 / ev1 bracket the device run).
+// `slots` and `devs` are set as soon as the frames hold them, whatever happens
+// next (the caller releases them).
+static tbr_status enqueue_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                 std::vector<int> &slots, std::vector<FrameDev> &devs, bool device_points) {
     int64_t max_n = 0;
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
@@ -1312,27 +1433,36 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
             st = E.launch_graph((int)slots.size(), o.hr);
         }
     }
-    if (st == TBR_OK) TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    if (st) return st;
+    TBR_CUDA(cudaEventRecord(E.ev1, E.stream));
+    // Everything the caller gets back in one round trip: the results in the
+    // order of the active list (= slots) and the counters.
+    const int n = (int)slots.size();
+    k_gather_results<<<(int)std::min<size_t>(1024, (n * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0,
+                       E.stream>>>(E.P.results, E.d_active, n, E.d_res_stage);
+    TBR_CUDA(cudaGetLastError());
+    TBR_CUDA(cudaMemcpyAsync(E.h_results, E.d_res_stage, sizeof(FrameResult) * n, cudaMemcpyDeviceToHost,
+                             E.stream));
+    TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
+    return TBR_OK;
+}
+
+static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                  std::vector<FrameResult> &res, std::vector<uint8_t *> masks,
+                                  float *ms_out, int *steps_out, bool device_points = false) {
+    Engine &E = ctx->E;
+    std::vector<int> slots;
+    std::vector<FrameDev> devs;
+    tbr_status st = enqueue_frames(E, fr, o, slots, devs, device_points);
     if (st == TBR_OK) {
-        // Everything the caller gets back in one round trip: the results in
-        // the order of the active list (= slots), the masks, the counters.
-        const int n = (int)slots.size();
-        k_gather_results<<<(int)std::min<size_t>(1024, (n * (sizeof(FrameResult) / 8) + 255) / 256), 256, 0,
-                           E.stream>>>(E.P.results, E.d_active, n, E.d_res_stage);
-        TBR_CUDA(cudaGetLastError());
-        TBR_CUDA(cudaMemcpyAsync(E.h_results, E.d_res_stage, sizeof(FrameResult) * n, cudaMemcpyDeviceToHost,
-                                 E.stream));
         for (size_t i = 0; i < slots.size(); ++i)
             if (i < masks.size() && masks[i])
                 TBR_CUDA(cudaMemcpyAsync(masks[i], E.P.mask + devs[i].blk_off * kSub, fr[i].n,
                                          cudaMemcpyDeviceToHost, E.stream));
-        TBR_CUDA(cudaMemcpyAsync(E.h_counters, E.P.counters, 8 * kCNum, cudaMemcpyDeviceToHost, E.stream));
         TBR_CUDA(cudaStreamSynchronize(E.stream));
-        if (E.h_counters[kCError] & kErrTimeout) st = fail(TBR_ERR_TIMEOUT, "bounded device wait expired");
-        else if (E.h_counters[kCError] & kErrOverflow)
-            st = fail(TBR_ERR_INTERNAL, "step limit or capacity exceeded");
+        st = run_status(E.h_counters);
         if (st == TBR_OK) {
-            res.assign(E.h_results, E.h_results + n);
+            res.assign(E.h_results, E.h_results + slots.size());
             if (steps_out) *steps_out = (int)E.h_counters[kCSteps];
             float ms = 0.f;
             cudaEventElapsedTime(&ms, E.ev0, E.ev1);
@@ -1340,10 +1470,7 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
         }
     }
     cudaStreamSynchronize(E.stream);
-    for (size_t i = 0; i < slots.size(); ++i) {
-        E.blocks.release(devs[i].blk_off, devs[i].n_blocks);
-        E.free_slots.push_back(slots[i]);
-    }
+    release_frames(E, slots, devs);
     return st;
 }
 
@@ -1382,6 +1509,7 @@ tbr_status tbr_estimate_absolute_pose(tbr_context *ctx, const double *points2D, 
         fh.replay_count = ext->replay_count;
     }
     std::lock_guard<std::mutex> lk(ctx->E.mu);
+    retire_tickets(ctx);
     std::vector<FrameResult> res;
     float ms = 0.f;
     int steps = 0;
@@ -1454,6 +1582,7 @@ tbr_status tbr_estimate_batch(tbr_context *ctx, const tbr_frame_desc *frames, in
         fr.push_back(frame_host(frames[i], ro));
     }
     std::lock_guard<std::mutex> lk(ctx->E.mu);
+    retire_tickets(ctx);
     std::vector<FrameResult> res;
     std::vector<uint8_t *> masks(n_frames, nullptr);
     if (inliers)
@@ -1496,6 +1625,7 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
         fr.push_back(frame_host(d, ro));
     }
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     if (stream) {  // the producer's pending writes come first
         TBR_CUDA(cudaEventRecord(E.ev_ingest, (cudaStream_t)stream));
@@ -1517,12 +1647,106 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
     return TBR_OK;
 }
 
+tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                     tbr_ticket **ticket) {
+    if (!ctx || !frames || n_frames < 1 || !ticket) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    *ticket = nullptr;
+    if (n_frames > kMaxActive) return fail(TBR_ERR_INVALID_ARG, "more than 1024 frames in one submission");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (tbr_status c = check_ransac(ro)) return c;
+    RunOptions o = make_run_options(&ro, nullptr, ext);
+    std::vector<FrameHost> fr;
+    for (int i = 0; i < n_frames; ++i) {
+        if (tbr_status c = check_frame(frames[i])) return c;
+        fr.push_back(frame_host(frames[i], ro));
+    }
+    std::lock_guard<std::mutex> lk(ctx->E.mu);
+    Engine &E = ctx->E;
+    const int k = E.next_set;
+    if (E.owner[k]) retire_ticket(E.owner[k]);  // the oldest submission's downloads use set k
+    E.bind_set(k);
+    std::unique_ptr<tbr_ticket> t(new tbr_ticket);
+    tbr_status st = enqueue_frames(E, fr, o, t->slots, t->devs, false);
+    if (st == TBR_OK) {
+        const cudaError_t e = cudaEventRecord(E.ev_done, E.stream);
+        if (e != cudaSuccess) st = fail(TBR_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
+    }
+    if (st) {
+        cudaStreamSynchronize(E.stream);
+        release_frames(E, t->slots, t->devs);
+        return st;
+    }
+    t->ctx = ctx;
+    t->set = k;
+    for (auto &f : fr) t->ns.push_back(f.n);
+    E.owner[k] = t.get();
+    E.next_set = k ^ 1;
+    ctx->tickets.push_back(t.get());
+    {
+        std::lock_guard<std::mutex> g(g_tickets_mu);
+        g_tickets[t.get()] = ctx;
+    }
+    *ticket = t.release();
+    return TBR_OK;
+}
+
+tbr_status tbr_estimate_batch_collect(tbr_ticket *t, tbr_frame_result *results, uint8_t *const *inliers) {
+    tbr_context *ctx = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_tickets_mu);
+        auto it = t ? g_tickets.find(t) : g_tickets.end();
+        if (it == g_tickets.end())
+            return fail(TBR_ERR_INVALID_ARG, "unknown ticket (collected, or its context destroyed)");
+        ctx = it->second;
+        g_tickets.erase(it);
+    }
+    Engine &E = ctx->E;
+    std::lock_guard<std::mutex> lk(E.mu);
+    retire_ticket(t);
+    tbr_status st = t->st;
+    std::string msg = t->msg;
+    const size_t n = t->slots.size();
+    if (st == TBR_OK && inliers) {
+        // On a stream of their own: the masks wait for nothing queued since.
+        for (size_t i = 0; i < n && st == TBR_OK; ++i) {
+            if (!inliers[i]) continue;
+            const cudaError_t e = cudaMemcpyAsync(inliers[i], E.P.mask + t->devs[i].blk_off * kSub, t->ns[i],
+                                                  cudaMemcpyDeviceToHost, E.stream_out);
+            if (e != cudaSuccess) {
+                st = TBR_ERR_CUDA;
+                msg = std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e);
+            }
+        }
+        const cudaError_t e = cudaStreamSynchronize(E.stream_out);
+        if (st == TBR_OK && e != cudaSuccess) {
+            st = TBR_ERR_CUDA;
+            msg = std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e);
+        }
+    }
+    if (st == TBR_OK && results)
+        for (size_t i = 0; i < n; ++i) {
+            for (int k = 0; k < 4; ++k) results[i].q[k] = t->res[i].q[k];
+            for (int k = 0; k < 3; ++k) results[i].t[k] = t->res[i].t[k];
+            results[i].status = TBR_OK;
+            fill_stats(t->res[i], t->ns[i], &results[i].stats, t->ms);
+        }
+    release_frames(E, t->slots, t->devs);
+    ctx->tickets.erase(std::find(ctx->tickets.begin(), ctx->tickets.end(), t));
+    delete t;
+    if (st) return fail(st, msg);
+    return TBR_OK;
+}
+
 tbr_status tbr_get_inliers(tbr_context *ctx, const double q[4], const double t[3], const double *x,
                            const double *X, int64_t n, double sq_threshold, uint8_t *inliers,
                            int64_t *count) {
     if (!ctx || !q || !t || !x || !X || n < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     if (n == 0) {
         if (count) *count = 0;
@@ -1590,6 +1814,7 @@ tbr_status tbr_bundle_adjust(tbr_context *ctx, const double *x, const double *X,
     const bool weighted = honor && weights != nullptr;
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     RunOptions o;
     FrameHost fh{x, X, std::max<int64_t>(n, 1), {K[0], K[1], K[2], K[3]}, 0, 1.0, nullptr, 0};
@@ -1739,6 +1964,7 @@ tbr_status tbr_batch_create(tbr_context *ctx, const tbr_frame_desc *frames, int3
     }
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     auto *b = new tbr_batch();
     b->ctx = ctx;
@@ -1795,6 +2021,7 @@ tbr_status tbr_batch_autotune(tbr_batch *b, int32_t repeats, tbr_tune_entry *ent
     if (!live_batch(b) || repeats < 1 || max < 0) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(b->ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     const int n = (int)b->slots.size();
     struct Shape {
@@ -1887,6 +2114,7 @@ tbr_status tbr_batch_run(tbr_batch *b) {
     if (!live_batch(b)) return fail(TBR_ERR_INVALID_ARG, "NULL or destroyed batch");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(b->ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaEventRecord(b->e0, E.stream));
     TBR_CUDA(cudaGraphLaunch(b->exec, E.stream));
@@ -1909,6 +2137,7 @@ tbr_status tbr_batch_results(tbr_batch *b, tbr_frame_result *results) {
     if (!live_batch(b) || !results) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(b->ctx);
     TBR_CUDA(cudaStreamSynchronize(E.stream));
     float ms = 0.f;
     if (b->launched) cudaEventElapsedTime(&ms, b->e0, b->e1);
@@ -1929,6 +2158,7 @@ tbr_status tbr_batch_profile(tbr_batch *b, tbr_kernel_profile *out, int32_t max,
     if (!live_batch(b) || !out) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = b->ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(b->ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     Engine::Profile pr;
     k_reset_frames<<<b->Q.n_active, 128, 0, E.stream>>>(b->Q, b->d_init);
@@ -1953,6 +2183,7 @@ tbr_status tbr_measure_fp32_peak(tbr_context *ctx, double *tflops) {
     if (!ctx || !tflops) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     const int blocks = E.num_sms * 8, threads = 256, iters = 1 << 14;
     float *sink = (float *)E.P.hS32;  // never written (see k_fp32_peak)
@@ -1975,6 +2206,7 @@ void tbr_batch_destroy(tbr_batch *b) {
         if (!b || !g_batches.erase(b)) return;  // NULL, or already freed with its context
     }
     std::lock_guard<std::mutex> lk(b->ctx->E.mu);
+    retire_tickets(b->ctx);
     batch_free(b);
 }
 
@@ -2514,6 +2746,7 @@ tbr_status tbr_debug_score_samples(tbr_context *ctx, const double *points2D, con
         return fail(TBR_ERR_INVALID_ARG, "bad arguments");
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     RunOptions o;
     if (ext) {  // scoring shape only
         tbr_ext_options sh;
@@ -2672,6 +2905,7 @@ tbr_status tbr_debug_bounded_wait(tbr_context *ctx, uint32_t polls) {
     if (!ctx || polls < 1 || polls > (1u << 22)) return fail(TBR_ERR_INVALID_ARG, "polls must be in [1, 2^22]");
     Engine &E = ctx->E;
     std::lock_guard<std::mutex> lk(E.mu);
+    retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
     k_debug_bounded_wait<<<1, 32, 0, E.stream>>>(E.P.counters, polls);
