@@ -485,6 +485,63 @@ def estimate_batch(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None =
     return out
 
 
+def estimate_batch_submit(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None) -> "BatchTicket":
+    """Queues the frames' whole run (tbr_estimate_batch_submit) and returns at
+    once; BatchTicket.collect() waits for it and returns what estimate_batch
+    returns. Submitting the next batch before collecting this one overlaps the
+    host work of a call (descriptors, staging, launches, the result round trip)
+    with the device work of the previous one; a context runs two submitted
+    batches at a time. The frames' arrays are read while the batch runs, so
+    the ticket keeps them referenced until collect."""
+    arr, keep = _frame_descs(frames)
+    ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+    ext = _lib.ExtOptionsC()
+    h = C.c_void_p()
+    with ctx._lock:
+        check(_lib.lib().tbr_estimate_batch_submit(ctx.handle, arr, len(frames), C.byref(ro), C.byref(ext),
+                                                   C.byref(h)))
+    return BatchTicket(ctx, h, [keep[2 * i].shape[0] for i in range(len(frames))], keep)
+
+
+class BatchTicket:
+    """A submitted batch (estimate_batch_submit); collect() once."""
+
+    def __init__(self, ctx: Context, handle, ns, keep):
+        self.ctx, self._h, self._ns, self._keep = ctx, handle, ns, keep
+
+    def collect(self, masks: bool = False, as_array: bool = False):
+        """Waits for the batch and returns its results as estimate_batch does."""
+        if not self._h:
+            raise RuntimeError("ticket already collected")
+        n = len(self._ns)
+        res = (_lib.FrameResultC * n)()
+        mbufs = mptrs = None
+        if masks:
+            mbufs = [np.zeros(k, np.uint8) for k in self._ns]
+            mptrs = (C.c_void_p * n)(*[m.ctypes.data for m in mbufs])
+        h, self._h = self._h, None
+        try:
+            with self.ctx._lock:
+                check(_lib.lib().tbr_estimate_batch_collect(h, res, C.cast(mptrs, C.c_void_p) if masks else None))
+        finally:
+            self._keep = None
+        out = _results(res, n, as_array)
+        if as_array:
+            return (out, mbufs) if masks else out
+        if masks:
+            for o, m in zip(out, mbufs):
+                o["inliers"] = m
+        return out
+
+    def __del__(self):
+        try:  # an uncollected ticket: release its frames' workspace
+            if self._h:
+                h, self._h = self._h, None
+                _lib.lib().tbr_estimate_batch_collect(h, None, None)
+        except Exception:
+            pass
+
+
 def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None,
                           as_array: bool = False):
     """Frames whose correspondences are already on the context's GPU

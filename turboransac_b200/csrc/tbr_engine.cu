@@ -203,10 +203,18 @@ class Engine {
     void *d_stage_alias = nullptr;              // device address of the pinned staging buffer
     cudaEvent_t ev_done = nullptr;              // a submitted batch's downloads have landed
     cudaStream_t stream_out = nullptr;          // inlier masks of a collected batch
+    // Ingestion of the first part of a host batch runs on stream_in, beside
+    // whatever the context stream still runs (it writes only the new frames'
+    // blocks, from tables in d_ingest_first); the context stream waits on
+    // ev_in before it prepares those frames.
+    cudaStream_t stream_in = nullptr;
+    cudaEvent_t ev_in = nullptr;
+    char *d_ingest_first = nullptr;
     std::mutex mu;  // one call at a time per context
 
-    // Per-call host buffers: h_stage (with its size and device alias),
-    // h_counters, h_results, ev0, ev1 and ev_done above are the bound set;
+    // Per-call buffers: h_stage (with its size and device alias),
+    // d_ingest_first, h_counters, h_results, ev0, ev1 and ev_done above are
+    // the bound set;
     // `spare` holds the other one. Submitted batches use the two sets in turn
     // (next_set), so that one can be staged while the other's copies and
     // downloads are still queued; owner[k] is the ticket whose queued work
@@ -215,6 +223,7 @@ class Engine {
         void *h_stage = nullptr;
         size_t h_stage_bytes = 0;
         void *d_stage_alias = nullptr;
+        char *d_ingest_first = nullptr;
         unsigned long long *h_counters = nullptr;
         FrameResult *h_results = nullptr;
         cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_done = nullptr;
@@ -227,6 +236,7 @@ class Engine {
         std::swap(h_stage, spare.h_stage);
         std::swap(h_stage_bytes, spare.h_stage_bytes);
         std::swap(d_stage_alias, spare.d_stage_alias);
+        std::swap(d_ingest_first, spare.d_ingest_first);
         std::swap(h_counters, spare.h_counters);
         std::swap(h_results, spare.h_results);
         std::swap(ev0, spare.ev0);
@@ -253,6 +263,8 @@ class Engine {
         if (ev_ingest) cudaEventDestroy(ev_ingest);
         if (ev_done) cudaEventDestroy(ev_done);
         if (stream_out) cudaStreamDestroy(stream_out);
+        if (stream_in) cudaStreamDestroy(stream_in);
+        if (ev_in) cudaEventDestroy(ev_in);
         if (spare.h_stage) cudaFreeHost(spare.h_stage);
         if (spare.h_counters) cudaFreeHost(spare.h_counters);
         if (spare.h_results) cudaFreeHost(spare.h_results);
@@ -279,6 +291,8 @@ class Engine {
         TBR_CUDA(cudaEventCreateWithFlags(&ev_ingest, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreateWithFlags(&ev_done, cudaEventDisableTiming));
         TBR_CUDA(cudaStreamCreateWithFlags(&stream_out, cudaStreamNonBlocking));
+        TBR_CUDA(cudaStreamCreateWithFlags(&stream_in, cudaStreamNonBlocking));
+        TBR_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
         TBR_CUDA(cudaEventCreate(&spare.ev0));
         TBR_CUDA(cudaEventCreate(&spare.ev1));
         TBR_CUDA(cudaEventCreateWithFlags(&spare.ev_done, cudaEventDisableTiming));
@@ -310,6 +324,8 @@ class Engine {
         add((void **)&d_admit, sizeof(FrameDev) * kMaxActive);
         add((void **)&d_res_stage, sizeof(FrameResult) * kMaxActive);
         add((void **)&d_ingest, kIngestTableBytes);
+        add((void **)&d_ingest_first, kIngestTableBytes);
+        add((void **)&spare.d_ingest_first, kIngestTableBytes);
         add((void **)&d_res_slots, sizeof(int32_t) * kMaxActive);
         add((void **)&P.uv64, 16 * np);
         add((void **)&P.X64, 24 * np);
@@ -1010,15 +1026,16 @@ static size_t ingest_tile_bytes(const std::vector<FrameHost> &fr) {
 // Writes a table (count header + tiles) at byte `off` of the pinned mirror
 // `h` and enqueues its upload to the same offset of d_ingest; returns the
 // device address of the table and advances `off`.
-static const int64_t *put_table(Engine &E, char *h, size_t &off, const std::vector<IngestTile> &t) {
+static const int64_t *put_table(Engine &E, char *h, size_t &off, const std::vector<IngestTile> &t,
+                                 char *d_tables, cudaStream_t st) {
     if (off + 16 + sizeof(IngestTile) * t.size() > Engine::kIngestTableBytes) return nullptr;
     int64_t *hdr = (int64_t *)(h + off);
     hdr[0] = (int64_t)t.size();
     hdr[1] = 0;
     if (!t.empty()) std::memcpy(hdr + 2, t.data(), sizeof(IngestTile) * t.size());
     const size_t bytes = 16 + sizeof(IngestTile) * t.size();
-    const int64_t *d = (const int64_t *)(E.d_ingest + off);
-    if (cudaMemcpyAsync((void *)d, hdr, bytes, cudaMemcpyHostToDevice, E.stream) != cudaSuccess) return nullptr;
+    const int64_t *d = (const int64_t *)(d_tables + off);
+    if (cudaMemcpyAsync((void *)d, hdr, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess) return nullptr;
     off += (bytes + 15) & ~size_t(15);
     return d;
 }
@@ -1044,9 +1061,11 @@ static const void *mapped_address(const void *p) {
 // kStaggerFirstShare of the bytes) is ingested and prepared before the loop
 // graph starts; the rest is admitted kPending and ingested and prepared by the
 // graph itself beside the first engine step, and starts RANSAC in the second
-// (a frame's samples and results do not depend on the step it starts in;
-// nothing waits on another stream). E.ev0 then marks the start of the first
-// part's preparation.
+// (a frame's samples and results do not depend on the step it starts in).
+// The first part is ingested on stream_in, so that it overlaps whatever the
+// context stream still runs (a batch submitted before); the context stream
+// waits for it before the preparation. E.ev0 then marks the start of the
+// first part's preparation.
 //
 // `slots`, `max_n` and `devs` are set as soon as the frames hold slots (the
 // caller releases them whatever happens next).
@@ -1149,6 +1168,10 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
         while (left[g].load(std::memory_order_acquire) > 0) std::this_thread::yield();
     };
     const size_t tile = ingest_tile_bytes(fr);
+    // With `launch` the first part is ingested on stream_in, beside the work
+    // still queued on the context stream (the new frames' blocks and their
+    // tables are this call's alone).
+    cudaStream_t in = launch ? E.stream_in : E.stream;
     auto enqueue = [&]() -> tbr_status {
         tbr_status s2 = upload_records(E, A);
         if (s2) return s2;
@@ -1164,15 +1187,18 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
             t.clear();
             for (size_t k = gb[g]; k < gb[g + 1]; ++k) add_frame_tiles(t, E, A.devs[k], fr[k].n, su[k], sx[k], tile);
             wait_group(g);
-            const int64_t *d = put_table(E, h, off, t);
+            const int64_t *d = put_table(E, h, off, t, launch ? E.d_ingest_first : E.d_ingest, in);
             if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
-            k_ingest<<<Engine::kIngestGridHost, 256, 0, E.stream>>>(d);
+            k_ingest<<<Engine::kIngestGridHost, 256, 0, in>>>(d);
             TBR_CUDA(cudaGetLastError());
         }
         if (!launch) return TBR_OK;
+        TBR_CUDA(cudaEventRecord(E.ev_in, in));
+        TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_in, 0));
         size_t off0 = 0;
         wait_group(G);  // the graph reads the late frames' staging copies
-        if (!put_table(E, h, off0, late)) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+        if (!put_table(E, h, off0, late, E.d_ingest, E.stream))
+            return fail(TBR_ERR_CUDA, "ingestion table upload failed");
         TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
         Pools Qf = E.P;
         Qf.n_active = (int32_t)n_first;
@@ -1219,7 +1245,7 @@ static tbr_status admit_frames(Engine &E, const std::vector<FrameHost> &fr, cons
         const size_t tile = ingest_tile_bytes(fr);
         for (size_t i = 0; i < fr.size(); ++i) add_frame_tiles(t, E, A.devs[i], fr[i].n, fr[i].uv, fr[i].xyz, tile);
         size_t off = 0;
-        const int64_t *d = put_table(E, (char *)E.h_stage + rec, off, t);
+        const int64_t *d = put_table(E, (char *)E.h_stage + rec, off, t, E.d_ingest, E.stream);
         if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
         k_ingest<<<E.num_sms * 2, 256, 0, E.stream>>>(d);
         TBR_CUDA(cudaGetLastError());
