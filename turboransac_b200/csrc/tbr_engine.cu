@@ -1065,7 +1065,9 @@ static const void *mapped_address(const void *p) {
 // The first part is ingested on stream_in, so that it overlaps whatever the
 // context stream still runs (a batch submitted before); the context stream
 // waits for it before the preparation. E.ev0 then marks the start of the
-// first part's preparation.
+// first part's preparation. Without `stagger` (a submission queued behind
+// another batch, whose run hides the ingestion) every frame is in the first
+// part and the plain loop graph runs.
 //
 // `slots`, `max_n` and `devs` are set as soon as the frames hold slots (the
 // caller releases them whatever happens next).
@@ -1076,7 +1078,7 @@ constexpr double kStaggerFirstShare = 0.35;
 
 static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
                                     std::vector<int> &slots, int64_t &max_n, std::vector<FrameDev> &devs,
-                                    bool launch) {
+                                    bool launch, bool stagger = true) {
     constexpr size_t kPiece = 1u << 20;
     const size_t n = fr.size();
     const size_t tab_off = stage_bytes(fr);
@@ -1106,7 +1108,7 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
     }
     size_t n_first = n;
     Engine::Stagger sg;
-    if (launch) {
+    if (launch && stagger) {
         size_t acc = 0;
         const size_t first = (size_t)(kStaggerFirstShare * (double)total);
         n_first = 0;
@@ -1195,10 +1197,12 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
         if (!launch) return TBR_OK;
         TBR_CUDA(cudaEventRecord(E.ev_in, in));
         TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_in, 0));
-        size_t off0 = 0;
-        wait_group(G);  // the graph reads the late frames' staging copies
-        if (!put_table(E, h, off0, late, E.d_ingest, E.stream))
-            return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+        if (stagger) {
+            size_t off0 = 0;
+            wait_group(G);  // the graph reads the late frames' staging copies
+            if (!put_table(E, h, off0, late, E.d_ingest, E.stream))
+                return fail(TBR_ERR_CUDA, "ingestion table upload failed");
+        }
         TBR_CUDA(cudaEventRecord(E.ev0, E.stream));
         Pools Qf = E.P;
         Qf.n_active = (int32_t)n_first;
@@ -1206,7 +1210,7 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
         for (size_t k = 0; k < n_first; ++k) max_first = std::max(max_first, fr[k].n);
         E.launch_prep(Qf, (int)n_first, max_first, E.stream);
         E.pp = o.pp;
-        return E.launch_graph((int)n, o.hr, &sg);
+        return E.launch_graph((int)n, o.hr, stagger ? &sg : nullptr);
     };
     st = enqueue();
     for (auto &x : th) x.join();
@@ -1436,12 +1440,14 @@ void tbr_context_destroy(tbr_context *ctx) {
 
 // Queues a whole run of the frames on the context's stream and returns: the
 // admission (for a large host batch, ingestion overlapped with the first
-// step), the loop graph, then the results' gather and their download, with the
+// step, or -- `behind` another queued batch -- with that batch's run), the
+// loop graph, then the results' gather and their download, with the
 // counters, into the bound call buffers (ev0 / ev1 bracket the device run).
 // `slots` and `devs` are set as soon as the frames hold them, whatever happens
 // next (the caller releases them).
 static tbr_status enqueue_frames(Engine &E, const std::vector<FrameHost> &fr, const RunOptions &o,
-                                 std::vector<int> &slots, std::vector<FrameDev> &devs, bool device_points) {
+                                 std::vector<int> &slots, std::vector<FrameDev> &devs, bool device_points,
+                                 bool behind = false) {
     int64_t max_n = 0;
     TBR_CUDA(cudaSetDevice(E.device));
     TBR_CUDA(cudaMemsetAsync(E.P.counters, 0, 8 * kCNum, E.stream));
@@ -1449,7 +1455,7 @@ static tbr_status enqueue_frames(Engine &E, const std::vector<FrameHost> &fr, co
     for (auto &f : fr) in_bytes += 40 * (size_t)f.n;
     tbr_status st;
     if (!device_points && fr.size() >= 2 && in_bytes >= kStaggerMinBytes) {
-        st = admit_host_frames(E, fr, o, slots, max_n, devs, true);
+        st = admit_host_frames(E, fr, o, slots, max_n, devs, true, !behind);
     } else {
         st = admit_frames(E, fr, o, slots, max_n, &devs, device_points);
         if (st == TBR_OK) {
@@ -1695,7 +1701,9 @@ tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *fra
     if (E.owner[k]) retire_ticket(E.owner[k]);  // the oldest submission's downloads use set k
     E.bind_set(k);
     std::unique_ptr<tbr_ticket> t(new tbr_ticket);
-    tbr_status st = enqueue_frames(E, fr, o, t->slots, t->devs, false);
+    // Queued behind the other set's batch (not yet waited for): that run
+    // hides this one's whole ingestion, so no staggered start.
+    tbr_status st = enqueue_frames(E, fr, o, t->slots, t->devs, false, E.owner[k ^ 1] != nullptr);
     if (st == TBR_OK) {
         const cudaError_t e = cudaEventRecord(E.ev_done, E.stream);
         if (e != cudaSuccess) st = fail(TBR_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
