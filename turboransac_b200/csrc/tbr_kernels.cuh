@@ -1015,6 +1015,7 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
         const int b0 = ch * f.chunk_blocks;
         const int b1 = min(f.n_blocks, b0 + f.chunk_blocks);
         const int ntiles = (b1 - b0 + 1) / 2;
+        const int64_t fn = f.n;  // read once: the asm barriers below would reload it every tile
         const float2 *g = P.pts32 + (f.blk_off + b0) * kBlockFloat2;
         auto tile_blocks = [&](int i) { return min(2, b1 - b0 - 2 * i); };
         if (tid == 0) {
@@ -1037,7 +1038,7 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
             if (s) ph1 ^= 1u; else ph0 ^= 1u;
             // A row of this thread's point.
             const int64_t p0 = (int64_t)(b0 + 2 * i) * kSub;
-            const int cnt = (int)min((int64_t)tile_blocks(i) * kSub, f.n - p0);
+            const int cnt = (int)min((int64_t)tile_blocks(i) * kSub, fn - p0);
             const bool v = tid < cnt;
             const float2 *tb = sPts + s * 2 * kBlockFloat2 + (tid >> 6) * kBlockFloat2;
             const int j = tid & (kSub - 1);
