@@ -1840,6 +1840,11 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     const double cam[4] = {f.lm_cam[0], f.lm_cam[1], f.lm_cam[2], f.lm_cam[3]};
     const double inv_sq_thr = f.lm_inv_sq_thr;
     const int64_t max_it = f.skip_refine ? 0 : f.lm_max_iter;
+    // Read once: every barrier of the loop would reload them from the record.
+    const double grad_tol = f.lm_grad_tol, step_tol = f.lm_step_tol, min_lambda = f.lm_min_lambda,
+                 max_lambda = f.lm_max_lambda, thr = f.lm_thr;
+    const int loss = f.lm_loss;
+    const bool weighted = f.lm_weighted != 0;
 
     auto cluster_totals = [&]() {  // after lm_pass: every CTA's part -> rank 0's tot
         cluster.sync();
@@ -1857,7 +1862,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
     }
     __syncthreads();
     if (max_it > 0)
-        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch, part);
+        lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, loss, thr, weighted, scratch, part);
     else if (threadIdx.x < kLMSums) part[threadIdx.x] = 0.0;
     __syncthreads();
     // One CTA: its pass totals are the frame's; a cluster sums its CTAs' in rank 0.
@@ -1891,7 +1896,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
                     g[k] = Jc[21 + k];
                     gn += g[k] * g[k];
                 }
-                if (sqrt(gn) < f.lm_grad_tol) brk = 1;
+                if (sqrt(gn) < grad_tol) brk = 1;
             }
             for (int k = 0; k < 6; ++k) J[k * 7] += lambda;
             double x[6];
@@ -1901,7 +1906,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
                 x[k] = -1 * x[k];
                 sn += x[k] * x[k];
             }
-            if (sqrt(sn) < f.lm_step_tol) brk = 1;
+            if (sqrt(sn) < step_tol) brk = 1;
             quat_step_post(q, x, qn);  // jaco.cuh:288-299
             double dt[3];
             quat_rotate(q, x[3], x[4], x[5], dt);
@@ -1912,8 +1917,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             // the pass's own barriers order this thread's next writes to them.
             __syncthreads();
             if (brk) break;
-            lm_pass(P, base, i0, i1, qn, tn, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch,
-                    part);
+            lm_pass(P, base, i0, i1, qn, tn, cam, inv_sq_thr, loss, thr, weighted, scratch, part);
         } else {
             cluster.sync();
             if (threadIdx.x == 0) {
@@ -1924,8 +1928,7 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             }
             __syncthreads();
             if (pbrk) break;
-            lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, f.lm_loss, f.lm_thr, f.lm_weighted != 0, scratch,
-                    part);
+            lm_pass(P, base, i0, i1, pq, pt, cam, inv_sq_thr, loss, thr, weighted, scratch, part);
             __syncthreads();
             cluster_totals();
         }
@@ -1933,14 +1936,14 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
             if (T[0] < cost) {
                 for (int k = 0; k < 4; ++k) q[k] = qn[k];
                 for (int k = 0; k < 3; ++k) t[k] = tn[k];
-                lambda = fmax(f.lm_min_lambda, lambda / 10);
+                lambda = fmax(min_lambda, lambda / 10);
                 cost = T[0];
                 for (int k = 0; k < 27; ++k) Jc[k] = T[1 + k];
                 recompute = 1;
             } else {
                 ++invalid;
                 for (int k = 0; k < 6; ++k) J[k * 7] -= lambda;
-                lambda = fmin(f.lm_max_lambda, lambda * 10);
+                lambda = fmin(max_lambda, lambda * 10);
                 recompute = 0;
             }
             ++iters;
