@@ -541,6 +541,9 @@ class Engine {
     static constexpr size_t kIngestTableBytes = 64 * 32 + sizeof(IngestTile) * kIngestTileCap;
     static constexpr int kIngestGridHost = 16;  // CTAs of a zero-copy ingestion: the link saturates at 16, and
                                                 // late frames are read beside the first engine step
+    static constexpr int kIngestGridBeside = 8;  // ... of one that runs beside another batch's run: there the
+                                                 // SMs it takes from that run cost more than link rate
+                                                 // (measured: 37.0k frames/s end to end against 36.4k with 16)
 
     // Split admission of a graph: the active frames from n_first on arrive
     // during the first step (kPending; their ingestion table at d_ingest).
@@ -1191,7 +1194,7 @@ static tbr_status admit_host_frames(Engine &E, const std::vector<FrameHost> &fr,
             wait_group(g);
             const int64_t *d = put_table(E, h, off, t, launch ? E.d_ingest_first : E.d_ingest, in);
             if (!d) return fail(TBR_ERR_CUDA, "ingestion table upload failed");
-            k_ingest<<<Engine::kIngestGridHost, 256, 0, in>>>(d);
+            k_ingest<<<stagger ? Engine::kIngestGridHost : Engine::kIngestGridBeside, 256, 0, in>>>(d);
             TBR_CUDA(cudaGetLastError());
         }
         if (!launch) return TBR_OK;
