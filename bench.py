@@ -700,8 +700,22 @@ def main():
         dt = time.perf_counter() - t0
         if i:
             dev_t.append(dt)
-    e2e_device_fps = world * args.frames * len(dev_t) / max_over_ranks(pg, sum(dev_t), dev)
-    del dframes
+    e2e_device_sync_fps = world * args.frames * len(dev_t) / max_over_ranks(pg, sum(dev_t), dev)
+    # ... and in its submitted form, two batches in flight, as the host leg.
+    from turboransac_b200 import estimate_batch_device_submit
+    w0, w1 = estimate_batch_device_submit(ctx, dframes, ro), estimate_batch_device_submit(ctx, dframes, ro)
+    w0.collect(as_array=True)
+    w1.collect(as_array=True)
+    k = max(2, args.steps)
+    t0 = time.perf_counter()
+    prev = estimate_batch_device_submit(ctx, dframes, ro)
+    for _ in range(k - 1):
+        cur = estimate_batch_device_submit(ctx, dframes, ro)
+        prev.collect(as_array=True)
+        prev = cur
+    prev.collect(as_array=True)
+    e2e_device_fps = world * args.frames * k / max_over_ranks(pg, time.perf_counter() - t0, dev)
+    del dframes, w0, w1, prev, cur
 
     # Plain per-frame calls (the reference's calling pattern) on the same frames.
     plain = None
@@ -775,7 +789,10 @@ def main():
                                            "call": "estimate_batch(ctx, frames, ro, as_array=True)"}},
             "e2e_device_inputs": {"value": e2e_device_fps, "unit": "frames/s", "h2d_bytes_per_step": 0,
                                   "d2h_bytes_per_step": d2h,
-                                  "inputs": "correspondences already in device memory (CUDA tensors)"},
+                                  "inputs": "correspondences already in device memory (CUDA tensors)",
+                                  "call": "estimate_batch_device_submit each step, then the previous step's "
+                                          "ticket.collect(as_array=True)",
+                                  "one_call_at_a_time": e2e_device_sync_fps},
             "plain_call": plain,
             "config0_plain": c0,
             "config1_scoring": c1,

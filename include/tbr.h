@@ -257,6 +257,13 @@ tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *fra
                                      const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
                                      tbr_ticket **ticket);
 tbr_status tbr_estimate_batch_collect(tbr_ticket *ticket, tbr_frame_result *results, uint8_t *const *inliers);
+/* The submitted form of tbr_estimate_batch_device (same rules as above, same
+ * collect): the frames' arrays are device memory of the context's GPU, copied
+ * after the work queued so far on `stream` (a cudaStream_t; NULL: the caller
+ * guarantees the data is ready), and must stay unchanged until collect. */
+tbr_status tbr_estimate_batch_device_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                            const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                            void *stream, tbr_ticket **ticket);
 
 /* Device-resident batch: upload once (host->device), run many times with the
  * inputs already in HBM, download results. run() launches the captured graph

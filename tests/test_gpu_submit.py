@@ -6,8 +6,8 @@ submission, and never after the context is gone."""
 import numpy as np
 import pytest
 
-from turboransac_b200 import (Camera_cuda, Context, RansacOptions_cuda, TbrError, estimate_batch,
-                              estimate_batch_submit, scenes)
+from turboransac_b200 import (Camera_cuda, Context, DeviceFrame, RansacOptions_cuda, TbrError, estimate_batch,
+                              estimate_batch_device, estimate_batch_device_submit, estimate_batch_submit, scenes)
 
 pytestmark = pytest.mark.gpu
 
@@ -89,3 +89,24 @@ def test_collect_after_context_destroy_is_refused(ctx):
     (r,) = estimate_batch_submit(ctx, [f], RO).collect()  # other contexts are unaffected
     (ref,) = estimate_batch(ctx, [f], RO)
     same([r], [ref], masks=False)
+
+
+def test_device_input_submissions_match_the_device_call(ctx):
+    """Device-resident correspondences through the submitted form, in flight
+    beside host submissions: the results of the device call and of the host
+    call, bit for bit, masks included."""
+    import torch
+    a, b, c = groups()
+    da, dc = [DeviceFrame(f) for f in a], [DeviceFrame(f) for f in c]
+    torch.cuda.synchronize()
+    ref_a = estimate_batch_device(ctx, da, RO)
+    ref_b = estimate_batch(ctx, b, RO)
+    ref_c = estimate_batch(ctx, c, RO, masks=True)
+    t1 = estimate_batch_device_submit(ctx, da, RO)
+    t2 = estimate_batch_submit(ctx, b, RO)
+    t3 = estimate_batch_device_submit(ctx, dc, RO)  # waits for t1's device work first
+    same(t1.collect(), ref_a, masks=False)
+    same(t3.collect(masks=True), ref_c)
+    same(t2.collect(), ref_b, masks=False)
+    with pytest.raises(ValueError):  # host arrays are refused by the device form
+        estimate_batch_device_submit(ctx, a, RO)

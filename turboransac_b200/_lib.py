@@ -114,7 +114,7 @@ EXPORTS = [
     "tbr_batch_results", "tbr_batch_destroy", "tbr_batch_profile", "tbr_batch_autotune", "tbr_measure_fp32_peak", "tbr_server_create", "tbr_server_submit",
     "tbr_server_submit_nocopy", "tbr_server_get_stats", "tbr_server_poll", "tbr_server_cancel", "tbr_server_drain", "tbr_server_destroy",
     "tbr_debug_score_samples", "tbr_debug_bounded_wait", "tbr_msac_score_noalloc",
-    "tbr_estimate_batch_submit", "tbr_estimate_batch_collect",
+    "tbr_estimate_batch_submit", "tbr_estimate_batch_collect", "tbr_estimate_batch_device_submit",
 ]
 
 
@@ -146,6 +146,9 @@ def lib() -> C.CDLL:
     L.tbr_estimate_batch_submit.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32, C.POINTER(RansacOptionsC),
                                             C.POINTER(ExtOptionsC), C.POINTER(vp)]
     L.tbr_estimate_batch_collect.argtypes = [vp, C.POINTER(FrameResultC), vp]
+    L.tbr_estimate_batch_device_submit.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32,
+                                                   C.POINTER(RansacOptionsC), C.POINTER(ExtOptionsC), vp,
+                                                   C.POINTER(vp)]
     L.tbr_batch_create.argtypes = [vp, C.POINTER(FrameDescC), C.c_int32, C.POINTER(RansacOptionsC),
                                    C.POINTER(ExtOptionsC), C.POINTER(vp)]
     L.tbr_batch_run.argtypes = [vp]

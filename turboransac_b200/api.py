@@ -542,21 +542,17 @@ class BatchTicket:
             pass
 
 
-def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None,
-                          as_array: bool = False):
-    """Frames whose correspondences are already on the context's GPU
-    (tbr_estimate_batch_device). Each frame has `uv` (n, 2) and `xyz` (n, 3)
-    float64 contiguous CUDA tensors (or objects with data_ptr()), `K` and
-    `seed`. `stream`: a torch.cuda.Stream (default: torch's current stream) whose
-    queued work the copy waits for. Results come back to the host, as dicts or
-    (as_array=True) as one record array of RESULT_DTYPE."""
+def _device_descs(frames):
+    """tbr_frame_desc entries of frames with contiguous float64 CUDA tensors
+    `uv` (n, 2) and `xyz` (n, 3): (record array, frame count)."""
     import torch
     f64 = torch.float64
     m = len(frames)
     uvs = [fr.uv for fr in frames]
     xyzs = [fr.xyz for fr in frames]
     for i, (u, x) in enumerate(zip(uvs, xyzs)):
-        if not (u.is_cuda and x.is_cuda and u.dtype == f64 and x.dtype == f64 and u.dim() == 2 and x.dim() == 2
+        if not (getattr(u, "is_cuda", False) and getattr(x, "is_cuda", False) and u.dtype == f64 and x.dtype == f64
+                and u.dim() == 2 and x.dim() == 2
                 and u.is_contiguous() and x.is_contiguous()):
             raise ValueError(f"frame {i}: uv and xyz must be contiguous float64 CUDA tensors (n, 2), (n, 3)")
         su, sx = u.shape, x.shape
@@ -574,6 +570,37 @@ def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda |
         a["seed"] = np.array(sd, np.uint64)
     except (OverflowError, ValueError, TypeError):
         a["seed"] = np.array([int(s) & _U64 for s in sd], np.uint64)
+    return a, m
+
+
+def estimate_batch_device_submit(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None,
+                                 stream=None) -> "BatchTicket":
+    """The submitted form of estimate_batch_device (tbr_estimate_batch_device_submit):
+    queues the run and returns a BatchTicket at once. The frames' tensors must
+    stay unchanged until collect; the ticket keeps them referenced."""
+    import torch
+    a, m = _device_descs(frames)
+    ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
+    ext = _lib.ExtOptionsC()
+    st = stream if stream is not None else torch.cuda.current_stream()
+    h = C.c_void_p()
+    with ctx._lock:
+        check(_lib.lib().tbr_estimate_batch_device_submit(ctx.handle, a.ctypes.data_as(C.POINTER(_lib.FrameDescC)),
+                                                          m, C.byref(ro), C.byref(ext), C.c_void_p(st.cuda_stream),
+                                                          C.byref(h)))
+    return BatchTicket(ctx, h, [int(fr.uv.shape[0]) for fr in frames], [(fr.uv, fr.xyz) for fr in frames])
+
+
+def estimate_batch_device(ctx: Context, frames, ransac_opt: RansacOptions_cuda | None = None, stream=None,
+                          as_array: bool = False):
+    """Frames whose correspondences are already on the context's GPU
+    (tbr_estimate_batch_device). Each frame has `uv` (n, 2) and `xyz` (n, 3)
+    float64 contiguous CUDA tensors (or objects with data_ptr()), `K` and
+    `seed`. `stream`: a torch.cuda.Stream (default: torch's current stream) whose
+    queued work the copy waits for. Results come back to the host, as dicts or
+    (as_array=True) as one record array of RESULT_DTYPE."""
+    import torch
+    a, m = _device_descs(frames)
     ro = (ransac_opt or RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)).to_c()
     ext = _lib.ExtOptionsC()
     res = (_lib.FrameResultC * m)()

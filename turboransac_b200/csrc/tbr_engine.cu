@@ -1599,6 +1599,26 @@ static FrameHost frame_host(const tbr_frame_desc &d, const tbr_ransac_options &r
     return {d.points2D, d.points3D, d.n, {d.K[0], d.K[1], d.K[2], d.K[3]}, d.seed,
             d.max_reproj_error > 0 ? d.max_reproj_error : ro.max_reproj_error, nullptr, 0};
 }
+// The device-input calls' frames: the plain call's checks, and both arrays
+// device memory of the context's GPU.
+static tbr_status device_frames(Engine &E, const tbr_frame_desc *frames, int32_t n, const tbr_ransac_options &ro,
+                                std::vector<FrameHost> &fr) {
+    for (int i = 0; i < n; ++i) {
+        const tbr_frame_desc &d = frames[i];
+        if (tbr_status c = check_frame(d)) return c;
+        for (const void *p : {(const void *)d.points2D, (const void *)d.points3D}) {
+            cudaPointerAttributes a;
+            if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory");
+            }
+            if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != E.device)
+                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory of the context's GPU");
+        }
+        fr.push_back(frame_host(d, ro));
+    }
+    return TBR_OK;
+}
 
 extern "C" {
 
@@ -1645,20 +1665,7 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
     RunOptions o = make_run_options(&ro, nullptr, ext);
     Engine &E = ctx->E;
     std::vector<FrameHost> fr;
-    for (int i = 0; i < n_frames; ++i) {
-        const tbr_frame_desc &d = frames[i];
-        if (tbr_status c = check_frame(d)) return c;
-        for (const void *p : {(const void *)d.points2D, (const void *)d.points3D}) {
-            cudaPointerAttributes a;
-            if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-                cudaGetLastError();
-                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory");
-            }
-            if ((a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) || a.device != E.device)
-                return fail(TBR_ERR_INVALID_ARG, "frame points are not device memory of the context's GPU");
-        }
-        fr.push_back(frame_host(d, ro));
-    }
+    if (tbr_status c = device_frames(E, frames, n_frames, ro, fr)) return c;
     std::lock_guard<std::mutex> lk(E.mu);
     retire_tickets(ctx);
     TBR_CUDA(cudaSetDevice(E.device));
@@ -1682,31 +1689,27 @@ tbr_status tbr_estimate_batch_device(tbr_context *ctx, const tbr_frame_desc *fra
     return TBR_OK;
 }
 
-tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
-                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
-                                     tbr_ticket **ticket) {
-    if (!ctx || !frames || n_frames < 1 || !ticket) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
-    *ticket = nullptr;
-    if (n_frames > kMaxActive) return fail(TBR_ERR_INVALID_ARG, "more than 1024 frames in one submission");
-    tbr_ransac_options ro;
-    tbr_default_ransac_options(&ro);
-    if (ransac_opt) ro = *ransac_opt;
-    if (tbr_status c = check_ransac(ro)) return c;
-    RunOptions o = make_run_options(&ro, nullptr, ext);
-    std::vector<FrameHost> fr;
-    for (int i = 0; i < n_frames; ++i) {
-        if (tbr_status c = check_frame(frames[i])) return c;
-        fr.push_back(frame_host(frames[i], ro));
-    }
+}  // extern "C"
+
+// The locked half of both submit calls: queue the run on the next call-buffer
+// set and hand out its ticket. With device_points the frames' arrays are
+// device memory, copied after the work queued on `stream` (if any).
+static tbr_status submit_frames(tbr_context *ctx, const std::vector<FrameHost> &fr, const RunOptions &o,
+                                bool device_points, void *stream, tbr_ticket **ticket) {
     std::lock_guard<std::mutex> lk(ctx->E.mu);
     Engine &E = ctx->E;
     const int k = E.next_set;
     if (E.owner[k]) retire_ticket(E.owner[k]);  // the oldest submission's downloads use set k
     E.bind_set(k);
+    if (device_points && stream) {  // the producer's pending writes come first
+        TBR_CUDA(cudaSetDevice(E.device));
+        TBR_CUDA(cudaEventRecord(E.ev_ingest, (cudaStream_t)stream));
+        TBR_CUDA(cudaStreamWaitEvent(E.stream, E.ev_ingest, 0));
+    }
     std::unique_ptr<tbr_ticket> t(new tbr_ticket);
     // Queued behind the other set's batch (not yet waited for): that run
     // hides this one's whole ingestion, so no staggered start.
-    tbr_status st = enqueue_frames(E, fr, o, t->slots, t->devs, false, E.owner[k ^ 1] != nullptr);
+    tbr_status st = enqueue_frames(E, fr, o, t->slots, t->devs, device_points, E.owner[k ^ 1] != nullptr);
     if (st == TBR_OK) {
         const cudaError_t e = cudaEventRecord(E.ev_done, E.stream);
         if (e != cudaSuccess) st = fail(TBR_ERR_CUDA, std::string("cudaEventRecord: ") + cudaGetErrorString(e));
@@ -1728,6 +1731,43 @@ tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *fra
     }
     *ticket = t.release();
     return TBR_OK;
+}
+
+extern "C" {
+
+tbr_status tbr_estimate_batch_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                     const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                     tbr_ticket **ticket) {
+    if (!ctx || !frames || n_frames < 1 || !ticket) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    *ticket = nullptr;
+    if (n_frames > kMaxActive) return fail(TBR_ERR_INVALID_ARG, "more than 1024 frames in one submission");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (tbr_status c = check_ransac(ro)) return c;
+    RunOptions o = make_run_options(&ro, nullptr, ext);
+    std::vector<FrameHost> fr;
+    for (int i = 0; i < n_frames; ++i) {
+        if (tbr_status c = check_frame(frames[i])) return c;
+        fr.push_back(frame_host(frames[i], ro));
+    }
+    return submit_frames(ctx, fr, o, false, nullptr, ticket);
+}
+
+tbr_status tbr_estimate_batch_device_submit(tbr_context *ctx, const tbr_frame_desc *frames, int32_t n_frames,
+                                            const tbr_ransac_options *ransac_opt, const tbr_ext_options *ext,
+                                            void *stream, tbr_ticket **ticket) {
+    if (!ctx || !frames || n_frames < 1 || !ticket) return fail(TBR_ERR_INVALID_ARG, "bad arguments");
+    *ticket = nullptr;
+    if (n_frames > kMaxActive) return fail(TBR_ERR_INVALID_ARG, "more than 1024 frames in one submission");
+    tbr_ransac_options ro;
+    tbr_default_ransac_options(&ro);
+    if (ransac_opt) ro = *ransac_opt;
+    if (tbr_status c = check_ransac(ro)) return c;
+    RunOptions o = make_run_options(&ro, nullptr, ext);
+    std::vector<FrameHost> fr;
+    if (tbr_status c = device_frames(ctx->E, frames, n_frames, ro, fr)) return c;
+    return submit_frames(ctx, fr, o, true, stream, ticket);
 }
 
 tbr_status tbr_estimate_batch_collect(tbr_ticket *t, tbr_frame_result *results, uint8_t *const *inliers) {
