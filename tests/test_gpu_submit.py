@@ -110,3 +110,21 @@ def test_device_input_submissions_match_the_device_call(ctx):
     same(t2.collect(), ref_b, masks=False)
     with pytest.raises(ValueError):  # host arrays are refused by the device form
         estimate_batch_device_submit(ctx, a, RO)
+
+
+def test_submission_beyond_the_free_workspace_is_refused():
+    """A small workspace: the second batch's points do not fit beside the
+    uncollected first one (TBR_ERR_OOM); the first is unaffected and the
+    second fits once the first is collected."""
+    c2 = Context(0, 512 << 20)
+    try:
+        big = [scenes.make_frame(30000, 0.5, 1.0, 9600 + i) for i in range(40)]
+        ref = estimate_batch(c2, big, RO)
+        t1 = estimate_batch_submit(c2, big, RO)
+        with pytest.raises(TbrError) as e:
+            estimate_batch_submit(c2, big, RO)
+        assert e.value.status == 2
+        same(t1.collect(), ref, masks=False)
+        same(estimate_batch_submit(c2, big, RO).collect(), ref, masks=False)
+    finally:
+        c2.close()
