@@ -70,3 +70,29 @@ def test_single_round_beyond_cap_is_flagged_and_deterministic(ctx):
     np.testing.assert_array_equal(r["q"], p0.q)
     np.testing.assert_array_equal(r["t"], p0.t)
     assert all(o["candidate_overflow"] == 0 for o in out[1:])
+
+
+def test_redo_in_normal_mode_keeps_multi_round_steps_and_matches_oracle(ctx, oracle):
+    """A small low-inlier frame of the serving pool (432 points, 100000 samples):
+    its multi-round steps hold more than 4096 candidates, so such a step is
+    redone, and later steps are sized by the candidate rate (several rounds each,
+    not one). The sample count, the selection and the pose are the FP64
+    oracle's; a batch with other frames gives the same."""
+    f = scenes.serving_request(216)
+    assert f.n == 432
+    ro = RansacOptions_cuda(max_iterations=1000, max_reproj_error=4.0)
+    st, pose, inl = ctx.estimate_absolute_pose(f.uv, f.xyz, CAM, ro, BundleOptions_cuda(), seed=f.seed)
+    d = st.details
+    o = oracle.estimate(f.uv, f.xyz, f.K, 4.0, seed=f.seed, samples_per_round=1000, threads=8)
+    info = o["info"]
+    assert d["samples"] == info.ransac.samples == 100000
+    assert d["best_sample"] == info.ransac.best_sample and d["best_solution"] == info.ransac.best_sol
+    assert abs(d["model_score"] - info.ransac.score) <= 1e-12 * info.ransac.score
+    assert d["candidate_overflow"] == 0
+    assert d["steps"] < d["rounds"] // 2  # steps of several rounds after the redo
+    np.testing.assert_array_equal(inl, o["inliers"])
+    assert quat_angle(pose.q, o["q"]) < 1e-6 and np.abs(pose.t - o["t"]).max() < 1e-6
+    mixed = estimate_batch(ctx, scenes.batched_frames(6, scale=0.3) + [f], ro)
+    r = mixed[-1]
+    assert r["samples"] == d["samples"] and r["best_sample"] == d["best_sample"]
+    assert quat_angle(r["q"], pose.q) < 1e-9

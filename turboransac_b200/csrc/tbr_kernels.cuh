@@ -1174,9 +1174,12 @@ __global__ void __launch_bounds__(kTcThreads, 4) k_score_tc(Pools P) {
 // absolute margin, and the candidate band contains the safe band. The band is
 // never narrowed. When more than kMaxCandFrame hypotheses fall inside it:
 //   * a step of several rounds (forced mode: more than kSplitSamples samples)
-//     is redone: the frame's later steps are limited to one round (forced:
-//     kSplitSamples samples), which bounds the candidates by 4 * B, and
-//     k_finalize discards this step. A frame's samples, selection and stop
+//     is redone: the frame's later steps are limited to the rounds that the
+//     step's candidate rate leaves room for (half the cap, and fewer rounds
+//     than the redone step, so repeated redos end at one round, which bounds
+//     the candidates by 4 * B; forced: kSplitSamples samples), and k_finalize
+//     discards this step; every step that fits then re-sizes the limit from
+//     its own rate, up or down. A frame's samples, selection and stop
 //     point do not depend on how its rounds are grouped into steps, so this
 //     changes no result;
 //   * a single round (B > kMaxCandFrame / 4) keeps the kMaxCandFrame smallest
@@ -1239,7 +1242,12 @@ __global__ void k_select(Pools P) {
         int want = cnt0, md = 0;                 // 0: every candidate
         if (cnt0 > kMaxCandFrame) {
             if (splittable) {
-                f.split = forced ? kSplitSamples : 1;
+                // Later steps run at most as many rounds as this step's
+                // candidate rate leaves room for with a margin of two, and
+                // fewer than this step's, so that repeated redos end at one
+                // round (forced mode: kSplitSamples samples).
+                f.split = forced ? kSplitSamples
+                                 : (int)max(1LL, min((long long)R - 1, (long long)kMaxCandFrame * R / (2LL * cnt0)));
                 want = 0;
                 md = 2;                          // redo the step
             } else {
@@ -1255,7 +1263,15 @@ __global__ void k_select(Pools P) {
                 md = 2;
             }
         }
-        if (md == 2) f.redo = 1;
+        if (md == 2) {
+            f.redo = 1;
+        } else if (!forced && f.split > 0) {
+            // A step that fit after a redo: its candidate rate sizes the next
+            // ones (margin of two), up as well as down, since the rate falls
+            // once a good model has been found.
+            f.split = (int)min((long long)kMaxRoundsPerStep,
+                               max(1LL, (long long)kMaxCandFrame * R / (2LL * max(cnt0, 1))));
+        }
         mode = md;
         need = (unsigned)want;
         kstar = ~0ull;
