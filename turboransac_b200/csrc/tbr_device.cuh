@@ -198,10 +198,22 @@ __device__ __forceinline__ void pose_from_depths(const d3 x[3], const d3 &X0, do
     }
 }
 
-// P3P for three unit bearings and world points; up to 4 poses written to
-// out[12*k]; returns their number. Same reorder, conic split, root filters
-// and early exit as p3p.cuh:9-222.
-__device__ int p3p_solve(const d3 xin[3], const d3 Xin[3], double *out) {
+// What every candidate of one P3P sample needs after the root filters: the
+// reordered bearings and first world point, inv([X01 X02 X01xX02]) and the
+// squared distances / bearing cosines of the depth polish.
+struct P3PCtx {
+    d3 x[3];
+    d3 X0;
+    double Mi[9];
+    double a01, a02, a12, m01, m02, m12;
+};
+
+// P3P for three unit bearings and world points, up to the candidates: the
+// depth triples that pass the root filters, in the order p3p.cuh:9-222 visits
+// them (line 0 then 1, root 0 then 1, the same early exit after line 0),
+// written to dep[3*k]; returns their number. Same reorder, conic split and
+// root filters as there.
+__device__ int p3p_candidates(const d3 xin[3], const d3 Xin[3], P3PCtx &c, double *dep) {
     d3 x[3] = {xin[0], xin[1], xin[2]};
     d3 X[3] = {Xin[0], Xin[1], Xin[2]};
     d3 X01 = d3sub(X[0], X[1]);
@@ -288,6 +300,10 @@ __device__ int p3p_solve(const d3 xin[3], const d3 Xin[3], double *out) {
         }
     }
 
+    for (int k = 0; k < 3; ++k) c.x[k] = x[k];
+    c.X0 = X[0];
+    for (int k = 0; k < 9; ++k) c.Mi[k] = Mi[k];
+    c.a01 = a01, c.a02 = a02, c.a12 = a12, c.m01 = m01, c.m02 = m02, c.m12 = m12;
     int n_sols = 0;
     for (int i = 0; i < 2; ++i) {
         const double p0 = pq[i][0], p1 = pq[i][1], p2 = pq[i][2];
@@ -305,8 +321,7 @@ __device__ int p3p_solve(const d3 xin[3], const d3 Xin[3], double *out) {
                 double d1 = tau * d2;
                 double d0 = (w0 * d2 + w1 * d1);
                 if (d0 < 0) continue;
-                polish_depths(d0, d1, d2, a01, a02, a12, m01, m02, m12);
-                pose_from_depths(x, X[0], d0, d1, d2, Mi, out + 12 * n_sols);
+                dep[3 * n_sols] = d0, dep[3 * n_sols + 1] = d1, dep[3 * n_sols + 2] = d2;
                 ++n_sols;
             }
         } else {
@@ -323,14 +338,30 @@ __device__ int p3p_solve(const d3 xin[3], const d3 Xin[3], double *out) {
                 double d1 = tau * d0;
                 double d2 = w0 * d0 + w1 * d1;
                 if (d2 < 0.0) continue;
-                polish_depths(d0, d1, d2, a01, a02, a12, m01, m02, m12);
-                pose_from_depths(x, X[0], d0, d1, d2, Mi, out + 12 * n_sols);
+                dep[3 * n_sols] = d0, dep[3 * n_sols + 1] = d1, dep[3 * n_sols + 2] = d2;
                 ++n_sols;
             }
         }
         if (n_sols > 0 && G) break;
     }
     return n_sols;
+}
+
+// One candidate of p3p_candidates to its pose (12 doubles, row-major [R | t]):
+// the depth polish, then the pose from the depths (p3p.cuh's inner loop).
+__device__ __forceinline__ void p3p_finish(const P3PCtx &c, double d0, double d1, double d2, double *P) {
+    polish_depths(d0, d1, d2, c.a01, c.a02, c.a12, c.m01, c.m02, c.m12);
+    pose_from_depths(c.x, c.X0, d0, d1, d2, c.Mi, P);
+}
+
+// P3P for three unit bearings and world points; up to 4 poses written to
+// out[12*k]; returns their number (p3p.cuh:9-222).
+__device__ __forceinline__ int p3p_solve(const d3 xin[3], const d3 Xin[3], double *out) {
+    P3PCtx c;
+    double dep[12];
+    const int n = p3p_candidates(xin, Xin, c, dep);
+    for (int k = 0; k < n; ++k) p3p_finish(c, dep[3 * k], dep[3 * k + 1], dep[3 * k + 2], out + 12 * k);
+    return n;
 }
 
 // ---------------------------------------------------------- quaternions -----

@@ -460,20 +460,37 @@ __global__ void k_plan(Pools P) {
 // ransac.cuh:176-217). Solutions are appended to the frame's hypothesis region
 // with one atomic per frame per warp; each carries id = sample*4 + solution,
 // so ordering never depends on scheduling.
+// One thread per sample draws its triple and finds its P3P candidates (the
+// root filters); the warp then shares out the candidates -- 0 to 4 a sample --
+// so that the depth polish and the pose, most of the arithmetic, run on full
+// warps instead of once per candidate slot that any lane of the warp needs.
+// Every candidate runs p3p_solve's own steps (p3p_finish) and keeps its order
+// (hId = sample * 4 + solution); the compiler may fuse a multiply-add
+// differently than in a per-thread loop, so poses can differ from that form in
+// the last bits, never in which samples give solutions.
+struct P3PStage {  // one lane's sample, staged for its warp
+    P3PCtx c;
+    double dep[12];
+    int64_t h0, s;  // its first hypothesis slot, its sample id
+    int a, n;       // active index of its frame, candidates
+};
 __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
+    __shared__ P3PStage stage[128];
+    __shared__ int excl[128];
     const int64_t total = (int64_t)P.counters[kCSamplesTotal];
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, wb = threadIdx.x & ~31;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t g0 = (int64_t)blockIdx.x * blockDim.x; g0 < total; g0 += stride) {
         const int64_t g = g0 + threadIdx.x;
         const bool valid = g < total;
+        P3PStage &me = stage[threadIdx.x];
         int a = -1;
         int nsol = 0;
-        double sols[48];
+        int64_t s = 0;
         if (valid) {
             a = find_segment(P.sample_prefix, P.n_active, g);
             const FrameDev &f = P.frames[P.active[a]];
-            const int64_t s = f.step_first + (g - P.sample_prefix[a]);
+            s = f.step_first + (g - P.sample_prefix[a]);
             int32_t idx[3];
             if (f.replay) {
                 idx[0] = f.replay[3 * s];
@@ -492,7 +509,7 @@ __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
                 xb[k] = bearing(P.xn64[2 * p], P.xn64[2 * p + 1]);
                 Xs[k] = {P.X64[3 * p], P.X64[3 * p + 1], P.X64[3 * p + 2]};
             }
-            nsol = p3p_solve(xb, Xs, sols);
+            nsol = p3p_candidates(xb, Xs, me.c, me.dep);
         }
         // Warp-aggregated reservation; a warp's samples are contiguous in g, so
         // lanes of one frame form one contiguous run.
@@ -511,45 +528,59 @@ __global__ void __launch_bounds__(128) k_sample_p3p(Pools P) {
         if (lane == first && a >= 0 && grp_total > 0)
             slot0 = atomicAdd(&P.frames[P.active[a]].hyp_count, grp_total);
         slot0 = __shfl_sync(act, slot0, first);
-        if (valid && nsol > 0) {
-            const FrameDev &f = P.frames[P.active[a]];
-            const int64_t s = f.step_first + (g - P.sample_prefix[a]);
-            const int64_t h0 = f.hyp_base + slot0 + (incl - nsol - before);
-            const double itau = 1.0 / f.tau;
-            for (int k = 0; k < nsol; ++k) {
-                const double *S = sols + 12 * k;
-                const int64_t h = h0 + k;
+        if (nsol > 0) me.h0 = P.frames[P.active[a]].hyp_base + slot0 + (incl - nsol - before);
+        me.s = s;
+        me.a = a;
+        me.n = nsol;
+        excl[threadIdx.x] = incl - nsol;
+        const int T = __shfl_sync(0xffffffffu, incl, 31);  // the warp's candidates
+        __syncwarp();
+        for (int j = lane; j < T; j += 32) {
+            // Owner: the last lane whose exclusive prefix is <= j.
+            int lo = 0, hi = 31;
 #pragma unroll
-                for (int e = 0; e < 12; ++e) P.hP64[12 * h + e] = S[e];
-                P.hId[h] = s * 4 + k;
-                // Scoring form: rows 0, 1 scaled by 1/tau, translation moved to the
-                // centred frame (t + R c), all in FP64 before the FP32 rounding.
-                float *Q = P.hP32 + 12 * h;
-                float q32[12];
-                bool finite = true;
-#pragma unroll
-                for (int r = 0; r < 3; ++r) {
-                    const double tc = S[4 * r + 3] + S[4 * r] * f.centre[0] + S[4 * r + 1] * f.centre[1] +
-                                      S[4 * r + 2] * f.centre[2];
-                    const double sc = r < 2 ? itau : 1.0;
-                    q32[4 * r] = (float)(S[4 * r] * sc);
-                    q32[4 * r + 1] = (float)(S[4 * r + 1] * sc);
-                    q32[4 * r + 2] = (float)(S[4 * r + 2] * sc);
-                    q32[4 * r + 3] = (float)(tc * sc);
-                }
-                // Rotation rows (scaled by 1/tau) within 2^40 and translations within
-                // 2^80 keep every depth of a staged point (within 2^80) below 2^123:
-                // no overflow, so no inf - inf and no NaN in the filter.
-#pragma unroll
-                for (int e = 0; e < 12; ++e)
-                    finite = finite && fabsf(q32[e]) <= ((e & 3) == 3 ? 0x1p80f : 0x1p40f);
-                // A pose outside that range scores every point as an outlier
-                // (depth -1, lateral offset 1).
-#pragma unroll
-                for (int e = 0; e < 12; ++e)
-                    Q[e] = finite ? q32[e] : (e == 3 || e == 7 ? 1.0f : (e == 11 ? -1.0f : 0.0f));
+            for (int it = 0; it < 5; ++it) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (excl[wb + mid] <= j) lo = mid; else hi = mid - 1;
             }
+            const P3PStage &o = stage[wb + lo];
+            const int k = j - excl[wb + lo];
+            double S[12];
+            p3p_finish(o.c, o.dep[3 * k], o.dep[3 * k + 1], o.dep[3 * k + 2], S);
+            const FrameDev &f = P.frames[P.active[o.a]];
+            const int64_t h = o.h0 + k;
+            const double itau = 1.0 / f.tau;
+#pragma unroll
+            for (int e = 0; e < 12; ++e) P.hP64[12 * h + e] = S[e];
+            P.hId[h] = o.s * 4 + k;
+            // Scoring form: rows 0, 1 scaled by 1/tau, translation moved to the
+            // centred frame (t + R c), all in FP64 before the FP32 rounding.
+            float *Q = P.hP32 + 12 * h;
+            float q32[12];
+            bool finite = true;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const double tc = S[4 * r + 3] + S[4 * r] * f.centre[0] + S[4 * r + 1] * f.centre[1] +
+                                  S[4 * r + 2] * f.centre[2];
+                const double sc = r < 2 ? itau : 1.0;
+                q32[4 * r] = (float)(S[4 * r] * sc);
+                q32[4 * r + 1] = (float)(S[4 * r + 1] * sc);
+                q32[4 * r + 2] = (float)(S[4 * r + 2] * sc);
+                q32[4 * r + 3] = (float)(tc * sc);
+            }
+            // Rotation rows (scaled by 1/tau) within 2^40 and translations within
+            // 2^80 keep every depth of a staged point (within 2^80) below 2^123:
+            // no overflow, so no inf - inf and no NaN in the filter.
+#pragma unroll
+            for (int e = 0; e < 12; ++e)
+                finite = finite && fabsf(q32[e]) <= ((e & 3) == 3 ? 0x1p80f : 0x1p40f);
+            // A pose outside that range scores every point as an outlier
+            // (depth -1, lateral offset 1).
+#pragma unroll
+            for (int e = 0; e < 12; ++e)
+                Q[e] = finite ? q32[e] : (e == 3 || e == 7 ? 1.0f : (e == 11 ? -1.0f : 0.0f));
         }
+        __syncwarp();  // the staging is reused by the next samples of this warp
     }
 }
 
