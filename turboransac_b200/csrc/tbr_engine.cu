@@ -196,7 +196,7 @@ class Engine {
     int score_grid[6] = {0, 0, 0, 0, 0, 0};  // (HP, PP) = (1,4), (2,2), (2,4), (4,2), (3,2), (3,4)
     int rescore_grid = 0, p3p_grid = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaStream_t stream2 = nullptr;             // refinement branch of captured graphs
+    cudaStream_t stream2 = nullptr;             // late frames' ingestion in captured graphs; serving refinement
     cudaStream_t stream3 = nullptr;             // cluster LM beside the one-CTA LM
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_lm_fork = nullptr, ev_lm_join = nullptr;
@@ -554,8 +554,11 @@ class Engine {
     static int prep_bx(int64_t max_n) { return (int)std::min<int64_t>(64, std::max<int64_t>(1, (max_n + 1023) / 1024)); }
 
     // The step loop as one graph: [reset ->] while (any frame in RANSAC)
-    // { RANSAC step || inliers + LM of the frames that finished in the previous
-    // step (disjoint frames) ; loop test } -> inliers + LM of the last step's.
+    // { RANSAC step ; loop test } -> inliers + LM of every frame. A frame's LM
+    // is latency-bound and each one-CTA LM fills an SM, so running it beside
+    // RANSAC stretched the steps more than refining every frame at the end,
+    // with the whole GPU and clusters from kLMClusterMinTail inliers, costs
+    // (6.46 ms against 6.52 ms a batch of the batched workload).
     // With d_init, a reset node first restores the frames from d_init. With sg,
     // the first step runs before the loop, beside the ingestion and preparation
     // of the frames that arrive late, which start RANSAC in the second step.
@@ -613,12 +616,7 @@ class Engine {
             ok = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
                  cudaSuccess;
             if (ok) {
-                cudaEventRecord(ev_fork, stream);
-                cudaStreamWaitEvent(stream2, ev_fork, 0);
-                launch_refine(Q, n, stream2);
                 launch_ransac(Q, n, hr, stream);
-                cudaEventRecord(ev_join, stream2);
-                cudaStreamWaitEvent(stream, ev_join, 0);
                 k_loop_ctl<<<1, 1, 0, stream>>>(Q, h, 100000ull);
                 ok = cudaStreamEndCapture(stream, &body) == cudaSuccess;
             }
@@ -627,7 +625,7 @@ class Engine {
             cudaGraph_t tail = nullptr;
             ok = cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed) == cudaSuccess;
             if (ok) {
-                Pools Qt = Q;  // nothing runs beside the last step's refinement
+                Pools Qt = Q;  // nothing runs beside the refinement
                 Qt.lm_cluster_min = kLMClusterMinTail;
                 launch_refine(Qt, n, stream);
                 ok = cudaStreamEndCapture(stream, &tail) == cudaSuccess;
@@ -2567,8 +2565,9 @@ static tbr_status server_step(tbr_server *s) {
         E.P.n_active = na;
         if (na >= kServerOverlapFrames) {
             // Many resident frames: the refinement of frames that finished RANSAC
-            // in earlier steps runs beside this step's RANSAC (disjoint frames),
-            // as in the batch graph; a frame is refined one step after it finishes.
+            // in earlier steps runs beside this step's RANSAC (disjoint frames);
+            // a frame is refined one step after it finishes (a stream of requests
+            // has no last step to defer it to, unlike a batch).
             TBR_CUDA(cudaEventRecord(E.ev_fork, E.stream));
             TBR_CUDA(cudaStreamWaitEvent(E.stream2, E.ev_fork, 0));
             E.launch_refine(E.P, na, E.stream2);

@@ -2020,10 +2020,10 @@ __device__ __forceinline__ void lm_frame(const Pools &P, int slot) {
 }
 
 // Frames with fewer inliers than Pools::lm_cluster_min run their LM on one CTA,
-// larger ones on a cluster of kLMCluster CTAs. Beside RANSAC (frames finishing
-// in earlier steps) throughput wins: one CTA up to kLMClusterMin. After the last
-// step nothing else runs and the LM is the whole remaining time: clusters from
-// kLMClusterMinTail.
+// larger ones on a cluster of kLMCluster CTAs. Beside RANSAC (the server's steps
+// with many resident frames) throughput wins: one CTA up to kLMClusterMin. After
+// a batch's last step, and in the server's steps with few frames, nothing else
+// runs and the LM is the whole remaining time: clusters from kLMClusterMinTail.
 constexpr int64_t kLMClusterMin = 10000;
 constexpr int64_t kLMClusterMinTail = 3000;
 
