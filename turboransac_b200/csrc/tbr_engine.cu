@@ -247,6 +247,7 @@ class Engine {
 
     ~Engine() {
         if (stream) cudaStreamSynchronize(stream);
+        if (stream_in) cudaStreamSynchronize(stream_in);
         for (auto &g : graph_cache) cudaGraphExecDestroy(g.exec);
         if (d_base) cudaFree(d_base);
         if (h_stage) cudaFreeHost(h_stage);
@@ -1503,6 +1504,7 @@ static tbr_status estimate_frames(tbr_context *ctx, const std::vector<FrameHost>
         }
     }
     cudaStreamSynchronize(E.stream);
+    cudaStreamSynchronize(E.stream_in);  // an admission that failed may have left ingestion queued there
     release_frames(E, slots, devs);
     return st;
 }
@@ -1714,6 +1716,7 @@ static tbr_status submit_frames(tbr_context *ctx, const std::vector<FrameHost> &
     }
     if (st) {
         cudaStreamSynchronize(E.stream);
+        cudaStreamSynchronize(E.stream_in);  // an admission that failed may have left ingestion queued there
         release_frames(E, t->slots, t->devs);
         return st;
     }
