@@ -49,3 +49,25 @@ def test_no_device_is_a_clean_error():
     st = L.tbr_context_create(0, 0, ctypes.byref(h))
     assert st == 3  # TBR_ERR_CUDA
     assert b"no CUDA device" in L.tbr_last_error()
+
+
+def test_submit_and_collect_refuse_bad_arguments_before_any_device_call():
+    """The submitted batch calls check their arguments on the host: a NULL
+    context, frame list or ticket pointer, and a ticket that was never handed
+    out, are refused with TBR_ERR_INVALID_ARG and a message."""
+    from turboransac_b200 import _lib
+    L = _lib.lib()
+    ro = _lib.RansacOptionsC()
+    L.tbr_default_ransac_options(ctypes.byref(ro))
+    fr = (_lib.FrameDescC * 1)()
+    t = ctypes.c_void_p()
+    assert L.tbr_estimate_batch_submit(None, fr, 1, ctypes.byref(ro), None, ctypes.byref(t)) == 1
+    assert L.tbr_estimate_batch_device_submit(None, fr, 1, ctypes.byref(ro), None, None, ctypes.byref(t)) == 1
+    assert L.tbr_estimate_batch_submit(ctypes.c_void_p(8), None, 1, ctypes.byref(ro), None, ctypes.byref(t)) == 1
+    assert L.tbr_estimate_batch_submit(ctypes.c_void_p(8), fr, 0, ctypes.byref(ro), None, ctypes.byref(t)) == 1
+    assert L.tbr_estimate_batch_submit(ctypes.c_void_p(8), fr, 1, ctypes.byref(ro), None, None) == 1
+    assert L.tbr_estimate_batch_submit(ctypes.c_void_p(8), fr, 1025, ctypes.byref(ro), None, ctypes.byref(t)) == 1
+    assert b"1024" in L.tbr_last_error()
+    assert L.tbr_estimate_batch_collect(None, None, None) == 1
+    assert L.tbr_estimate_batch_collect(ctypes.c_void_p(16), None, None) == 1  # never handed out
+    assert b"unknown ticket" in L.tbr_last_error()
