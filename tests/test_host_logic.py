@@ -89,3 +89,19 @@ def test_camera_parameters_are_the_four_pinhole_values():
     for bad in ([525.0, 319.5, 239.5], [525.0, 525.0, 319.5, 239.5, 0.0]):
         with pytest.raises(ValueError):
             api._camera_K(api.Camera_cuda(1, 640, 480, bad))
+
+
+def test_submitted_forms_check_frames_before_the_context():
+    """estimate_batch_submit refuses malformed host frames, and the device form
+    refuses frames that are not float64 CUDA tensors, on the host before any
+    call reaches the library (no context or GPU is needed to see it)."""
+    import dataclasses
+    f = scenes.plain_frame(0)
+    bad = dataclasses.replace(f, xyz=f.xyz[:-1])
+    with pytest.raises(ValueError):
+        api.estimate_batch_submit(None, [f, bad])
+    with pytest.raises(ValueError):
+        api.estimate_batch_device_submit(None, [f])  # numpy arrays, not CUDA tensors
+    t = api.BatchTicket(None, None, [3], None)
+    with pytest.raises(RuntimeError):  # nothing to collect
+        t.collect()
